@@ -1,0 +1,588 @@
+"""fecl_b200: B200-native batched soft-decision decoding with FeCl's API.
+
+A Python mirror of the FeCl C++ interface (src/Codec.h, src/Ldpc.h, src/Turbo.h,
+src/Trellis.h) on top of the C-ABI in include/fecl_b200.h.  Names, argument
+meaning and error behaviour follow the reference:
+
+    code = Ldpc(Ldpc.EncoderOptions(Ldpc.DvbS2.matrix(16200, Fraction(1, 2))),
+                Ldpc.DecoderOptions().algorithm(Exact).iterations(20))
+    bits = code.decode(llr)                       # Codec::decode, src/Codec.h:210-238
+    out = Codec.Output().msg().state()
+    code.soDecode(Codec.Input().parity(llr), out)  # Codec::soDecode, src/Codec.h:249-307
+
+Host numpy arrays go through FECL_HOST_MEMORY (the call copies in, decodes on
+the GPU and copies out); torch CUDA tensors go through FECL_DEVICE_MEMORY on the
+current torch stream.  Size mismatches raise ValueError, as the reference throws
+std::invalid_argument.  Bits are uint8 0/1 (the reference uses BitField<size_t>).
+"""
+import ctypes as C
+from fractions import Fraction
+
+import numpy as np
+
+from . import _lib
+from ._lib import check as _check
+from ._lib import lib as _L
+
+__all__ = [
+    "Exact", "Linear", "Approximate", "Serial", "Parallel", "Custom",
+    "SparseBitMatrix", "Trellis", "Codec", "Ldpc", "Turbo", "FeclError", "lib_path",
+]
+
+# DecoderAlgorithm (src/DecoderAlgorithm.h:30-34) and SchedulingType (src/SchedulingType.h:32-39)
+Exact, Linear, Approximate = 0, 1, 2
+Serial, Parallel, Custom = 0, 1, 2
+FeclError = _lib.FeclError
+lib_path = _lib.LIB_PATH
+
+
+def _u32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None and a.size else C.c_void_p(0)
+
+
+class SparseBitMatrix:
+    """A binary matrix in CSR form (SparseBitMatrix, src/BitMatrix.h:42-624)."""
+
+    def __init__(self, rows, cols, row_ptr, col_idx):
+        self._rows, self._cols = int(rows), int(cols)
+        self.row_ptr = _u32(row_ptr)
+        self.col_idx = _u32(col_idx)
+        if self.row_ptr.size != self._rows + 1:
+            raise ValueError("row_ptr must hold rows + 1 entries")
+
+    @classmethod
+    def from_dense(cls, dense):
+        d = np.asarray(dense) != 0
+        rows = [np.nonzero(r)[0] for r in d]
+        ptr = np.zeros(len(rows) + 1, dtype=np.uint32)
+        ptr[1:] = np.cumsum([len(r) for r in rows])
+        idx = np.concatenate(rows) if rows else np.zeros(0, np.uint32)
+        return cls(d.shape[0], d.shape[1], ptr, idx)
+
+    def rows(self):
+        return self._rows
+
+    def cols(self):
+        return self._cols
+
+    def size(self):
+        return int(self.col_idx.size)
+
+    def row(self, r):
+        return self.col_idx[self.row_ptr[r]:self.row_ptr[r + 1]]
+
+    def rowSizes(self):
+        return np.diff(self.row_ptr.astype(np.int64))
+
+    def to_dense(self):
+        d = np.zeros((self._rows, self._cols), dtype=np.uint8)
+        for r in range(self._rows):
+            d[r, self.row(r)] = 1
+        return d
+
+    def __eq__(self, other):
+        return (self._rows, self._cols) == (other._rows, other._cols) and np.array_equal(
+            self.row_ptr, other.row_ptr) and np.array_equal(self.col_idx, other.col_idx)
+
+
+class Trellis:
+    """Trellis(constraintLengths, generator, feedback) -- src/Trellis.cpp:76-143.
+    Tables are indexed [state * inputCount + input] (src/Trellis.h:131-172)."""
+    Tail, Truncate = 0, 1
+
+    def __init__(self, constraintLengths, generator, feedback=None):
+        cl = _u32(constraintLengths)
+        gen = np.ascontiguousarray(np.asarray(generator, dtype=np.uint64))
+        if gen.ndim != 2 or gen.shape[0] != cl.size:
+            raise ValueError("Invalid number of generators")
+        fb = None if not feedback else np.ascontiguousarray(np.asarray(feedback, dtype=np.uint64))
+        sc, ic, osz = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _check(_L.fecl_trellis_build(cl.size, _ptr(cl), gen.shape[1], _ptr(gen), _ptr(fb), C.byref(sc), C.byref(ic),
+                                     C.byref(osz), None, None))
+        self.next_state = np.zeros(sc.value * ic.value, dtype=np.uint32)
+        self.output = np.zeros(sc.value * ic.value, dtype=np.uint32)
+        _check(_L.fecl_trellis_build(cl.size, _ptr(cl), gen.shape[1], _ptr(gen), _ptr(fb), C.byref(sc), C.byref(ic),
+                                     C.byref(osz), _ptr(self.next_state), _ptr(self.output)))
+        self._sc, self._ic, self._os = sc.value, ic.value, osz.value
+
+    def stateCount(self):
+        return self._sc
+
+    def inputCount(self):
+        return self._ic
+
+    def outputSize(self):
+        return self._os
+
+    def getNextState(self, s, u):
+        return int(self.next_state[s * self._ic + u])
+
+    def getOutput(self, s, u):
+        return int(self.output[s * self._ic + u])
+
+    def _c(self):
+        return _lib.fecl_trellis(self._sc, self._ic, self._os, self.next_state.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                 self.output.ctypes.data_as(C.POINTER(C.c_uint32)))
+
+
+def _is_device(x):
+    return hasattr(x, "is_cuda") and x.is_cuda
+
+
+def _dtype_code(a):
+    if _is_device(a):
+        import torch
+        m = {torch.float64: _lib.F64, torch.float32: _lib.F32, torch.float16: _lib.F16}
+    else:
+        m = {np.dtype(np.float64): _lib.F64, np.dtype(np.float32): _lib.F32, np.dtype(np.float16): _lib.F16}
+    try:
+        return m[a.dtype]
+    except KeyError:
+        raise ValueError("L-values must be float64, float32 or float16")
+
+
+class Codec:
+    """fec::Codec (src/Codec.h:46-127): the operations every code family offers."""
+
+    class Input:
+        """Codec::Input (src/detail/Codec.h:142-171): parity (required), syst, state."""
+
+        def __init__(self):
+            self._v = {}
+
+        def parity(self, x):
+            self._v["parity"] = x
+            return self
+
+        def syst(self, x):
+            self._v["syst"] = x
+            return self
+
+        def state(self, x):
+            self._v["state"] = x
+            return self
+
+        def msg(self, x):
+            self._v["msg"] = x
+            return self
+
+    class Output:
+        """Codec::Output: name the outputs wanted; after soDecode, call them without
+        argument to read the arrays (host) or tensors (device)."""
+
+        def __init__(self, dtype=np.float64):
+            self._want = []
+            self._v = {}
+            self.dtype = dtype
+
+        def _get_or_want(self, name):
+            if name in self._v:
+                return self._v[name]
+            self._want.append(name)
+            return self
+
+        def msg(self):
+            return self._get_or_want("msg")
+
+        def syst(self):
+            return self._get_or_want("syst")
+
+        def parity(self):
+            return self._get_or_want("parity")
+
+        def state(self):
+            return self._get_or_want("state")
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+        s = _lib.fecl_sizes()
+        _check(_L.fecl_codec_sizes(self._h, C.byref(s)))
+        self._sizes = (s.msg, s.syst, s.parity, s.state)
+        self._work_group = 8
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _L.fecl_destroy(h)
+            self._h = C.c_void_p(0)
+
+    def msgSize(self):
+        return self._sizes[0]
+
+    def systSize(self):
+        return self._sizes[1]
+
+    def paritySize(self):
+        return self._sizes[2]
+
+    def stateSize(self):
+        return self._sizes[3]
+
+    # Codec::getWorkGroupSize / setWorkGroupSize (src/Codec.h:65-66): a CPU thread count
+    # in the reference; kept for API compatibility, the device decoder ignores it.
+    def getWorkGroupSize(self):
+        return self._work_group
+
+    def setWorkGroupSize(self, n):
+        self._work_group = int(n)
+
+    def _frames(self, n, size, what):
+        blocks = n // size
+        if n != blocks * size:
+            raise ValueError("Invalid size for %s" % what)
+        return blocks
+
+    def encode(self, msg):
+        """Codec::encode -- src/Codec.h:171-198."""
+        m = np.ascontiguousarray(np.asarray(msg, dtype=np.uint8).ravel())
+        n = self._frames(m.size, self.msgSize(), "message")
+        parity = np.zeros(n * self.paritySize(), dtype=np.uint8)
+        _check(_L.fecl_encode(self._h, _ptr(m), n, _ptr(parity), _lib.HOST_MEMORY, None))
+        return parity
+
+    def check(self, parity):
+        """Codec::check -- src/Codec.h:137-145."""
+        p = np.ascontiguousarray(np.asarray(parity, dtype=np.uint8).ravel())
+        n = self._frames(p.size, self.paritySize(), "parity")
+        ok = C.c_int32(0)
+        _check(_L.fecl_check(self._h, _ptr(p), n, C.byref(ok)))
+        return bool(ok.value)
+
+    def decode(self, parity, iterations=False):
+        """Codec::decode -- src/Codec.h:210-238.  Returns the hard message bits and,
+        with iterations=True, the per-frame iteration counts."""
+        if _is_device(parity):
+            import torch
+            x = parity.contiguous().view(-1)
+            n = self._frames(x.numel(), self.paritySize(), "parity")
+            msg = torch.empty(n * self.msgSize(), dtype=torch.uint8, device=x.device)
+            it = torch.empty(n, dtype=torch.int32, device=x.device) if iterations else None
+            stream = torch.cuda.current_stream(x.device).cuda_stream
+            _check(_L.fecl_decode(self._h, C.c_void_p(x.data_ptr()), _dtype_code(x), n, C.c_void_p(msg.data_ptr()),
+                                  C.c_void_p(it.data_ptr()) if it is not None else None, _lib.DEVICE_MEMORY,
+                                  C.c_void_p(stream)))
+            return (msg, it) if iterations else msg
+        x = np.asarray(parity)
+        if x.dtype not in (np.float64, np.float32, np.float16):
+            x = x.astype(np.float64)
+        x = np.ascontiguousarray(x.ravel())
+        n = self._frames(x.size, self.paritySize(), "parity")
+        msg = np.zeros(n * self.msgSize(), dtype=np.uint8)
+        it = np.zeros(n, dtype=np.int32) if iterations else None
+        _check(_L.fecl_decode(self._h, _ptr(x), _dtype_code(x), n, _ptr(msg), _ptr(it) if it is not None else None,
+                              _lib.HOST_MEMORY, None))
+        return (msg, it) if iterations else msg
+
+    def soDecode(self, input, output):
+        """Codec::soDecode -- src/Codec.h:249-307."""
+        v = input._v
+        if "parity" not in v:
+            raise ValueError("Input must contains parity")
+        if "msg" in v:
+            raise ValueError("Input should not contain msg")
+        par = v["parity"]
+        device = _is_device(par)
+        n_par = par.numel() if device else np.asarray(par).size
+        n = self._frames(n_par, self.paritySize(), "parity")
+        if "syst" in v and (v["syst"].numel() if device else np.asarray(v["syst"]).size) != n * self.systSize():
+            raise ValueError("Invalid size for msg")
+        if "state" in v and (v["state"].numel() if device else np.asarray(v["state"]).size) != n * self.stateSize():
+            raise ValueError("Invalid size for state")
+        sizes = {"msg": self.msgSize(), "syst": self.systSize(), "parity": self.paritySize(), "state": self.stateSize()}
+        io = _lib.fecl_so_io()
+        keep = []
+        if device:
+            import torch
+            dt = par.dtype
+            ins = {k: v[k].contiguous().view(-1).to(dt) for k in ("parity", "syst", "state") if k in v}
+            odt = torch.float64 if output.dtype == np.float64 else torch.float32
+            outs = {k: torch.empty(n * sizes[k], dtype=odt, device=par.device) for k in output._want}
+            ptr = lambda t: t.data_ptr()
+            flags = _lib.DEVICE_MEMORY
+            stream = C.c_void_p(torch.cuda.current_stream(par.device).cuda_stream)
+            io.in_dtype = _dtype_code(ins["parity"])
+        else:
+            x = np.asarray(par)
+            dt = x.dtype if x.dtype in (np.float64, np.float32, np.float16) else np.float64
+            ins = {k: np.ascontiguousarray(np.asarray(v[k], dtype=dt).ravel()) for k in ("parity", "syst", "state") if k in v}
+            odt = np.float64 if output.dtype == np.float64 else np.float32
+            outs = {k: np.zeros(n * sizes[k], dtype=odt) for k in output._want}
+            ptr = lambda a: a.ctypes.data
+            flags = _lib.HOST_MEMORY
+            stream = None
+            io.in_dtype = _dtype_code(ins["parity"])
+        io.out_dtype = _lib.F64 if output.dtype == np.float64 else _lib.F32
+        for k, t in ins.items():
+            setattr(io, k, ptr(t))
+            keep.append(t)
+        for k, t in outs.items():
+            setattr(io, {"msg": "msg", "syst": "syst_out", "parity": "parity_out", "state": "state_out"}[k], ptr(t))
+        _check(_L.fecl_so_decode(self._h, C.byref(io), n, flags, stream))
+        output._v.update(outs)
+        output._want = []
+        return output
+
+
+class Ldpc(Codec):
+    """fec::Ldpc -- src/Ldpc.h:59-108."""
+
+    class EncoderOptions:
+        def __init__(self, checkMatrix):
+            self._H = checkMatrix
+
+        def checkMatrix(self):
+            return self._H
+
+    class DecoderOptions:
+        """Ldpc::DecoderOptions -- src/detail/Ldpc.h:56-74 (iterations defaults to 50
+        here; the reference leaves it uninitialised)."""
+
+        def __init__(self):
+            self._alg = Approximate
+            self._it = 50
+            self._sf = {0: [1.0]}
+            self._precision = _lib.MSG_F32
+            self._fixed = False
+
+        def algorithm(self, a=None):
+            if a is None:
+                return self._alg
+            self._alg = int(a)
+            return self
+
+        def iterations(self, n=None):
+            if n is None:
+                return self._it
+            self._it = int(n)
+            return self
+
+        def scalingFactor(self, f=None):
+            if f is None:
+                return self._sf
+            self._sf = dict(f) if isinstance(f, dict) else {0: [float(f)]}
+            return self
+
+        def precision(self, p=None):
+            if p is None:
+                return self._precision
+            self._precision = int(p)
+            return self
+
+        def fixedIterations(self, on=None):
+            if on is None:
+                return self._fixed
+            self._fixed = bool(on)
+            return self
+
+    class PunctureOptions:
+        pass
+
+    class Gallager:
+        @staticmethod
+        def matrix(n, wc, wr, seed=0):
+            """Ldpc::Gallager::matrix -- src/Ldpc.cpp:77-102."""
+            rows, nnz = C.c_uint32(), C.c_uint64()
+            _check(_L.fecl_gallager_matrix(n, wc, wr, seed, C.byref(rows), C.byref(nnz), None, None))
+            ptr = np.zeros(rows.value + 1, np.uint32)
+            idx = np.zeros(nnz.value, np.uint32)
+            _check(_L.fecl_gallager_matrix(n, wc, wr, seed, C.byref(rows), C.byref(nnz), _ptr(ptr), _ptr(idx)))
+            return SparseBitMatrix(rows.value, n, ptr, idx)
+
+    class DvbS2:
+        @staticmethod
+        def matrix(n, rate):
+            """Standard DVB-S2 check matrix for n in {16200, 64800} (Ldpc::DvbS2::matrix,
+            src/DvbS2.cpp:1595-1645).  rate is a Fraction or one of the listed floats."""
+            fr = Fraction(rate).limit_denominator(16)
+            rows, cols, nnz = C.c_uint32(), C.c_uint32(), C.c_uint64()
+            _check(_L.fecl_dvbs2_matrix(n, fr.numerator, fr.denominator, C.byref(rows), C.byref(cols), C.byref(nnz), None, None))
+            ptr = np.zeros(rows.value + 1, np.uint32)
+            idx = np.zeros(nnz.value, np.uint32)
+            _check(_L.fecl_dvbs2_matrix(n, fr.numerator, fr.denominator, C.byref(rows), C.byref(cols), C.byref(nnz),
+                                        _ptr(ptr), _ptr(idx)))
+            return SparseBitMatrix(rows.value, cols.value, ptr, idx)
+
+    def __init__(self, encoder, decoder=None, workGroupSize=8):
+        H = encoder.checkMatrix() if isinstance(encoder, Ldpc.EncoderOptions) else encoder
+        decoder = decoder or Ldpc.DecoderOptions()
+        self._degrees = H.rowSizes()
+        opts, keep = self._options(decoder)
+        h = C.c_void_p()
+        _check(_L.fecl_ldpc_create(H.rows(), H.cols(), _ptr(H.row_ptr), _ptr(H.col_idx), C.byref(opts), C.byref(h)))
+        super().__init__(h.value)
+        self._decoder = decoder
+        self._work_group = workGroupSize
+
+    def _options(self, d):
+        """scalingMapToVector (src/detail/Ldpc.cpp:64-112): map {degree: [per-iteration]}
+        with key 0 as default -> table [iterations or 1][maxDegree-1]."""
+        deg = self._degrees
+        maxd = int(deg.max())
+        m = d.scalingFactor()
+        if 0 in m:
+            default = list(m[0])
+            if len(default) != 1 and len(default) != d.iterations():
+                raise ValueError("Wrong size for scaling factor")
+            vec = [[default[i]] * (maxd - 1) for i in range(len(default))]
+            for key, vals in m.items():
+                if 2 <= key and key - 2 < maxd - 1:
+                    if len(vals) != len(vec):
+                        raise ValueError("Wrong size for scaling factor")
+                    for j in range(len(vec)):
+                        vec[j][key - 2] = vals[j]
+        else:
+            length = max(len(v) for v in m.values())
+            if length != 1 and length != d.iterations():
+                raise ValueError("Wrong size for scaling factor")
+            vec = [[0.0] * (maxd - 1) for _ in range(length)]
+            for dg in deg:
+                if int(dg) not in m:
+                    raise ValueError("Scaling factor not defined and no default")
+                vals = m[int(dg)]
+                if len(vals) != length:
+                    raise ValueError("Wrong size for scaling factor")
+                for j in range(length):
+                    vec[j][int(dg) - 2] = vals[j]
+        table = np.ascontiguousarray(np.asarray(vec, dtype=np.float64))
+        o = _lib.fecl_ldpc_options()
+        o.algorithm = d.algorithm()
+        o.iterations = d.iterations()
+        o.scaling = table.ctypes.data_as(C.POINTER(C.c_double))
+        o.scaling_iterations = table.shape[0]
+        o.scaling_degrees = table.shape[1]
+        o.precision = d.precision()
+        o.fixed_iterations = 1 if d.fixedIterations() else 0
+        self._table = table
+        return o, table
+
+    def setDecoderOptions(self, decoder):
+        opts, keep = self._options(decoder)
+        _check(_L.fecl_ldpc_set_options(self._h, C.byref(opts)))
+        self._decoder = decoder
+
+    def getDecoderOptions(self):
+        return self._decoder
+
+    def checks(self):
+        """The transformed check matrix (detail::Ldpc::Structure::checks); its edge
+        order is the layout of the soft state."""
+        rows, cols, nnz = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        _check(_L.fecl_ldpc_checks(self._h, C.byref(rows), C.byref(cols), C.byref(nnz), None, None))
+        ptr = np.zeros(rows.value + 1, np.uint32)
+        idx = np.zeros(nnz.value, np.uint32)
+        _check(_L.fecl_ldpc_checks(self._h, C.byref(rows), C.byref(cols), C.byref(nnz), _ptr(ptr), _ptr(idx)))
+        return SparseBitMatrix(rows.value, cols.value, ptr, idx)
+
+
+class Turbo(Codec):
+    """fec::Turbo -- src/Turbo.h:55-116."""
+
+    class Lte3Gpp:
+        @staticmethod
+        def interleaver(length):
+            """Turbo::Lte3Gpp::interleaver -- src/Lte3Gpp.cpp:219-237."""
+            p = np.zeros(int(length), np.uint32)
+            _check(_L.fecl_lte_interleaver(int(length), _ptr(p)))
+            return p
+
+    class EncoderOptions:
+        """Turbo::EncoderOptions -- src/detail/Turbo.h:59-72."""
+
+        def __init__(self, trellis, interleaver):
+            self._trellis = list(trellis) if isinstance(trellis, (list, tuple)) else [trellis]
+            self._perm = [np.asarray(p, dtype=np.uint32) for p in interleaver]
+            self._term = [Trellis.Tail]
+
+        def interleaver(self, perms):
+            self._perm = [np.asarray(p, dtype=np.uint32) for p in perms]
+            return self
+
+        def termination(self, t):
+            self._term = list(t) if isinstance(t, (list, tuple)) else [t]
+            return self
+
+    class DecoderOptions:
+        """Turbo::DecoderOptions -- src/detail/Turbo.h:77-101."""
+
+        def __init__(self):
+            self._it, self._sched, self._alg, self._sf = 6, Serial, Linear, [[1.0]]
+            self._precision = _lib.MSG_F32
+
+        def iterations(self, n=None):
+            if n is None:
+                return self._it
+            self._it = int(n)
+            return self
+
+        def scheduling(self, s=None):
+            if s is None:
+                return self._sched
+            self._sched = int(s)
+            return self
+
+        def algorithm(self, a=None):
+            if a is None:
+                return self._alg
+            self._alg = int(a)
+            return self
+
+        def scalingFactor(self, f=None):
+            if f is None:
+                return self._sf
+            self._sf = [list(map(float, r)) for r in f] if isinstance(f, (list, tuple)) else [[float(f)]]
+            return self
+
+        def precision(self, p=None):
+            if p is None:
+                return self._precision
+            self._precision = int(p)
+            return self
+
+    def __init__(self, encoder, decoder=None, workGroupSize=8, lte_length=None):
+        decoder = decoder or Turbo.DecoderOptions()
+        opts, keep = self._options(decoder)
+        h = C.c_void_p()
+        if lte_length is not None:
+            _check(_L.fecl_turbo_create_lte(int(lte_length), C.byref(opts), C.byref(h)))
+        else:
+            tr = (_lib.fecl_trellis * len(encoder._trellis))(*[t._c() for t in encoder._trellis])
+            lens = _u32([p.size for p in encoder._perm])
+            data = _u32(np.concatenate(encoder._perm)) if sum(p.size for p in encoder._perm) else np.zeros(1, np.uint32)
+            term = np.ascontiguousarray(np.asarray(encoder._term, dtype=np.int32))
+            _check(_L.fecl_turbo_create(len(encoder._perm), tr, len(encoder._trellis), _ptr(data), _ptr(lens), _ptr(term),
+                                        term.size, C.byref(opts), C.byref(h)))
+        super().__init__(h.value)
+        self._decoder = decoder
+        self._work_group = workGroupSize
+
+    @classmethod
+    def lte(cls, K, decoder=None):
+        """The LTE turbo code of 3GPP TS 36.212 for block size K: RSC (13, 15) octal,
+        Tail, {identity, Lte3Gpp.interleaver(K)}."""
+        return cls(None, decoder, lte_length=K)
+
+    def _options(self, d):
+        sf = np.ascontiguousarray(np.asarray(d.scalingFactor(), dtype=np.float64))
+        if sf.ndim != 2:
+            raise ValueError("Wrong size for scaling factor")
+        o = _lib.fecl_turbo_options()
+        o.algorithm = d.algorithm()
+        o.iterations = d.iterations()
+        o.scheduling = d.scheduling()
+        o.scaling = sf.ctypes.data_as(C.POINTER(C.c_double))
+        o.scaling_rows, o.scaling_cols = sf.shape
+        o.precision = d.precision()
+        self._sf_table = sf
+        return o, sf
+
+    def setDecoderOptions(self, decoder):
+        opts, keep = self._options(decoder)
+        _check(_L.fecl_turbo_set_options(self._h, C.byref(opts)))
+        self._decoder = decoder
+
+    def getDecoderOptions(self):
+        return self._decoder

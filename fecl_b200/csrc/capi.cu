@@ -1,0 +1,719 @@
+// The C-ABI entry points declared in include/fecl_b200.h.
+//
+// Each codec owns its host description (LdpcCode / TurboCode), the device copy of
+// that description, a device workspace that grows to the largest batch seen, and a
+// stream for host-memory calls.  Calls on one codec are serialised by a mutex; a
+// device-memory call leaves an event behind that the next call on the codec waits
+// for before it reuses the workspace.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fecl_b200.h"
+#include "device/kernels.hpp"
+#include "host/codes.hpp"
+
+namespace {
+
+thread_local std::string g_error;
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] void fail(int code, const std::string& msg) { throw Error{code, msg}; }
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fail(e == cudaErrorMemoryAllocation ? FECL_ENOMEM : FECL_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return FECL_OK;
+  } catch (const Error& e) {
+    g_error = e.msg;
+    return e.code;
+  } catch (const std::invalid_argument& e) {
+    g_error = e.what();
+    return FECL_EINVAL;
+  } catch (const std::bad_alloc&) {
+    g_error = "host allocation failed";
+    return FECL_ENOMEM;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return FECL_EINVAL;
+  }
+}
+
+// A device allocation owned by a codec.
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() {
+    if (ptr) cudaFree(ptr);
+  }
+  void reserve(size_t n) {
+    if (n <= bytes) return;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    cuda_check(cudaMalloc(&ptr, n), "cudaMalloc");
+    bytes = n;
+  }
+  template <class T>
+  void upload(const std::vector<T>& v) {
+    reserve(std::max<size_t>(v.size() * sizeof(T), 16));
+    if (!v.empty()) cuda_check(cudaMemcpy(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(ptr);
+  }
+};
+
+// Carves aligned slices out of one workspace allocation.
+struct Carver {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  }
+};
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+size_t dsize(int dtype) {
+  switch (dtype) {
+    case FECL_F64: return 8;
+    case FECL_F32: return 4;
+    case FECL_F16: return 2;
+  }
+  fail(FECL_EINVAL, "Invalid element type");
+}
+
+}  // namespace
+
+struct fecl_codec_s {
+  int kind = 0;  // 0 LDPC, 1 turbo
+  int device = 0;
+  std::unique_ptr<fecl::LdpcCode> ldpc;
+  std::unique_ptr<fecl::TurboCode> turbo;
+  std::mutex mu;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  bool pending = false;
+  // device description
+  DeviceBuffer row_ptr, col_idx, col_ptr, col_edges, sf;
+  std::vector<std::unique_ptr<DeviceBuffer>> tables;
+  fecl::LdpcDeviceCode ldev;
+  fecl::TurboDeviceCode tdev;
+  // workspace
+  DeviceBuffer ws;
+
+  ~fecl_codec_s() {
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+    if (done) cudaEventDestroy(done);
+  }
+
+  uint64_t msg() const { return kind == 0 ? ldpc->msg_size() : turbo->msg_size(); }
+  uint64_t syst() const { return kind == 0 ? ldpc->syst_size() : turbo->syst_size(); }
+  uint64_t parity() const { return kind == 0 ? ldpc->parity_size() : turbo->parity_size(); }
+  uint64_t state() const { return kind == 0 ? ldpc->state_size() : turbo->state_size(); }
+
+  void init_runtime() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+      cudaGetLastError();
+      fail(FECL_ENODEV, "no CUDA device is visible");
+    }
+    cuda_check(cudaGetDevice(&device), "cudaGetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "cudaEventCreate");
+  }
+
+  void upload_ldpc() {
+    const fecl::Csr& H = ldpc->checks();
+    row_ptr.upload(H.row_ptr);
+    col_idx.upload(H.col_idx);
+    // per-bit edge lists in increasing edge order
+    std::vector<uint32_t> cp(H.cols + 1, 0), ce(H.nnz());
+    for (auto c : H.col_idx) cp[c + 1]++;
+    for (uint32_t b = 0; b < H.cols; ++b) cp[b + 1] += cp[b];
+    std::vector<uint32_t> fill(cp.begin(), cp.end() - 1);
+    for (uint64_t e = 0; e < H.nnz(); ++e) ce[fill[H.col_idx[e]]++] = uint32_t(e);
+    col_ptr.upload(cp);
+    col_edges.upload(ce);
+    ldev.M = int32_t(H.rows);
+    ldev.N = int32_t(H.cols);
+    ldev.E = int64_t(H.nnz());
+    ldev.msg = int32_t(ldpc->msg_size());
+    ldev.d_max = int32_t(ldpc->max_check_degree());
+    ldev.row_ptr = row_ptr.as<uint32_t>();
+    ldev.col_idx = col_idx.as<uint32_t>();
+    ldev.col_ptr = col_ptr.as<uint32_t>();
+    ldev.col_edges = col_edges.as<uint32_t>();
+    upload_ldpc_options();
+  }
+
+  void upload_ldpc_options() {
+    const auto& d = ldpc->decoder();
+    const int stride = int(ldpc->max_check_degree()) - 1;
+    std::vector<float> t;
+    for (auto& row : d.scaling)
+      for (int k = 0; k < stride; ++k) t.push_back(float(row[k]));
+    sf.upload(t);
+    ldev.sf = sf.as<float>();
+    ldev.n_sf = int32_t(d.scaling.size());
+    ldev.sf_stride = stride;
+    ldev.algorithm = d.algorithm;
+    ldev.iterations = int32_t(d.iterations);
+    ldev.fixed_iterations = d.fixed_iterations;
+  }
+
+  void upload_turbo() {
+    const auto& cs = turbo->constituents();
+    if (cs.size() > size_t(fecl::kMaxConstituents)) fail(FECL_EUNSUPPORTED, "too many constituents for the device decoder");
+    tables.clear();
+    tdev.n = int32_t(cs.size());
+    tdev.msg = int32_t(turbo->msg_size());
+    tdev.syst = int32_t(turbo->syst_size());
+    tdev.parity = int32_t(turbo->parity_size());
+    tdev.state = int32_t(turbo->state_size());
+    tdev.tail = int32_t(turbo->syst_tail_size());
+    tdev.max_steps = 0;
+    tdev.max_states = 0;
+    for (size_t j = 0; j < cs.size(); ++j) {
+      const auto& c = cs[j];
+      auto& k = tdev.c[j];
+      k.state_count = int32_t(c.trellis.state_count);
+      k.input_count = int32_t(c.trellis.input_count);
+      k.input_size = int32_t(c.trellis.input_size);
+      k.output_size = int32_t(c.trellis.output_size);
+      k.length = int32_t(c.length);
+      k.tail = int32_t(c.tail);
+      k.termination = c.termination;
+      k.msg_size = int32_t(c.msg_size());
+      k.syst_size = int32_t(c.syst_size());
+      k.syst_tail_size = int32_t(c.syst_tail_size());
+      k.parity_size = int32_t(c.parity_size());
+      for (auto* v : {&c.trellis.next_state, &c.trellis.output, &c.perm}) {
+        tables.emplace_back(new DeviceBuffer);
+        tables.back()->upload(*v);
+      }
+      k.next_state = tables[tables.size() - 3]->as<uint32_t>();
+      k.output = tables[tables.size() - 2]->as<uint32_t>();
+      k.perm = tables[tables.size() - 1]->as<uint32_t>();
+      tdev.max_steps = std::max(tdev.max_steps, int32_t(c.length + c.tail));
+      tdev.max_states = std::max(tdev.max_states, int32_t(c.trellis.state_count));
+    }
+    upload_turbo_options();
+  }
+
+  void upload_turbo_options() {
+    const auto& d = turbo->decoder();
+    std::vector<float> t;
+    for (size_t j = 0; j < turbo->constituents().size(); ++j)
+      for (uint32_t i = 0; i < std::max<uint32_t>(d.iterations, 1); ++i) t.push_back(float(turbo->scaling_factor(i, j)));
+    sf.upload(t);
+    tdev.sf = sf.as<float>();
+    tdev.algorithm = d.algorithm;
+    tdev.iterations = int32_t(d.iterations);
+    tdev.scheduling = d.scheduling;
+  }
+
+  bool on_device = false;
+  // Device resources are created at the first decode, so that host-side operations
+  // (encode, check, the transformed matrix) work without a GPU.
+  void ensure_device() {
+    if (on_device) return;
+    init_runtime();
+    if (kind == 0) upload_ldpc();
+    else upload_turbo();
+    on_device = true;
+  }
+
+  // Orders this call after the previous device-memory call on the codec.
+  void wait_previous(cudaStream_t s) {
+    if (pending) cuda_check(cudaStreamWaitEvent(s, done, 0), "cudaStreamWaitEvent");
+  }
+  void mark(cudaStream_t s) {
+    cuda_check(cudaEventRecord(done, s), "cudaEventRecord");
+    pending = true;
+  }
+};
+
+namespace {
+
+fecl::LdpcDecoderConfig ldpc_config(const fecl_ldpc_options* o, uint32_t max_degree) {
+  fecl::LdpcDecoderConfig cfg;
+  if (!o) return cfg;
+  cfg.algorithm = o->algorithm;
+  cfg.iterations = o->iterations;
+  if (o->iterations == 0) fail(FECL_EINVAL, "Invalid number of iterations");
+  cfg.precision = o->precision;
+  cfg.fixed_iterations = o->fixed_iterations;
+  if (o->scaling) {
+    if (o->scaling_iterations == 0 || o->scaling_degrees == 0) fail(FECL_EINVAL, "Wrong size for scaling factor");
+    cfg.scaling.assign(o->scaling_iterations, {});
+    for (uint32_t i = 0; i < o->scaling_iterations; ++i)
+      cfg.scaling[i].assign(o->scaling + size_t(i) * o->scaling_degrees,
+                            o->scaling + size_t(i + 1) * o->scaling_degrees);
+  }
+  (void)max_degree;
+  return cfg;
+}
+
+fecl::TurboDecoderConfig turbo_config(const fecl_turbo_options* o) {
+  fecl::TurboDecoderConfig cfg;
+  if (!o) return cfg;
+  cfg.algorithm = o->algorithm;
+  cfg.iterations = o->iterations;
+  cfg.scheduling = o->scheduling;
+  cfg.precision = o->precision;
+  if (o->scaling) {
+    if (o->scaling_rows == 0 || o->scaling_cols == 0) fail(FECL_EINVAL, "Wrong size for scaling factor");
+    cfg.scaling.assign(o->scaling_rows, {});
+    for (uint32_t r = 0; r < o->scaling_rows; ++r)
+      cfg.scaling[r].assign(o->scaling + size_t(r) * o->scaling_cols, o->scaling + size_t(r + 1) * o->scaling_cols);
+  }
+  return cfg;
+}
+
+fecl::Csr csr_in(uint32_t rows, uint32_t cols, const uint32_t* row_ptr, const uint32_t* col_idx) {
+  if (!row_ptr || !col_idx) fail(FECL_EINVAL, "null check matrix");
+  fecl::Csr H;
+  H.rows = rows;
+  H.cols = cols;
+  H.row_ptr.assign(row_ptr, row_ptr + rows + 1);
+  if (H.row_ptr[0] != 0) fail(FECL_EINVAL, "row_ptr must start at 0");
+  for (uint32_t r = 0; r < rows; ++r)
+    if (H.row_ptr[r + 1] < H.row_ptr[r]) fail(FECL_EINVAL, "row_ptr must be non-decreasing");
+  H.col_idx.assign(col_idx, col_idx + H.row_ptr[rows]);
+  return H;
+}
+
+void csr_out(const fecl::Csr& H, uint32_t* rows, uint32_t* cols, uint64_t* nnz, uint32_t* row_ptr, uint32_t* col_idx) {
+  if (rows) *rows = H.rows;
+  if (cols) *cols = H.cols;
+  if (nnz) *nnz = H.nnz();
+  if (row_ptr) {
+    std::memcpy(row_ptr, H.row_ptr.data(), H.row_ptr.size() * sizeof(uint32_t));
+    if (col_idx) std::memcpy(col_idx, H.col_idx.data(), H.col_idx.size() * sizeof(uint32_t));
+  }
+}
+
+fecl_codec_s* checked(fecl_codec_t c) {
+  if (!c) fail(FECL_EINVAL, "null codec");
+  return c;
+}
+
+// Runs a decode.  Host-memory calls stage buffers through the workspace on the
+// codec's stream and wait; device-memory calls launch on the caller's stream.
+void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard, int32_t* iters, bool soft,
+                int32_t flags, cudaStream_t user_stream) {
+  c->ensure_device();
+  DeviceGuard dg(c->device);
+  const bool host = (flags == FECL_HOST_MEMORY);
+  if (flags != FECL_HOST_MEMORY && flags != FECL_DEVICE_MEMORY) fail(FECL_EINVAL, "Invalid memory flag");
+  cudaStream_t s = host ? c->stream : user_stream;
+  const size_t isz = dsize(io->in_dtype);
+  const size_t osz = soft ? dsize(io->out_dtype) : 4;
+  const uint64_t P = c->parity(), S = c->syst(), M = c->msg(), X = c->state();
+
+  Carver cv;
+  size_t o_llr = 0, o_syst = 0, o_state = 0, o_hard = 0, o_iters = 0, o_msg = 0, o_so = 0, o_po = 0, o_sto = 0;
+  if (host) {
+    o_llr = cv.take(n * P * isz);
+    if (io->syst) o_syst = cv.take(n * S * isz);
+    if (io->state) o_state = cv.take(n * X * isz);
+    if (hard) o_hard = cv.take(n * M);
+    if (iters) o_iters = cv.take(n * 4);
+    if (io->msg) o_msg = cv.take(n * M * osz);
+    if (io->syst_out) o_so = cv.take(n * S * osz);
+    if (io->parity_out) o_po = cv.take(n * P * osz);
+    if (io->state_out) o_sto = cv.take(n * X * osz);
+  }
+  size_t o_s1 = 0, o_s2 = 0, o_s3 = 0, o_s4 = 0, o_s5 = 0;
+  if (c->kind == 0) {
+    o_s1 = cv.take(n * c->ldev.E * 4);
+    o_s2 = cv.take(n * P * 4);
+    o_s3 = cv.take(n * P * 4);
+  } else {
+    o_s1 = cv.take(n * P * 4);
+    o_s2 = cv.take(n * P * 4);
+    o_s3 = cv.take(n * X * 4);
+    o_s4 = cv.take(n * X * 4);
+    o_s5 = cv.take(n * uint64_t(c->tdev.max_steps) * c->tdev.max_states * 4);
+  }
+  c->wait_previous(s);
+  if (c->ws.bytes < cv.off) {
+    // the old workspace may still be read by earlier work on other streams
+    if (c->pending) cuda_check(cudaEventSynchronize(c->done), "cudaEventSynchronize");
+    c->ws.reserve(cv.off);
+  }
+  char* base = c->ws.as<char>();
+  auto dptr = [&](size_t off) -> void* { return base + off; };
+
+  const void* d_llr = io->parity;
+  const void* d_syst = io->syst;
+  const void* d_state = io->state;
+  uint8_t* d_hard = hard;
+  int32_t* d_iters = iters;
+  void *d_msg = io->msg, *d_so = io->syst_out, *d_po = io->parity_out, *d_sto = io->state_out;
+  if (host) {
+    d_llr = dptr(o_llr);
+    cuda_check(cudaMemcpyAsync(dptr(o_llr), io->parity, n * P * isz, cudaMemcpyHostToDevice, s), "copy in");
+    if (io->syst) {
+      d_syst = dptr(o_syst);
+      cuda_check(cudaMemcpyAsync(dptr(o_syst), io->syst, n * S * isz, cudaMemcpyHostToDevice, s), "copy in");
+    }
+    if (io->state) {
+      d_state = dptr(o_state);
+      cuda_check(cudaMemcpyAsync(dptr(o_state), io->state, n * X * isz, cudaMemcpyHostToDevice, s), "copy in");
+    }
+    if (hard) d_hard = static_cast<uint8_t*>(dptr(o_hard));
+    if (iters) d_iters = static_cast<int32_t*>(dptr(o_iters));
+    if (io->msg) d_msg = dptr(o_msg);
+    if (io->syst_out) d_so = dptr(o_so);
+    if (io->parity_out) d_po = dptr(o_po);
+    if (io->state_out) d_sto = dptr(o_sto);
+  }
+
+  cudaError_t e;
+  if (c->kind == 0) {
+    fecl::LdpcRun r;
+    r.nframes = int64_t(n);
+    r.llr = d_llr;
+    r.llr_dtype = io->in_dtype;
+    r.syst_in = d_syst;
+    r.state_in = d_state;
+    r.hard = d_hard;
+    r.iters = d_iters;
+    r.msg_out = d_msg;
+    r.syst_out = d_so;
+    r.parity_out = d_po;
+    r.state_out = d_sto;
+    r.out_dtype = io->out_dtype;
+    r.c2v = static_cast<float*>(dptr(o_s1));
+    r.app = static_cast<float*>(dptr(o_s2));
+    r.chan = static_cast<float*>(dptr(o_s3));
+    e = fecl::launch_ldpc_flood(c->ldev, r, s);
+  } else {
+    fecl::TurboRun r;
+    r.nframes = int64_t(n);
+    r.soft = soft ? 1 : 0;
+    r.llr = d_llr;
+    r.llr_dtype = io->in_dtype;
+    r.syst_in = d_syst;
+    r.state_in = d_state;
+    r.hard = d_hard;
+    r.iters = d_iters;
+    r.msg_out = d_msg;
+    r.syst_out = d_so;
+    r.parity_out = d_po;
+    r.state_out = d_sto;
+    r.out_dtype = io->out_dtype;
+    r.parity_in = static_cast<float*>(dptr(o_s1));
+    r.parity_buf = static_cast<float*>(dptr(o_s2));
+    r.ext = static_cast<float*>(dptr(o_s3));
+    r.ext_buf = static_cast<float*>(dptr(o_s4));
+    r.alpha = static_cast<float*>(dptr(o_s5));
+    e = fecl::launch_turbo_generic(c->tdev, r, s);
+  }
+  if (e == cudaErrorInvalidValue) fail(FECL_EUNSUPPORTED, "code shape not supported by the device decoder");
+  cuda_check(e, "kernel launch");
+
+  if (host) {
+    if (hard) cuda_check(cudaMemcpyAsync(hard, d_hard, n * M, cudaMemcpyDeviceToHost, s), "copy out");
+    if (iters) cuda_check(cudaMemcpyAsync(iters, d_iters, n * 4, cudaMemcpyDeviceToHost, s), "copy out");
+    if (io->msg) cuda_check(cudaMemcpyAsync(io->msg, d_msg, n * M * osz, cudaMemcpyDeviceToHost, s), "copy out");
+    if (io->syst_out) cuda_check(cudaMemcpyAsync(io->syst_out, d_so, n * S * osz, cudaMemcpyDeviceToHost, s), "copy out");
+    if (io->parity_out)
+      cuda_check(cudaMemcpyAsync(io->parity_out, d_po, n * P * osz, cudaMemcpyDeviceToHost, s), "copy out");
+    if (io->state_out)
+      cuda_check(cudaMemcpyAsync(io->state_out, d_sto, n * X * osz, cudaMemcpyDeviceToHost, s), "copy out");
+    cuda_check(cudaStreamSynchronize(s), "decode");
+    c->pending = false;
+  } else {
+    c->mark(s);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fecl_version(void) { return "fecl_b200 0.1 (sm_100a)"; }
+
+const char* fecl_last_error(void) { return g_error.c_str(); }
+
+const char* fecl_strerror(int status) {
+  switch (status) {
+    case FECL_OK: return "success";
+    case FECL_EINVAL: return "invalid argument";
+    case FECL_ECUDA: return "CUDA error";
+    case FECL_ENOMEM: return "out of memory";
+    case FECL_ETIMEDOUT: return "device wait timed out";
+    case FECL_EUNSUPPORTED: return "unsupported on the device";
+    case FECL_ENODEV: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+int fecl_dvbs2_matrix(uint32_t n, uint32_t rate_num, uint32_t rate_den, uint32_t* rows, uint32_t* cols, uint64_t* nnz,
+                      uint32_t* row_ptr, uint32_t* col_idx) {
+  return guarded([&] {
+    if (rate_den == 0) fail(FECL_EINVAL, "Invalid rate");
+    csr_out(fecl::dvbs2_matrix(n, rate_num, rate_den), rows, cols, nnz, row_ptr, col_idx);
+  });
+}
+
+int fecl_gallager_matrix(uint32_t n, uint32_t wc, uint32_t wr, uint64_t seed, uint32_t* rows, uint64_t* nnz,
+                         uint32_t* row_ptr, uint32_t* col_idx) {
+  return guarded([&] { csr_out(fecl::gallager_matrix(n, wc, wr, seed), rows, nullptr, nnz, row_ptr, col_idx); });
+}
+
+int fecl_ldpc_create(uint32_t rows, uint32_t cols, const uint32_t* row_ptr, const uint32_t* col_idx,
+                     const fecl_ldpc_options* options, fecl_codec_t* out) {
+  return guarded([&] {
+    if (!out) fail(FECL_EINVAL, "null output");
+    std::unique_ptr<fecl_codec_s> c(new fecl_codec_s);
+    c->kind = 0;
+    c->ldpc.reset(new fecl::LdpcCode(csr_in(rows, cols, row_ptr, col_idx)));
+    if (options) c->ldpc->set_decoder(ldpc_config(options, c->ldpc->max_check_degree()));
+    *out = c.release();
+  });
+}
+
+int fecl_ldpc_set_options(fecl_codec_t codec, const fecl_ldpc_options* options) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 0) fail(FECL_EINVAL, "not an LDPC codec");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->ldpc->set_decoder(ldpc_config(options, c->ldpc->max_check_degree()));
+    if (c->on_device) {
+      DeviceGuard dg(c->device);
+      if (c->pending) cuda_check(cudaEventSynchronize(c->done), "cudaEventSynchronize");
+      c->upload_ldpc_options();
+    }
+  });
+}
+
+int fecl_ldpc_checks(fecl_codec_t codec, uint32_t* rows, uint32_t* cols, uint64_t* nnz, uint32_t* row_ptr,
+                     uint32_t* col_idx) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 0) fail(FECL_EINVAL, "not an LDPC codec");
+    csr_out(c->ldpc->checks(), rows, cols, nnz, row_ptr, col_idx);
+  });
+}
+
+int fecl_trellis_build(uint32_t ninputs, const uint32_t* constraint_lengths, uint32_t noutputs,
+                       const uint64_t* generators, const uint64_t* feedback, uint32_t* state_count,
+                       uint32_t* input_count, uint32_t* output_size, uint32_t* next_state, uint32_t* output) {
+  return guarded([&] {
+    if (ninputs == 0 || noutputs == 0 || !constraint_lengths || !generators) fail(FECL_EINVAL, "Invalid number of generators");
+    std::vector<uint32_t> cl(constraint_lengths, constraint_lengths + ninputs);
+    for (auto v : cl)
+      if (v < 2) fail(FECL_EINVAL, "Invalid constraint length");
+    std::vector<std::vector<uint64_t>> gen(ninputs);
+    for (uint32_t i = 0; i < ninputs; ++i) gen[i].assign(generators + size_t(i) * noutputs, generators + size_t(i + 1) * noutputs);
+    std::vector<uint64_t> fb;
+    if (feedback) fb.assign(feedback, feedback + ninputs);
+    auto t = fecl::Trellis::from_generators(cl, gen, fb);
+    if (state_count) *state_count = t.state_count;
+    if (input_count) *input_count = t.input_count;
+    if (output_size) *output_size = t.output_size;
+    if (next_state) std::memcpy(next_state, t.next_state.data(), t.next_state.size() * 4);
+    if (output) std::memcpy(output, t.output.data(), t.output.size() * 4);
+  });
+}
+
+int fecl_turbo_create(uint32_t n_constituents, const fecl_trellis* trellis, uint32_t n_trellis, const uint32_t* perm_data,
+                      const uint32_t* perm_len, const int32_t* termination, uint32_t n_termination,
+                      const fecl_turbo_options* options, fecl_codec_t* out) {
+  return guarded([&] {
+    if (!out) fail(FECL_EINVAL, "null output");
+    if (!trellis || n_trellis == 0) fail(FECL_EINVAL, "Trellis and Permutation count don't match");
+    std::vector<fecl::Trellis> tr;
+    for (uint32_t i = 0; i < n_trellis; ++i)
+      tr.push_back(fecl::Trellis::from_tables(trellis[i].state_count, trellis[i].input_count, trellis[i].output_size,
+                                              trellis[i].next_state, trellis[i].output));
+    std::vector<std::vector<uint32_t>> perms(n_constituents);
+    size_t off = 0;
+    for (uint32_t i = 0; i < n_constituents; ++i) {
+      const uint32_t len = perm_len ? perm_len[i] : 0;
+      if (len && !perm_data) fail(FECL_EINVAL, "null interleaver data");
+      perms[i].assign(perm_data + off, perm_data + off + len);
+      off += len;
+    }
+    std::vector<int> term;
+    if (termination && n_termination)
+      term.assign(termination, termination + n_termination);
+    else
+      term.push_back(FECL_TAIL);
+    std::unique_ptr<fecl_codec_s> c(new fecl_codec_s);
+    c->kind = 1;
+    c->turbo.reset(new fecl::TurboCode(tr, perms, term));
+    if (options) c->turbo->set_decoder(turbo_config(options));
+    *out = c.release();
+  });
+}
+
+int fecl_lte_interleaver(uint32_t K, uint32_t* perm) {
+  return guarded([&] {
+    auto p = fecl::lte_interleaver(K);
+    if (perm) std::memcpy(perm, p.data(), p.size() * 4);
+  });
+}
+
+int fecl_turbo_create_lte(uint32_t K, const fecl_turbo_options* options, fecl_codec_t* out) {
+  return guarded([&] {
+    if (!out) fail(FECL_EINVAL, "null output");
+    auto t = fecl::lte_trellis();
+    std::vector<std::vector<uint32_t>> perms{{}, fecl::lte_interleaver(K)};
+    std::unique_ptr<fecl_codec_s> c(new fecl_codec_s);
+    c->kind = 1;
+    c->turbo.reset(new fecl::TurboCode({t}, perms, {FECL_TAIL}));
+    if (options) c->turbo->set_decoder(turbo_config(options));
+    *out = c.release();
+  });
+}
+
+int fecl_turbo_set_options(fecl_codec_t codec, const fecl_turbo_options* options) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 1) fail(FECL_EINVAL, "not a turbo codec");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->turbo->set_decoder(turbo_config(options));
+    if (c->on_device) {
+      DeviceGuard dg(c->device);
+      if (c->pending) cuda_check(cudaEventSynchronize(c->done), "cudaEventSynchronize");
+      c->upload_turbo_options();
+    }
+  });
+}
+
+int fecl_codec_sizes(fecl_codec_t codec, fecl_sizes* sizes) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (!sizes) fail(FECL_EINVAL, "null output");
+    sizes->msg = c->msg();
+    sizes->syst = c->syst();
+    sizes->parity = c->parity();
+    sizes->state = c->state();
+  });
+}
+
+int fecl_encode(fecl_codec_t codec, const uint8_t* msg, uint64_t nframes, uint8_t* parity, int32_t flags, void* stream) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (!msg || !parity) fail(FECL_EINVAL, "null buffer");
+    const uint64_t M = c->msg(), P = c->parity();
+    std::vector<uint8_t> hm, hp;
+    const uint8_t* m = msg;
+    uint8_t* p = parity;
+    if (flags == FECL_DEVICE_MEMORY) {
+      DeviceGuard dg(c->device);
+      hm.resize(nframes * M);
+      hp.resize(nframes * P);
+      cuda_check(cudaMemcpyAsync(hm.data(), msg, hm.size(), cudaMemcpyDeviceToHost, (cudaStream_t)stream), "copy");
+      cuda_check(cudaStreamSynchronize((cudaStream_t)stream), "copy");
+      m = hm.data();
+      p = hp.data();
+    } else if (flags != FECL_HOST_MEMORY) {
+      fail(FECL_EINVAL, "Invalid memory flag");
+    }
+    for (uint64_t f = 0; f < nframes; ++f) {
+      if (c->kind == 0) c->ldpc->encode(m + f * M, p + f * P);
+      else c->turbo->encode(m + f * M, p + f * P);
+    }
+    if (flags == FECL_DEVICE_MEMORY) {
+      DeviceGuard dg(c->device);
+      cuda_check(cudaMemcpyAsync(parity, hp.data(), hp.size(), cudaMemcpyHostToDevice, (cudaStream_t)stream), "copy");
+      cuda_check(cudaStreamSynchronize((cudaStream_t)stream), "copy");
+    }
+  });
+}
+
+int fecl_check(fecl_codec_t codec, const uint8_t* parity, uint64_t nframes, int32_t* ok) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (!parity || !ok) fail(FECL_EINVAL, "null buffer");
+    const uint64_t P = c->parity();
+    int32_t r = 1;
+    for (uint64_t f = 0; f < nframes && r; ++f) r = (c->kind == 0 ? c->ldpc->check(parity + f * P) : c->turbo->check(parity + f * P)) ? 1 : 0;
+    *ok = r;
+  });
+}
+
+int fecl_decode(fecl_codec_t codec, const void* llr, int32_t llr_dtype, uint64_t nframes, uint8_t* msg, int32_t* iterations,
+                int32_t flags, void* stream) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (!llr || !msg) fail(FECL_EINVAL, "null buffer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    fecl_so_io io{};
+    io.parity = llr;
+    io.in_dtype = llr_dtype;
+    io.out_dtype = FECL_F32;
+    if (nframes == 0) return;
+    run_decode(c, &io, nframes, msg, iterations, false, flags, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fecl_so_decode(fecl_codec_t codec, const fecl_so_io* io, uint64_t nframes, int32_t flags, void* stream) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (!io) fail(FECL_EINVAL, "null io");
+    if (!io->parity) fail(FECL_EINVAL, "Input must contains parity");
+    if (io->out_dtype != FECL_F64 && io->out_dtype != FECL_F32) fail(FECL_EINVAL, "Invalid output element type");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (nframes == 0) return;
+    run_decode(c, io, nframes, nullptr, nullptr, true, flags, static_cast<cudaStream_t>(stream));
+  });
+}
+
+void fecl_destroy(fecl_codec_t codec) {
+  if (!codec) return;
+  if (!codec->on_device) {
+    delete codec;
+    return;
+  }
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(codec->device);
+  delete codec;
+  if (prev >= 0) cudaSetDevice(prev);
+}
+
+}  // extern "C"

@@ -1,0 +1,44 @@
+// Device-side helpers shared by the decoder kernels.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fecl {
+
+// Element types of caller buffers (FECL_F64 / FECL_F32 / FECL_F16).
+enum DType : int { kF64 = 0, kF32 = 1, kF16 = 2 };
+
+__device__ __forceinline__ float load_llr(const void* p, int dtype, size_t i) {
+  switch (dtype) {
+    case kF64: return float(static_cast<const double*>(p)[i]);
+    case kF16: return __half2float(static_cast<const __half*>(p)[i]);
+    default: return static_cast<const float*>(p)[i];
+  }
+}
+
+__device__ __forceinline__ void store_llr(void* p, int dtype, size_t i, float v) {
+  switch (dtype) {
+    case kF64: static_cast<double*>(p)[i] = double(v); break;
+    case kF16: static_cast<__half*>(p)[i] = __float2half_rn(v); break;
+    default: static_cast<float*>(p)[i] = v; break;
+  }
+}
+
+inline size_t dtype_size(int dtype) { return dtype == kF64 ? 8 : (dtype == kF16 ? 2 : 4); }
+
+// The reference's piecewise-linear log(1 + exp(-x)) (src/detail/LinearTable.h:56-81):
+// eight samples at x = i/2, linear in between, zero from x >= 3.5.
+struct LinearLut {
+  float y[8];
+};
+
+__device__ __forceinline__ float lut_log1pexpm(const LinearLut& t, float x) {
+  x *= 2.0f;
+  if (x >= 7.0f) return 0.0f;
+  const int i = int(x);
+  return (t.y[i + 1] - t.y[i]) * (x - float(i)) + t.y[i];
+}
+
+}  // namespace fecl

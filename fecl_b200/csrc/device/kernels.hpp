@@ -1,0 +1,95 @@
+// Host-callable launchers of the decoder kernels.  Plain structs of device
+// pointers and sizes; no CUDA types beyond cudaStream_t/cudaError_t.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fecl {
+
+// ---- LDPC ----------------------------------------------------------------
+
+// A check matrix laid out for the device: CSR by check (the edge order of the
+// soft state), plus for every bit the ids of its edges in increasing order.
+struct LdpcDeviceCode {
+  int32_t M = 0, N = 0, msg = 0, d_max = 0;
+  int64_t E = 0;
+  const uint32_t* row_ptr = nullptr;    // [M+1]
+  const uint32_t* col_idx = nullptr;    // [E]
+  const uint32_t* col_ptr = nullptr;    // [N+1]
+  const uint32_t* col_edges = nullptr;  // [E]
+  const float* sf = nullptr;            // [n_sf][sf_stride], entry [i][d-2]
+  int32_t n_sf = 1, sf_stride = 1;
+  int32_t algorithm = 2;
+  int32_t iterations = 1;
+  int32_t fixed_iterations = 0;
+};
+
+struct LdpcRun {
+  int64_t nframes = 0;
+  const void* llr = nullptr;  // [nframes][N]
+  int32_t llr_dtype = 1;
+  const void* syst_in = nullptr;   // [nframes][msg] (soft decode only)
+  const void* state_in = nullptr;  // [nframes][E]
+  uint8_t* hard = nullptr;         // [nframes][msg]
+  int32_t* iters = nullptr;        // [nframes]
+  void* msg_out = nullptr;         // [nframes][msg]
+  void* syst_out = nullptr;        // [nframes][msg]
+  void* parity_out = nullptr;      // [nframes][N]
+  void* state_out = nullptr;       // [nframes][E]
+  int32_t out_dtype = 1;
+  // scratch, FP32
+  float* c2v = nullptr;   // [nframes][E]
+  float* app = nullptr;   // [nframes][N]
+  float* chan = nullptr;  // [nframes][N]
+};
+
+cudaError_t launch_ldpc_flood(const LdpcDeviceCode& code, const LdpcRun& run, cudaStream_t stream);
+
+// ---- Turbo ---------------------------------------------------------------
+
+constexpr int kMaxConstituents = 8;
+
+struct TurboDeviceConstituent {
+  int32_t state_count, input_count, input_size, output_size;
+  int32_t length, tail, termination;
+  int32_t msg_size, syst_size, syst_tail_size, parity_size;
+  const uint32_t* next_state;  // [state_count * input_count]
+  const uint32_t* output;
+  const uint32_t* perm;        // [msg_size]
+};
+
+struct TurboDeviceCode {
+  int32_t n = 0;
+  int32_t msg = 0, syst = 0, parity = 0, state = 0, tail = 0;
+  int32_t max_steps = 0, max_states = 0;
+  TurboDeviceConstituent c[kMaxConstituents];
+  const float* sf = nullptr;  // [n][iterations] resolved scaling
+  int32_t algorithm = 1, iterations = 6, scheduling = 0;
+};
+
+struct TurboRun {
+  int64_t nframes = 0;
+  int32_t soft = 0;  // 1 for soDecode (scaling 1.0, outputs below)
+  const void* llr = nullptr;  // [nframes][parity]
+  int32_t llr_dtype = 1;
+  const void* syst_in = nullptr;
+  const void* state_in = nullptr;
+  uint8_t* hard = nullptr;
+  int32_t* iters = nullptr;
+  void* msg_out = nullptr;
+  void* syst_out = nullptr;
+  void* parity_out = nullptr;
+  void* state_out = nullptr;
+  int32_t out_dtype = 1;
+  // scratch, FP32, per frame
+  float* parity_in = nullptr;   // [nframes][parity]
+  float* parity_buf = nullptr;  // [nframes][parity]
+  float* ext = nullptr;         // [nframes][state]
+  float* ext_buf = nullptr;     // [nframes][state]
+  float* alpha = nullptr;       // [nframes][max_steps * max_states]
+};
+
+cudaError_t launch_turbo_generic(const TurboDeviceCode& code, const TurboRun& run, cudaStream_t stream);
+
+}  // namespace fecl

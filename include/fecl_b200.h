@@ -1,0 +1,219 @@
+/*
+ * fecl_b200 -- B200-native batched soft-decision decoding for FeCl codes.
+ *
+ * This is the C-ABI seam under FeCl's decode path.  In the reference the seam is
+ * the pair of protected virtuals every code family overrides,
+ *     Codec::decodeBlocks   (src/Codec.h:105; overridden in src/Ldpc.h:102, src/Turbo.h:110)
+ *     Codec::soDecodeBlocks (src/Codec.h:115; overridden in src/Ldpc.h:103, src/Turbo.h:111)
+ * reached from the public templates Codec::decode / soDecode / encode / check
+ * (src/Codec.h:68-82, 137-307) and from the Matlab function table
+ * (wrap/wrap.h:51-253).  Every function below takes plain pointers and sizes;
+ * no CUDA or C++ type crosses it except an opaque `void* stream` (a cudaStream_t).
+ *
+ * Conventions kept from the reference:
+ *   - L-values are L = ln p(x=1)/p(x=0): a positive value favours bit 1
+ *     (src/Codec.h:203-205).
+ *   - Buffers are frame-major: [nframes][paritySize] in, [nframes][msgSize] out,
+ *     the soft-output layouts of src/Ldpc.h:45-57 and src/Turbo.h:36-53.
+ *   - LDPC hard decisions use APP >= 0 -> 1 (src/detail/BpDecoder/BpDecoderImpl.cpp:68),
+ *     turbo hard decisions use APP > 0 -> 1 (src/detail/TurboDecoder/TurboDecoderImpl.cpp:70).
+ *   - Size mismatches and invalid options, which the reference reports by throwing
+ *     std::invalid_argument, return FECL_EINVAL with the reference's message in
+ *     fecl_last_error().
+ *
+ * Memory: with FECL_HOST_MEMORY every pointer is host memory and the call returns
+ * when the results are written.  With FECL_DEVICE_MEMORY every pointer is device
+ * memory of the current device and the call is asynchronous on `stream`.
+ */
+#ifndef FECL_B200_H
+#define FECL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------- */
+#define FECL_OK 0
+#define FECL_EINVAL (-1)       /* bad size or option (std::invalid_argument in the reference) */
+#define FECL_ECUDA (-2)        /* a CUDA runtime call failed */
+#define FECL_ENOMEM (-3)       /* device or host allocation failed */
+#define FECL_ETIMEDOUT (-4)    /* a bounded device-side wait gave up */
+#define FECL_EUNSUPPORTED (-5) /* option combination not implemented on the device */
+#define FECL_ENODEV (-6)       /* no CUDA device visible */
+
+/* ---- enums (values follow the reference's enums) --------------------------- */
+/* DecoderAlgorithm, src/DecoderAlgorithm.h:30-34 */
+#define FECL_EXACT 0
+#define FECL_LINEAR 1
+#define FECL_APPROXIMATE 2
+/* SchedulingType, src/SchedulingType.h:32-39 */
+#define FECL_SERIAL 0
+#define FECL_PARALLEL 1
+#define FECL_CUSTOM 2
+/* Trellis::Termination, src/Trellis.h */
+#define FECL_TAIL 0
+#define FECL_TRUNCATE 1
+/* element types of L-value buffers */
+#define FECL_F64 0
+#define FECL_F32 1
+#define FECL_F16 2
+/* precision of the decoder's internal messages (an extension; FP32 is the reference-parity mode) */
+#define FECL_MSG_F32 0
+#define FECL_MSG_F16 1
+#define FECL_MSG_I8 2
+/* memory flags */
+#define FECL_HOST_MEMORY 0
+#define FECL_DEVICE_MEMORY 1
+
+typedef struct fecl_codec_s* fecl_codec_t;
+
+typedef struct {
+  uint64_t msg;    /* Codec::msgSize    (src/Codec.h:60) */
+  uint64_t syst;   /* Codec::systSize   (src/Codec.h:61) */
+  uint64_t parity; /* Codec::paritySize (src/Codec.h:62) */
+  uint64_t state;  /* Codec::stateSize  (src/Codec.h:63) */
+} fecl_sizes;
+
+/* ---- LDPC ------------------------------------------------------------------ */
+
+/* Ldpc::DecoderOptions, src/detail/Ldpc.h:56-74. */
+typedef struct {
+  int32_t algorithm;   /* FECL_EXACT / FECL_LINEAR / FECL_APPROXIMATE */
+  uint32_t iterations; /* maximum iterations; the syndrome stop of
+                          src/detail/BpDecoder/BpDecoderImpl.cpp:49-61 applies */
+  /* Scaling of check-node outputs, row-major [scaling_iterations][scaling_degrees]:
+   * entry [i][d-2] scales rows of degree d at iteration i (i taken modulo
+   * scaling_iterations), as Ldpc::Structure::scalingFactor (src/detail/Ldpc.cpp:134-138).
+   * NULL means 1.0 everywhere. */
+  const double* scaling;
+  uint32_t scaling_iterations;
+  uint32_t scaling_degrees;
+  int32_t precision;  /* FECL_MSG_F32 (reference parity) / FECL_MSG_F16 / FECL_MSG_I8 */
+  int32_t fixed_iterations; /* 0: reference syndrome stop; 1: always run `iterations` (extension) */
+} fecl_ldpc_options;
+
+/* fec::Ldpc(EncoderOptions(H), DecoderOptions) -- src/Ldpc.h:83, src/detail/Ldpc.cpp:34-55.
+ * H is given in CSR form (rows = checks); the constructor transforms it for
+ * encoding exactly as src/detail/Ldpc.cpp:216-331 does, which may reorder rows
+ * and permute columns; fecl_ldpc_checks returns the transformed matrix. */
+int fecl_ldpc_create(uint32_t rows, uint32_t cols, const uint32_t* row_ptr, const uint32_t* col_idx,
+                     const fecl_ldpc_options* options, fecl_codec_t* out);
+
+/* Ldpc::setDecoderOptions -- src/Ldpc.h:91. */
+int fecl_ldpc_set_options(fecl_codec_t codec, const fecl_ldpc_options* options);
+
+/* The transformed check matrix the decoder iterates over (detail::Ldpc::Structure::checks,
+ * src/detail/Ldpc.h:110).  Its edge order is the layout of the LDPC soft state.
+ * Call with row_ptr == NULL to obtain the sizes. */
+int fecl_ldpc_checks(fecl_codec_t codec, uint32_t* rows, uint32_t* cols, uint64_t* nnz, uint32_t* row_ptr,
+                     uint32_t* col_idx);
+
+/* Standard DVB-S2 parity-check matrix for n in {16200, 64800} and rate num/den
+ * (Ldpc::DvbS2::matrix, src/DvbS2.cpp:1595-1645).  Built to ETSI EN 302 307 from the
+ * same address tables; the reference builder is only correct for (64800, 1/2), where
+ * the two agree edge for edge.  Call with row_ptr == NULL to obtain the sizes. */
+int fecl_dvbs2_matrix(uint32_t n, uint32_t rate_num, uint32_t rate_den, uint32_t* rows, uint32_t* cols,
+                      uint64_t* nnz, uint32_t* row_ptr, uint32_t* col_idx);
+
+/* Ldpc::Gallager::matrix -- src/Ldpc.cpp:77-102 (same generator and draws). */
+int fecl_gallager_matrix(uint32_t n, uint32_t wc, uint32_t wr, uint64_t seed, uint32_t* rows, uint64_t* nnz,
+                         uint32_t* row_ptr, uint32_t* col_idx);
+
+/* ---- Turbo ----------------------------------------------------------------- */
+
+/* A trellis as next-state / output tables indexed [state * input_count + input]
+ * (src/Trellis.h:131-172). */
+typedef struct {
+  uint32_t state_count;
+  uint32_t input_count;  /* 2^inputSize */
+  uint32_t output_size;  /* output bits per branch */
+  const uint32_t* next_state;
+  const uint32_t* output;
+} fecl_trellis;
+
+/* Trellis(constraintLengths, generator, feedback) -- src/Trellis.cpp:76-143.
+ * generators[i * noutputs + k] is the generator of input i, output k; feedback may be NULL.
+ * Writes state_count * input_count entries to next_state/output when they are non-NULL. */
+int fecl_trellis_build(uint32_t ninputs, const uint32_t* constraint_lengths, uint32_t noutputs,
+                       const uint64_t* generators, const uint64_t* feedback, uint32_t* state_count,
+                       uint32_t* input_count, uint32_t* output_size, uint32_t* next_state, uint32_t* output);
+
+/* Turbo::DecoderOptions -- src/detail/Turbo.h:77-101. */
+typedef struct {
+  int32_t algorithm;   /* default FECL_LINEAR in the reference */
+  uint32_t iterations; /* default 6 */
+  int32_t scheduling;  /* FECL_SERIAL / FECL_PARALLEL */
+  /* scaling[row][col], rows = 1 or constituent count, cols = 1 or iterations
+   * (Turbo::Structure::scalingFactor, src/detail/Turbo.cpp:148-153). NULL = 1.0. */
+  const double* scaling;
+  uint32_t scaling_rows;
+  uint32_t scaling_cols;
+  int32_t precision; /* FECL_MSG_F32 (reference parity) / FECL_MSG_F16 */
+} fecl_turbo_options;
+
+/* fec::Turbo(EncoderOptions(trellis, interleavers).termination(t), DecoderOptions)
+ * -- src/Turbo.h:100, src/detail/Turbo.cpp:45-103.  n_trellis and n_termination are 1
+ * or n_constituents.  perm_len[i] == 0 means the identity on the message. */
+int fecl_turbo_create(uint32_t n_constituents, const fecl_trellis* trellis, uint32_t n_trellis,
+                      const uint32_t* perm_data, const uint32_t* perm_len, const int32_t* termination,
+                      uint32_t n_termination, const fecl_turbo_options* options, fecl_codec_t* out);
+
+/* The LTE turbo code of 3GPP TS 36.212: RSC Trellis({4},{{015}},{013}), Tail, and
+ * {identity, Turbo::Lte3Gpp::interleaver(K)} (src/Lte3Gpp.cpp:219-237). */
+int fecl_turbo_create_lte(uint32_t K, const fecl_turbo_options* options, fecl_codec_t* out);
+
+/* Turbo::Lte3Gpp::interleaver -- perm[i] = (f1*i + f2*i^2) mod K. */
+int fecl_lte_interleaver(uint32_t K, uint32_t* perm);
+
+/* Turbo::setDecoderOptions -- src/Turbo.h:105. */
+int fecl_turbo_set_options(fecl_codec_t codec, const fecl_turbo_options* options);
+
+/* ---- every codec ----------------------------------------------------------- */
+
+int fecl_codec_sizes(fecl_codec_t codec, fecl_sizes* sizes);
+
+/* Codec::encode -- src/Codec.h:171-198.  Bits are one byte each (0/1). */
+int fecl_encode(fecl_codec_t codec, const uint8_t* msg, uint64_t nframes, uint8_t* parity, int32_t flags,
+                void* stream);
+
+/* Codec::check -- src/Codec.h:137-145; *ok = 1 when every frame is a codeword. */
+int fecl_check(fecl_codec_t codec, const uint8_t* parity, uint64_t nframes, int32_t* ok);
+
+/* Codec::decode -- src/Codec.h:210-238.  llr: [nframes][paritySize] of llr_dtype;
+ * msg: [nframes][msgSize] bytes 0/1.  iterations (nullable): per frame, the number
+ * of iterations the decoder ran (LDPC: check-node updates; turbo: iterations). */
+int fecl_decode(fecl_codec_t codec, const void* llr, int32_t llr_dtype, uint64_t nframes, uint8_t* msg,
+                int32_t* iterations, int32_t flags, void* stream);
+
+/* Codec::soDecode -- src/Codec.h:249-307.  Every pointer but `parity` may be NULL. */
+typedef struct {
+  const void* parity; /* [nframes][paritySize], required */
+  const void* syst;   /* [nframes][systSize] a-priori on the systematic bits */
+  const void* state;  /* [nframes][stateSize] decoder state to resume from */
+  int32_t in_dtype;   /* element type of the three inputs */
+  void* msg;          /* [nframes][msgSize]   a-posteriori L-values */
+  void* syst_out;     /* [nframes][systSize]  extrinsic on systematic bits */
+  void* parity_out;   /* [nframes][paritySize] extrinsic on every code bit */
+  void* state_out;    /* [nframes][stateSize] decoder state */
+  int32_t out_dtype;  /* element type of the four outputs (FECL_F64 or FECL_F32) */
+} fecl_so_io;
+
+int fecl_so_decode(fecl_codec_t codec, const fecl_so_io* io, uint64_t nframes, int32_t flags, void* stream);
+
+void fecl_destroy(fecl_codec_t codec);
+
+const char* fecl_strerror(int status);
+/* Message of the last failing call on this thread. */
+const char* fecl_last_error(void);
+
+/* Library version and the device architecture the kernels were built for. */
+const char* fecl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FECL_B200_H */
