@@ -1,0 +1,326 @@
+#!/usr/bin/env python3
+"""Benchmark of the decode hot path: LTE turbo decoding on the GPU.
+
+Workload (one "step"): one batch of 1024 LTE turbo frames, K = 6144, rate 1/3,
+8-state RSC (13, 15 octal) with trellis termination and the LTE QPP interleaver,
+BPSK over AWGN at Eb/N0 = 0.7 dB, FP32 L-values, max-log-MAP (Approximate),
+6 iterations, serial scheduling; synthetic seeded frames.
+
+value      decoded info Mbit/s with the L-values resident in device memory (each rank
+           decodes its own batch; whole-job bits / max-over-ranks device time).
+e2e        the same metric through the public decode call with pinned host buffers:
+           host->device copy of the L-values and device->host copy of the bits inside
+           the timed region.
+roofline   the dominant kernel against the measured HBM copy bandwidth, with the
+           algorithmic bytes of one decode over the decode's device time.
+
+`--impl reference` times the reference FeCl decoder compiled from its sources
+(oracle/_ref) on this machine's host cores on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "decoded info Mbit/s at matched FER vs plain GPU path; p50/p99 latency"
+K = 6144
+FRAMES = 1024
+ITERATIONS = 6
+EBN0_DB = 0.7
+SEED = 2024
+
+
+def workload_config(n_gpus):
+    return {
+        "workload": "LTE turbo decode, K=6144 x 1024 frames per GPU, rate 1/3 RSC(13,15) + QPP, "
+                    "max-log-MAP, 6 iterations, serial, Eb/N0 0.7 dB, FP32 L-values",
+        "K": K, "frames_per_gpu": FRAMES, "iterations": ITERATIONS, "algorithm": "Approximate (max-log-MAP)",
+        "scheduling": "Serial", "ebn0_db": EBN0_DB, "llr_dtype": "f32",
+        "l2": "flushed between timed steps (256 MiB write); inputs 75.5 MB per GPU",
+        "parallelism": "frame shards, replicas per GPU" if n_gpus > 1 else "single GPU",
+    }
+
+
+def algorithmic_bytes_per_frame(k=K, iters=ITERATIONS, s_llr=4, s_ext=4):
+    """Minimal traffic of one frame decode: the L-values once, then per
+    half-iteration the systematic + parity + a-priori reads and the extrinsic
+    write, then one byte per decoded bit."""
+    return (3 * k + 12) * s_llr + iters * 2 * ((2 * k + 3) * s_llr + 2 * (k + 3) * s_ext) + k
+
+
+def make_inputs(code, frames, seed):
+    import numpy as np
+    from fecl_b200 import channel as ch
+    msg = ch.random_bits(frames * code.msgSize(), seed)
+    cw = code.encode(msg)
+    llr = ch.awgn_llr(cw, EBN0_DB, code.msgSize() / code.paritySize(), seed, np.float32)
+    return msg, llr
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per decode of the dominant kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "turbo_lte_traffic.json")) as f:
+            return json.load(f).get("dram_bytes_per_decode")
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        try:
+            self.f.seek(0)
+            rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+            os.unlink(self.f.name)
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_reference(frames_sample, llr, code_sizes):
+    """Time the reference FeCl decoder (oracle/_ref) with all host threads on a
+    bounded sample of the workload.  Falls back to the C restatement of the oracle."""
+    import numpy as np
+    from oracle import ref
+    import fecl_b200 as F
+    cores = os.cpu_count() or 1
+    n = frames_sample
+    x = np.ascontiguousarray(llr[: n * code_sizes["parity"]], dtype=np.float64)
+    if ref.available():
+        rc = ref.RefCodec.turbo([([4], [[0o15]], [0o13])], [np.arange(K), F.Turbo.Lte3Gpp.interleaver(K)], 0,
+                                F.Approximate, F.Serial, ITERATIONS, workgroup=cores)
+        t = time.perf_counter()
+        bits = rc.decode(x)
+        dt = time.perf_counter() - t
+        kind = "reference"
+    else:
+        from oracle import restated
+        if not restated.available():
+            return None, None
+        t = time.perf_counter()
+        bits, _ = restated.turbo_lte_decode(K, F.Approximate, ITERATIONS, F.Serial, x, threads=cores)
+        dt = time.perf_counter() - t
+        kind = "port"
+    return {"value": n * K / dt / 1e6, "unit": "Mbit/s", "cores": cores, "kind": kind,
+            "sample": "%d frames of the workload, one decode, %d threads, %.2f s wall" % (n, cores, dt)}, bits
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference_arm(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    import numpy as np
+    import fecl_b200 as F
+    from oracle import ref
+    code = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(ITERATIONS).scheduling(F.Serial))
+    sizes = {"parity": code.paritySize()}
+    cores = os.cpu_count() or 1
+    sample = max(8, min(FRAMES, cores * 8))
+    msg, llr = make_inputs(code, sample, SEED)
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfecl_ref.so was not built on this machine"}))
+        return 0
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb, _ = cpu_reference(sample, llr, sizes)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.median(vals)
+    cb["value"] = v
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "Mbit/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sample * K / v / 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(world), "cpu_baseline": cb,
+        "e2e": {"value": round(v, 3), "unit": "Mbit/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-decodes", type=int, default=0,
+                    help="only run this many decodes of the workload (for ncu captures) and exit")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import fecl_b200 as F
+    dec = F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(ITERATIONS).scheduling(F.Serial)
+    code = F.Turbo.lte(K, dec)
+    msg, llr = make_inputs(code, FRAMES, SEED + rank)
+    d_llr = torch.from_numpy(llr).cuda()
+    d_bits = torch.empty(FRAMES * K, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    if args.profile_decodes:
+        for _ in range(args.profile_decodes):
+            code.decode(d_llr, out=d_bits)
+        torch.cuda.synchronize()
+        return 0
+
+    for _ in range(max(args.warmup, 3)):
+        code.decode(d_llr, out=d_bits)
+    barrier()
+
+    # ---- device-resident timing
+    times = []
+    with ClockSampler(local) as clk:
+        barrier()
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            code.decode(d_llr, out=d_bits)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        barrier()
+    clocks = clk.summary()
+    bits = d_bits.cpu().numpy()
+    fer = float(np.mean(np.any(bits.reshape(FRAMES, K) != msg.reshape(FRAMES, K), axis=1)))
+    ms = statistics.mean(times)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * FRAMES * K / (ms * 1e-3) / 1e6
+
+    # ---- end to end through the public call with pinned host buffers
+    h_llr = torch.from_numpy(llr).pin_memory()
+    h_bits = torch.empty(FRAMES * K, dtype=torch.uint8).pin_memory()
+    code.decode(h_llr, out=h_bits)
+    e2e_times = []
+    barrier()
+    for _ in range(max(2, args.steps // 2)):
+        t0 = time.perf_counter()
+        code.decode(h_llr, out=h_bits)
+        e2e_times.append(time.perf_counter() - t0)
+    barrier()
+    e2e_s = statistics.mean(e2e_times)
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * FRAMES * K / e2e_s / 1e6
+
+    peak, peak_kind = measured_peaks()
+    alg = algorithmic_bytes_per_frame() * FRAMES
+    achieved = alg / (ms * 1e-3) / 1e9
+    traffic = profiled_traffic()
+
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "Mbit/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(world),
+        "fer": fer, "latency_ms": {"p50": round(statistics.median(times), 4),
+                                   "p99": round(sorted(times)[min(len(times) - 1, int(0.99 * len(times)))], 4)},
+        "e2e": {"value": round(e2e_value, 2), "unit": "Mbit/s", "h2d_bytes_per_step": int(llr.nbytes),
+                "d2h_bytes_per_step": int(FRAMES * K)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                     "kernel": "turbo_lte_kernel (+ input staging) per decode",
+                     "algorithmic_bytes_per_decode": alg},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb, ref_bits = cpu_reference(FRAMES, llr, {"parity": code.paritySize()})
+        line["cpu_baseline"] = cb
+        if ref_bits is not None:
+            line["matched_hard_decisions_vs_reference"] = bool(np.array_equal(ref_bits, bits))
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -134,7 +134,7 @@ def _is_device(x):
 
 
 def _dtype_code(a):
-    if _is_device(a):
+    if hasattr(a, "data_ptr"):
         import torch
         m = {torch.float64: _lib.F64, torch.float32: _lib.F32, torch.float16: _lib.F16}
     else:
@@ -206,8 +206,11 @@ class Codec:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            _L.fecl_destroy(h)
+        if h is not None and h.value and _L is not None:
+            try:
+                _L.fecl_destroy(h)
+            except Exception:
+                pass
             self._h = C.c_void_p(0)
 
     def msgSize(self):
@@ -221,6 +224,11 @@ class Codec:
 
     def stateSize(self):
         return self._sizes[3]
+
+    def setKernel(self, kernel):
+        """Extension: 'auto' (fastest kernel for the code) or 'generic' (the kernels that
+        walk the reference's operation order in FP32)."""
+        _check(_L.fecl_set_kernel(self._h, {"auto": _lib.KERNEL_AUTO, "generic": _lib.KERNEL_GENERIC}[kernel]))
 
     # Codec::getWorkGroupSize / setWorkGroupSize (src/Codec.h:65-66): a CPU thread count
     # in the reference; kept for API compatibility, the device decoder ignores it.
@@ -252,19 +260,33 @@ class Codec:
         _check(_L.fecl_check(self._h, _ptr(p), n, C.byref(ok)))
         return bool(ok.value)
 
-    def decode(self, parity, iterations=False):
+    def decode(self, parity, iterations=False, out=None):
         """Codec::decode -- src/Codec.h:210-238.  Returns the hard message bits and,
-        with iterations=True, the per-frame iteration counts."""
+        with iterations=True, the per-frame iteration counts.
+
+        parity may be a numpy array (host memory), a torch CUDA tensor (device memory,
+        asynchronous on the current stream) or a torch CPU tensor, ideally pinned (host
+        memory; the call copies in, decodes and copies out).  `out` optionally receives
+        the bits (same kind of memory as parity)."""
         if _is_device(parity):
             import torch
             x = parity.contiguous().view(-1)
             n = self._frames(x.numel(), self.paritySize(), "parity")
-            msg = torch.empty(n * self.msgSize(), dtype=torch.uint8, device=x.device)
+            msg = out if out is not None else torch.empty(n * self.msgSize(), dtype=torch.uint8, device=x.device)
             it = torch.empty(n, dtype=torch.int32, device=x.device) if iterations else None
             stream = torch.cuda.current_stream(x.device).cuda_stream
             _check(_L.fecl_decode(self._h, C.c_void_p(x.data_ptr()), _dtype_code(x), n, C.c_void_p(msg.data_ptr()),
                                   C.c_void_p(it.data_ptr()) if it is not None else None, _lib.DEVICE_MEMORY,
                                   C.c_void_p(stream)))
+            return (msg, it) if iterations else msg
+        if hasattr(parity, "data_ptr"):  # torch CPU tensor
+            import torch
+            x = parity.contiguous().view(-1)
+            n = self._frames(x.numel(), self.paritySize(), "parity")
+            msg = out if out is not None else torch.empty(n * self.msgSize(), dtype=torch.uint8)
+            it = torch.empty(n, dtype=torch.int32) if iterations else None
+            _check(_L.fecl_decode(self._h, C.c_void_p(x.data_ptr()), _dtype_code(x), n, C.c_void_p(msg.data_ptr()),
+                                  C.c_void_p(it.data_ptr()) if it is not None else None, _lib.HOST_MEMORY, None))
             return (msg, it) if iterations else msg
         x = np.asarray(parity)
         if x.dtype not in (np.float64, np.float32, np.float16):
@@ -583,6 +605,16 @@ class Turbo(Codec):
         opts, keep = self._options(decoder)
         _check(_L.fecl_turbo_set_options(self._h, C.byref(opts)))
         self._decoder = decoder
+
+    def setWindowTraining(self, steps):
+        """Extension: training steps of the windowed LTE decoder (multiple of 8, -1 default)."""
+        _check(_L.fecl_turbo_set_window_training(self._h, int(steps)))
+
+    def windowStats(self):
+        """Extension: (passes, fix-up rounds, recomputed segments) since the last call."""
+        a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(_L.fecl_turbo_window_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
 
     def getDecoderOptions(self):
         return self._decoder

@@ -13,6 +13,7 @@ OK, EINVAL, ECUDA, ENOMEM, ETIMEDOUT, EUNSUPPORTED, ENODEV = 0, -1, -2, -3, -4, 
 F64, F32, F16 = 0, 1, 2
 MSG_F32, MSG_F16, MSG_I8 = 0, 1, 2
 HOST_MEMORY, DEVICE_MEMORY = 0, 1
+KERNEL_AUTO, KERNEL_GENERIC = 0, 1
 
 
 class fecl_sizes(C.Structure):
@@ -85,6 +86,9 @@ SIGNATURES = [
     ("fecl_decode", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     ("fecl_so_decode", C.c_int, [C.c_void_p, C.POINTER(fecl_so_io), C.c_uint64, C.c_int32, C.c_void_p]),
     ("fecl_destroy", None, [C.c_void_p]),
+    ("fecl_set_kernel", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fecl_turbo_set_window_training", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fecl_turbo_window_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("fecl_strerror", C.c_char_p, [C.c_int]),
     ("fecl_last_error", C.c_char_p, []),
     ("fecl_version", C.c_char_p, []),

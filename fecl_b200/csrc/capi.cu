@@ -225,7 +225,11 @@ struct fecl_codec_s {
       k.syst_size = int32_t(c.syst_size());
       k.syst_tail_size = int32_t(c.syst_tail_size());
       k.parity_size = int32_t(c.parity_size());
-      for (auto* v : {&c.trellis.next_state, &c.trellis.output, &c.perm}) {
+      // interleavers are padded with zeros so that 8-entry vector loads never leave them
+      std::vector<uint32_t> padded_perm(c.perm);
+      padded_perm.resize(c.perm.size() + 16, 0);
+      for (const std::vector<uint32_t>* v : {&c.trellis.next_state, &c.trellis.output,
+                                             static_cast<const std::vector<uint32_t>*>(&padded_perm)}) {
         tables.emplace_back(new DeviceBuffer);
         tables.back()->upload(*v);
       }
@@ -251,6 +255,20 @@ struct fecl_codec_s {
   }
 
   bool on_device = false;
+  int lte_train = -1;
+  bool force_generic = false;
+  DeviceBuffer stats;  // windowed turbo counters
+  // The windowed kernel covers the LTE RSC pair with serial scheduling and FP32 messages
+  // for any K whose two exchange arrays fit in shared memory.
+  bool lte_fast_ok() const {
+    if (force_generic || kind != 1 || !turbo->is_lte_shape()) return false;
+    const auto& d = turbo->decoder();
+    if (d.scheduling != 0 || d.precision != 0 || d.iterations == 0) return false;
+    static const fecl::Trellis lte = fecl::lte_trellis();
+    for (const auto& c : turbo->constituents())
+      if (c.trellis.next_state != lte.next_state || c.trellis.output != lte.output) return false;
+    return turbo->msg_size() <= 12288;
+  }
   // Device resources are created at the first decode, so that host-side operations
   // (encode, check, the transformed matrix) work without a GPU.
   void ensure_device() {
@@ -363,7 +381,10 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
     if (io->state_out) o_sto = cv.take(n * X * osz);
   }
   size_t o_s1 = 0, o_s2 = 0, o_s3 = 0, o_s4 = 0, o_s5 = 0;
-  if (c->kind == 0) {
+  const bool lte_fast = c->kind == 1 && !soft && c->lte_fast_ok();
+  if (lte_fast) {
+    o_s1 = cv.take(fecl::turbo_lte_scratch_bytes(int(c->msg()), int64_t(n)));
+  } else if (c->kind == 0) {
     o_s1 = cv.take(n * c->ldev.E * 4);
     o_s2 = cv.take(n * P * 4);
     o_s3 = cv.take(n * P * 4);
@@ -427,6 +448,27 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
     r.app = static_cast<float*>(dptr(o_s2));
     r.chan = static_cast<float*>(dptr(o_s3));
     e = fecl::launch_ldpc_flood(c->ldev, r, s);
+  } else if (lte_fast) {
+    fecl::TurboLteParams r;
+    r.nframes = int64_t(n);
+    r.K = int32_t(c->msg());
+    r.iterations = c->tdev.iterations;
+    r.algorithm = c->tdev.algorithm;
+    r.train = c->lte_train;
+    r.perm[0] = c->tdev.c[0].perm;
+    r.perm[1] = c->tdev.c[1].perm;
+    r.sf = c->tdev.sf;
+    r.llr = d_llr;
+    r.llr_dtype = io->in_dtype;
+    r.hard = d_hard;
+    r.iters = d_iters;
+    r.scratch = static_cast<float*>(dptr(o_s1));
+    if (!c->stats.ptr) {
+      c->stats.reserve(3 * sizeof(unsigned long long));
+      cuda_check(cudaMemsetAsync(c->stats.ptr, 0, 3 * sizeof(unsigned long long), s), "cudaMemset");
+    }
+    r.stats = c->stats.as<unsigned long long>();
+    e = fecl::launch_turbo_lte(r, s);
   } else {
     fecl::TurboRun r;
     r.nframes = int64_t(n);
@@ -700,6 +742,44 @@ int fecl_so_decode(fecl_codec_t codec, const fecl_so_io* io, uint64_t nframes, i
     std::lock_guard<std::mutex> lk(c->mu);
     if (nframes == 0) return;
     run_decode(c, io, nframes, nullptr, nullptr, true, flags, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fecl_set_kernel(fecl_codec_t codec, int32_t kernel) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (kernel != FECL_KERNEL_AUTO && kernel != FECL_KERNEL_GENERIC) fail(FECL_EINVAL, "Invalid kernel selection");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->force_generic = (kernel == FECL_KERNEL_GENERIC);
+  });
+}
+
+int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 1) fail(FECL_EINVAL, "not a turbo codec");
+    if (steps != -1 && (steps < 0 || steps % 8 != 0 || steps > 4096)) fail(FECL_EINVAL, "training steps must be a multiple of 8");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->lte_train = steps;
+  });
+}
+
+int fecl_turbo_window_stats(fecl_codec_t codec, uint64_t* passes, uint64_t* fixup_rounds, uint64_t* recomputed) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 1) fail(FECL_EINVAL, "not a turbo codec");
+    std::lock_guard<std::mutex> lk(c->mu);
+    unsigned long long v[3] = {0, 0, 0};
+    if (c->stats.ptr) {
+      DeviceGuard dg(c->device);
+      if (c->pending) cuda_check(cudaEventSynchronize(c->done), "cudaEventSynchronize");
+      cuda_check(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+      cuda_check(cudaMemcpy(v, c->stats.ptr, sizeof(v), cudaMemcpyDeviceToHost), "stats");
+      cuda_check(cudaMemset(c->stats.ptr, 0, sizeof(v)), "stats");
+    }
+    if (passes) *passes = v[0];
+    if (fixup_rounds) *fixup_rounds = v[1];
+    if (recomputed) *recomputed = v[2];
   });
 }
 

@@ -92,4 +92,28 @@ struct TurboRun {
 
 cudaError_t launch_turbo_generic(const TurboDeviceCode& code, const TurboRun& run, cudaStream_t stream);
 
+// Windowed decoder for two constituents of the LTE RSC with Tail termination.
+struct TurboLteParams {
+  int64_t nframes = 0;
+  int32_t K = 0;
+  int32_t iterations = 6;
+  int32_t algorithm = 2;
+  int32_t train = -1;  // training steps before each segment (-1: default)
+  const uint32_t* perm[2] = {nullptr, nullptr};  // interleavers of the constituents
+  const float* sf = nullptr;                     // [2][iterations]
+  const void* llr = nullptr;
+  int32_t llr_dtype = 1;
+  uint8_t* hard = nullptr;
+  int32_t* iters = nullptr;
+  float* scratch = nullptr;  // turbo_lte_scratch_bytes(K, nframes)
+  unsigned long long* stats = nullptr;  // [3] passes, fix-up rounds, recomputed segments (nullable)
+  // filled by the launcher
+  int32_t Kp = 0, Tp = 0, seg_len = 0;
+  int64_t frame_stride = 0;
+  float* ck = nullptr;
+};
+
+size_t turbo_lte_scratch_bytes(int K, int64_t nframes);
+cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s);
+
 }  // namespace fecl

@@ -1,0 +1,551 @@
+// Windowed turbo decoder for two 8-state rate-1/2 constituents with Tail
+// termination (the LTE code of 3GPP TS 36.212 and every code of that shape),
+// serial scheduling, hard-decision decode, FP32 metrics.
+//
+// What it computes is the reference's full-frame BCJR (MapDecoderImpl,
+// src/detail/MapDecoder/MapDecoderImpl.cpp:80-235) inside the serial turbo loop
+// (TurboDecoderImpl::decodeBlock, src/detail/TurboDecoder/TurboDecoderImpl.cpp:31-72);
+// how it computes it is B200-shaped:
+//
+//   One CTA decodes one frame for all iterations.  The frame's two exchange arrays
+//   live in shared memory in natural bit order:
+//     X[k] = Ls[k] + e0[k]          (a-priori of constituent 1 before interleaving;
+//                                    also the partial a-posteriori sum)
+//     Y[k] = e1 at natural index k  (constituent 1 writes e1(t) to Y[pi(t)])
+//   so constituent 0 reads Ls + Y contiguously and constituent 1 gathers X[pi(t)].
+//
+//   Per half-iteration:
+//   A. 64 forward and 64 backward segments run concurrently (one thread each).  A
+//      segment starts from metrics obtained by a training run of G steps from a
+//      flat start, walks its steps and leaves metric checkpoints every 8 steps in
+//      global memory (L2) plus its end metrics in shared memory.
+//   A2. Verification.  Segment 0 (forward) and the last segment (backward) start
+//      from the exact trellis termination.  The training start of segment w is
+//      accepted when it matches, within FP32 rounding (kCloseTol), the end metrics
+//      that segment w-1 computed from its own accepted start; otherwise segment w
+//      is recomputed from that end.  Rounds repeat until every boundary is
+//      accepted, so every checkpoint equals the full-frame recursion up to
+//      rounding.  (Max-log and log-MAP forget their start exponentially fast;
+//      training merely makes fix-ups rare.)
+//   B. Every 8-step block is then independent: a thread reloads the forward
+//      checkpoint at the block start and the backward checkpoint at its end,
+//      recomputes the 8 forward vectors in registers and walks backward emitting
+//      the extrinsic values, scaled, minus the a-priori (MapDecoderImpl.cpp:203-212).
+//
+// Inputs are first converted into a padded FP32 scratch layout so that every
+// block load is 16-byte aligned.
+#include <math.h>
+
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace fecl {
+namespace {
+
+constexpr int kExact = 0, kLinear = 1, kApproximate = 2;
+constexpr int kThreads = 128;
+constexpr int kSegs = 64;  // segments per direction (one thread each)
+constexpr int kBlk = 8;    // checkpoint spacing / APP block length
+constexpr float kNegInf = -INFINITY;
+constexpr float kCloseTol = 1e-3f;
+
+__constant__ LinearLut c_lut;
+
+// The LTE RSC, Trellis({4}, {{015}}, {013}) (src/Trellis.cpp:76-143): with state bits
+// s0 s1 s2, the feedback bit is u ^ s0 ^ s1, the next state shifts it in at the top
+// and the parity output is u ^ s1 ^ s2.  Compile-time tables keep every metric in
+// registers.
+__host__ __device__ constexpr int lte_next(int s, int u) { return (s >> 1) | (((u ^ s ^ (s >> 1)) & 1) << 2); }
+__host__ __device__ constexpr int lte_out(int s, int u) { return (u ^ (s >> 1) ^ (s >> 2)) & 1; }
+
+template <int ALG>
+__device__ __forceinline__ float lsum(float a, float b) {
+  if (ALG == kApproximate) return fmaxf(a, b);
+  if (a == b) return a;
+  return fmaxf(a, b) + lut_log1pexpm(c_lut, fabsf(a - b));
+}
+
+// Two-term log-sum in the Exact (LogSum) form: max, then exp-sum, then log.
+__device__ __forceinline__ float esum2(float x0, float x1) {
+  const float m = fmaxf(x0, x1);
+  const float a = (x0 == m) ? 1.0f : expf(x0 - m);
+  const float b = (x1 == m) ? 1.0f : expf(x1 - m);
+  return logf(a + b) + m;
+}
+
+struct Gam {
+  float g[4];  // index (u << 1) | p : 0, Lp, La, La + Lp
+  __device__ __forceinline__ void set(float la, float lp) {
+    g[0] = 0.0f;
+    g[1] = lp;
+    g[2] = la;
+    g[3] = lp + la;
+  }
+  __device__ __forceinline__ float of(int s, int u) const { return g[(u << 1) | lte_out(s, u)]; }
+};
+
+// alpha_{t+1} from alpha_t (MapDecoderImpl.cpp:117-139, :237-274), normalised by its max.
+template <int ALG>
+__device__ __forceinline__ void fwd_step(float a[8], const Gam& g) {
+  float n[8];
+  if (ALG == kExact) {
+    float c0[8], c1[8];
+    bool first[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) first[s] = true;
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int d = lte_next(s, u);
+        const float v = a[s] + g.of(s, u);
+        if (first[d]) {
+          c0[d] = v;
+          first[d] = false;
+        } else {
+          c1[d] = v;
+        }
+      }
+#pragma unroll
+    for (int s = 0; s < 8; ++s) n[s] = esum2(c0[s], c1[s]);
+  } else {
+#pragma unroll
+    for (int s = 0; s < 8; ++s) n[s] = kNegInf;
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int d = lte_next(s, u);
+        n[d] = lsum<ALG>(n[d], a[s] + g.of(s, u));
+      }
+  }
+  float m = kNegInf;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) m = fmaxf(n[s], m);
+#pragma unroll
+  for (int s = 0; s < 8; ++s) a[s] = n[s] - m;
+}
+
+// beta_t from beta_{t+1} (MapDecoderImpl.cpp:141-172, :276-329), normalised by its max.
+template <int ALG>
+__device__ __forceinline__ void bwd_step(float b[8], const Gam& g) {
+  float n[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    const float x0 = b[lte_next(s, 0)] + g.of(s, 0);
+    const float x1 = b[lte_next(s, 1)] + g.of(s, 1);
+    if (ALG == kExact) n[s] = esum2(x0, x1);
+    else n[s] = lsum<ALG>(lsum<ALG>(kNegInf, x0), x1);
+  }
+  float m = kNegInf;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) m = fmaxf(n[s], m);
+#pragma unroll
+  for (int s = 0; s < 8; ++s) b[s] = n[s] - m;
+}
+
+// L(u) = post(sum over u=1) - post(sum over u=0) (msgUpdateImpl, MapDecoderImpl.cpp:331-376).
+template <int ALG>
+__device__ __forceinline__ float app_step(const float a[8], const float b[8], const Gam& g) {
+  float d[16];
+#pragma unroll
+  for (int s = 0; s < 8; ++s)
+#pragma unroll
+    for (int u = 0; u < 2; ++u) d[s * 2 + u] = g.of(s, u) + a[s] + b[lte_next(s, u)];
+  if (ALG == kExact) {
+    float mx0 = kNegInf, mx1 = kNegInf;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      mx0 = fmaxf(d[s * 2], mx0);
+      mx1 = fmaxf(d[s * 2 + 1], mx1);
+    }
+    float m0 = 0.0f, m1 = 0.0f;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      m0 = ((d[s * 2] == mx0) ? 1.0f : expf(d[s * 2] - mx0)) + m0;
+      m1 = ((d[s * 2 + 1] == mx1) ? 1.0f : expf(d[s * 2 + 1] - mx1)) + m1;
+    }
+    return (logf(m1) + mx1) - (logf(m0) + mx0);
+  } else {
+    float m0 = kNegInf, m1 = kNegInf;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      m0 = lsum<ALG>(m0, d[s * 2]);
+      m1 = lsum<ALG>(m1, d[s * 2 + 1]);
+    }
+    return m1 - m0;
+  }
+}
+
+struct Frame {
+  const float* Ls;   // [Tp] systematic L-values, zero past K
+  const float* Lp0;  // [Tp]  parity (with tail parity) of constituent 0
+  const float* Lp1;  // [Tp]
+  const float* ts;   // [8]   tail systematic of constituent 0 (3) then 1 (3)
+  float* cka;        // [nblk + 1][8]
+  float* ckb;        // [nblk + 1][8]
+};
+
+struct Shared {
+  float sv[2][kSegs][8];  // metrics at the segment boundary after training (fwd, bwd)
+  float ev[2][kSegs][8];  // end metrics of each segment (fwd, bwd)
+  float in[2][kSegs][8];  // start metrics handed to a recomputed segment
+  float flat[8];          // training start: all states equal
+  float term[8];          // trellis termination: state 0
+  int bad[2][kSegs];
+  int any_bad;
+  float etail[2][4];
+};
+
+// Inputs of one 8-step chunk [8c, 8c + 8): a-priori and parity L-values.  Every
+// array read here is padded to Tp = 8 * nblk entries, so the vector loads stay
+// inside the frame's scratch even for the chunk holding the tail steps.
+struct Chunk {
+  float la[kBlk];
+  float lp[kBlk];
+};
+
+__device__ __forceinline__ void load_chunk(int j, int c, int K, const Frame& fr, const float* X, const float* Y,
+                                           const uint32_t* __restrict__ perm, Chunk& ch) {
+  const int t0 = c * kBlk;
+  const float* Lp = j == 0 ? fr.Lp0 : fr.Lp1;
+  const float4 p0 = __ldg(reinterpret_cast<const float4*>(Lp + t0));
+  const float4 p1 = __ldg(reinterpret_cast<const float4*>(Lp + t0) + 1);
+  ch.lp[0] = p0.x; ch.lp[1] = p0.y; ch.lp[2] = p0.z; ch.lp[3] = p0.w;
+  ch.lp[4] = p1.x; ch.lp[5] = p1.y; ch.lp[6] = p1.z; ch.lp[7] = p1.w;
+  if (j == 0) {
+    const float4 s0 = __ldg(reinterpret_cast<const float4*>(fr.Ls + t0));
+    const float4 s1 = __ldg(reinterpret_cast<const float4*>(fr.Ls + t0) + 1);
+    const float4 y0 = reinterpret_cast<const float4*>(Y + t0)[0];
+    const float4 y1 = reinterpret_cast<const float4*>(Y + t0)[1];
+    ch.la[0] = s0.x + y0.x; ch.la[1] = s0.y + y0.y; ch.la[2] = s0.z + y0.z; ch.la[3] = s0.w + y0.w;
+    ch.la[4] = s1.x + y1.x; ch.la[5] = s1.y + y1.y; ch.la[6] = s1.z + y1.z; ch.la[7] = s1.w + y1.w;
+  } else {
+    const uint4 q0 = __ldg(reinterpret_cast<const uint4*>(perm + t0));
+    const uint4 q1 = __ldg(reinterpret_cast<const uint4*>(perm + t0) + 1);
+    ch.la[0] = X[q0.x]; ch.la[1] = X[q0.y]; ch.la[2] = X[q0.z]; ch.la[3] = X[q0.w];
+    ch.la[4] = X[q1.x]; ch.la[5] = X[q1.y]; ch.la[6] = X[q1.z]; ch.la[7] = X[q1.w];
+  }
+  if (t0 + kBlk > K) {
+#pragma unroll
+    for (int i = 0; i < kBlk; ++i) {
+      const int t = t0 + i;
+      if (t >= K) ch.la[i] = (t < K + 3) ? fr.ts[j * 3 + (t - K)] : 0.0f;
+    }
+  }
+}
+
+__device__ __forceinline__ void store_ck(float* ck, const float v[8]) {
+  float4* q = reinterpret_cast<float4*>(ck);
+  q[0] = make_float4(v[0], v[1], v[2], v[3]);
+  q[1] = make_float4(v[4], v[5], v[6], v[7]);
+}
+
+// One segment walk of constituent j, forward (fwd != 0) or backward.  The start
+// metrics are read from vin (shared memory).  Training steps outside the segment
+// run first without checkpoints -- forward over [t_train, a0), backward over
+// [a1, t_train) -- then the metrics at the segment boundary are written to vstart,
+// the segment's own steps run, leaving checkpoints at every multiple of 8 inside
+// [a0, a1) (and at T for the last backward segment), and the final metrics go to
+// vend.  Each 8-step chunk's inputs are fetched with 16-byte loads before its steps
+// run; other warps cover the latency.  Kept out of line so that Phase A and the
+// fix-up rounds share one copy of the code.
+template <int ALG>
+__device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, int a1, const float* vin, float* vstart,
+                                          float* vend, int K, int T, Frame fr, const float* X, const float* Y,
+                                          const uint32_t* perm) {
+  float v[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) v[s] = vin[s];
+  if (fwd) {
+    for (int c = t_train / kBlk; c * kBlk < a1; ++c) {
+      const int t0 = c * kBlk;
+      if (t0 == a0) {
+#pragma unroll
+        for (int s = 0; s < 8; ++s) vstart[s] = v[s];
+      }
+      if (t0 >= a0) store_ck(fr.cka + c * 8, v);
+      Chunk ch;
+      load_chunk(j, c, K, fr, X, Y, perm, ch);
+      const int n = min(kBlk, a1 - t0);
+#pragma unroll
+      for (int i = 0; i < kBlk; ++i) {
+        if (i < n) {
+          Gam g;
+          g.set(ch.la[i], ch.lp[i]);
+          fwd_step<ALG>(v, g);
+        }
+      }
+    }
+  } else {
+    const int nblk = (T + kBlk - 1) / kBlk;
+    if (t_train == a1) {
+#pragma unroll
+      for (int s = 0; s < 8; ++s) vstart[s] = v[s];
+      if (a1 == T) store_ck(fr.ckb + nblk * 8, v);
+    }
+    for (int c = (t_train - 1) / kBlk; c >= a0 / kBlk; --c) {
+      Chunk ch;
+      load_chunk(j, c, K, fr, X, Y, perm, ch);
+      const int hi = min(kBlk, t_train - c * kBlk);
+#pragma unroll
+      for (int i = kBlk - 1; i >= 0; --i) {
+        if (i < hi) {
+          Gam g;
+          g.set(ch.la[i], ch.lp[i]);
+          bwd_step<ALG>(v, g);
+        }
+      }
+      const int tm = c * kBlk;  // v now holds the metrics at time tm
+      if (tm == a1) {
+#pragma unroll
+        for (int s = 0; s < 8; ++s) vstart[s] = v[s];
+      }
+      if (tm >= a0 && tm < a1) store_ck(fr.ckb + c * 8, v);
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < 8; ++s) vend[s] = v[s];
+}
+
+__device__ __forceinline__ bool close8(const float* x, const float* y) {
+  bool ok = true;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) ok = ok && ((x[s] == y[s]) || fabsf(x[s] - y[s]) <= kCloseTol);
+  return ok;
+}
+
+template <int ALG>
+__global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p) {
+  extern __shared__ float smem[];
+  const int K = p.K, T = p.K + 3;
+  const int nblk = (T + kBlk - 1) / kBlk;
+  float* X = smem;
+  float* Y = smem + p.Kp;
+  Shared& sh = *reinterpret_cast<Shared*>(smem + 2 * p.Kp);
+  const int64_t f = blockIdx.x;
+  Frame fr;
+  const float* base = p.scratch + f * p.frame_stride;
+  fr.Ls = base;
+  fr.Lp0 = base + p.Kp;
+  fr.Lp1 = base + p.Kp + p.Tp;
+  fr.ts = base + p.Kp + 2 * p.Tp;
+  fr.cka = p.ck + f * int64_t(2 * (nblk + 1) * 8);
+  fr.ckb = fr.cka + (nblk + 1) * 8;
+  const int tid = threadIdx.x;
+  const int L = p.seg_len;
+  const int S = (T + L - 1) / L;
+
+  for (int k = tid; k < p.Kp; k += kThreads) {
+    X[k] = 0.0f;
+    Y[k] = 0.0f;
+  }
+  if (tid < 8) {
+    sh.flat[tid] = 0.0f;
+    sh.term[tid] = tid == 0 ? 0.0f : kNegInf;  // Tail: the trellis starts and ends in state 0
+  }
+  __syncthreads();
+
+  for (int it = 0; it < p.iterations; ++it) {
+    for (int j = 0; j < 2; ++j) {
+      const uint32_t* perm = j == 0 ? p.perm[0] : p.perm[1];
+      // ---- A: segments with training starts
+      {
+        const bool fwd = tid < kSegs;
+        const int w = fwd ? tid : tid - kSegs;
+        if (w < S) {
+          const int a0 = w * L, a1 = min(T, a0 + L);
+          int t_train;
+          const float* vin;
+          if (fwd) {
+            const bool exact = (w == 0 || a0 - p.train <= 0);
+            t_train = exact ? 0 : a0 - p.train;
+            vin = exact ? sh.term : sh.flat;
+          } else {
+            const bool exact = (w == S - 1 || a1 + p.train >= T);
+            t_train = exact ? T : a1 + p.train;
+            vin = exact ? sh.term : sh.flat;
+          }
+          segment_walk<ALG>(fwd, j, t_train, a0, a1, vin, sh.sv[fwd ? 0 : 1][w], sh.ev[fwd ? 0 : 1][w], K, T, fr, X,
+                            Y, perm);
+        }
+      }
+      __syncthreads();
+      // ---- A2: verify boundaries; recompute segments whose start disagrees
+      int rounds = 0;
+      for (int round = 0; round < S; ++round) {
+        if (tid == 0) sh.any_bad = 0;
+        __syncthreads();
+        {
+          const bool fwd = tid < kSegs;
+          const int w = fwd ? tid : tid - kSegs;
+          int bad = 0;
+          if (w < S) {
+            if (fwd && w > 0) bad = !close8(sh.sv[0][w], sh.ev[0][w - 1]);
+            if (!fwd && w < S - 1) bad = !close8(sh.sv[1][w], sh.ev[1][w + 1]);
+          }
+          if (w < S) sh.bad[fwd ? 0 : 1][w] = bad;
+          if (bad) sh.any_bad = 1;
+        }
+        __syncthreads();
+        if (!sh.any_bad) break;
+        ++rounds;
+        {
+          // Recompute every rejected segment from its neighbour's end.  The ends are
+          // copied before the barrier and rewritten after it, so a neighbour that is
+          // itself being recomputed is read in its old state; the next round checks
+          // the boundary again.
+          const bool fwd = tid < kSegs;
+          const int w = fwd ? tid : tid - kSegs;
+          const bool mine = w < S && sh.bad[fwd ? 0 : 1][w];
+          if (mine) {
+#pragma unroll
+            for (int s = 0; s < 8; ++s) sh.in[fwd ? 0 : 1][w][s] = fwd ? sh.ev[0][w - 1][s] : sh.ev[1][w + 1][s];
+          }
+          __syncthreads();
+          if (mine) {
+            if (p.stats) atomicAdd(p.stats + 2, 1ull);
+            const int a0 = w * L, a1 = min(T, a0 + L);
+            segment_walk<ALG>(fwd, j, fwd ? a0 : a1, a0, a1, sh.in[fwd ? 0 : 1][w], sh.sv[fwd ? 0 : 1][w],
+                              sh.ev[fwd ? 0 : 1][w], K, T, fr, X, Y, perm);
+          }
+        }
+        __syncthreads();
+      }
+      if (p.stats && tid == 0) {
+        atomicAdd(p.stats + 0, 1ull);
+        atomicAdd(p.stats + 1, (unsigned long long)rounds);
+      }
+      // ---- B: 8-step blocks, extrinsic output
+      const float sf = p.sf[j * p.iterations + it];
+      float* out = j == 0 ? X : Y;
+      for (int b = tid; b < nblk; b += kThreads) {
+        const int t0 = b * kBlk;
+        const int n = min(kBlk, T - t0);
+        float al[kBlk][8];
+        {
+          const float4* ck = reinterpret_cast<const float4*>(fr.cka + b * 8);
+          const float4 c0 = ck[0], c1 = ck[1];
+          al[0][0] = c0.x; al[0][1] = c0.y; al[0][2] = c0.z; al[0][3] = c0.w;
+          al[0][4] = c1.x; al[0][5] = c1.y; al[0][6] = c1.z; al[0][7] = c1.w;
+        }
+        Chunk in;
+        load_chunk(j, b, K, fr, X, Y, perm, in);
+#pragma unroll
+        for (int i = 1; i < kBlk; ++i) {
+          if (i < n) {
+#pragma unroll
+            for (int s = 0; s < 8; ++s) al[i][s] = al[i - 1][s];
+            Gam g;
+            g.set(in.la[i - 1], in.lp[i - 1]);
+            fwd_step<ALG>(al[i], g);
+          }
+        }
+        float be[8];
+        {
+          const float4* ck = reinterpret_cast<const float4*>(fr.ckb + (b + 1) * 8);
+          const float4 c0 = ck[0], c1 = ck[1];
+          be[0] = c0.x; be[1] = c0.y; be[2] = c0.z; be[3] = c0.w;
+          be[4] = c1.x; be[5] = c1.y; be[6] = c1.z; be[7] = c1.w;
+        }
+        float ext[kBlk];
+#pragma unroll
+        for (int i = kBlk - 1; i >= 0; --i) {
+          if (i < n) {
+            Gam g;
+            g.set(in.la[i], in.lp[i]);
+            const float l = app_step<ALG>(al[i], be, g);
+            ext[i] = sf * (l - in.la[i]);
+            if (i > 0) bwd_step<ALG>(be, g);
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < kBlk; ++i) {
+          if (i < n) {
+            const int t = t0 + i;
+            if (t < K) {
+              if (j == 0) out[t] = fr.Ls[t] + ext[i];
+              else out[perm[t]] = ext[i];
+            } else {
+              sh.etail[j][t - K] = ext[i];
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // a-posteriori and hard decision, TurboDecoderImpl.cpp:64-71
+  for (int k = tid; k < K; k += kThreads) p.hard[f * K + k] = uint8_t((X[k] + Y[k]) > 0.0f);
+  if (p.iters && tid == 0) p.iters[f] = p.iterations;
+}
+
+// Input [f][3K+12] in FeCl's turbo layout -> padded FP32 scratch.
+__global__ void turbo_lte_stage(TurboLteParams p) {
+  const int K = p.K;
+  const int64_t total = p.nframes * p.frame_stride;
+  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total; idx += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t f = idx / p.frame_stride;
+    const int i = int(idx - f * p.frame_stride);
+    const int64_t in0 = f * int64_t(3 * K + 12);
+    float v = 0.0f;
+    if (i < p.Kp) {
+      if (i < K) v = load_llr(p.llr, p.llr_dtype, in0 + i);
+    } else if (i < p.Kp + 2 * p.Tp) {
+      const int c = (i - p.Kp) / p.Tp, t = (i - p.Kp) % p.Tp;
+      if (t < K + 3) v = load_llr(p.llr, p.llr_dtype, in0 + K + 6 + c * (K + 3) + t);
+    } else {
+      const int t = i - p.Kp - 2 * p.Tp;
+      if (t < 6) v = load_llr(p.llr, p.llr_dtype, in0 + K + t);
+    }
+    p.scratch[idx] = v;
+  }
+}
+
+}  // namespace
+
+size_t turbo_lte_scratch_bytes(int K, int64_t nframes) {
+  const int T = K + 3;
+  const int nblk = (T + kBlk - 1) / kBlk;
+  const int Tp = nblk * kBlk;
+  const int Kp = Tp;
+  const int64_t stride = Kp + 2 * Tp + 8;
+  return size_t(nframes) * (size_t(stride) + size_t(2 * (nblk + 1) * 8)) * sizeof(float);
+}
+
+cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
+  static bool init = false;
+  if (!init) {
+    LinearLut l;
+    for (int i = 0; i < 8; ++i) l.y[i] = float(log(1.0 + exp(-(double(i) / 2.0))));
+    cudaError_t e = cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
+    if (e != cudaSuccess) return e;
+    init = true;
+  }
+  if (p.nframes <= 0) return cudaSuccess;
+  const int T = p.K + 3;
+  const int nblk = (T + kBlk - 1) / kBlk;
+  p.Tp = nblk * kBlk;
+  p.Kp = p.Tp;  // the systematic region and the exchange arrays are padded like the parity
+  p.frame_stride = p.Kp + 2 * p.Tp + 8;
+  p.ck = p.scratch + p.nframes * p.frame_stride;
+  int L = (T + kSegs - 1) / kSegs;
+  L = (L + kBlk - 1) / kBlk * kBlk;
+  p.seg_len = L;
+  if (p.train < 0) p.train = 96;
+  turbo_lte_stage<<<1184, 256, 0, s>>>(p);
+  const size_t smem = size_t(2 * p.Kp) * sizeof(float) + sizeof(Shared);
+  auto launch = [&](auto kern) -> cudaError_t {
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (err != cudaSuccess) return err;
+    kern<<<unsigned(p.nframes), kThreads, smem, s>>>(p);
+    return cudaGetLastError();
+  };
+  switch (p.algorithm) {
+    case kExact: return launch(turbo_lte_kernel<kExact>);
+    case kLinear: return launch(turbo_lte_kernel<kLinear>);
+    default: return launch(turbo_lte_kernel<kApproximate>);
+  }
+}
+
+}  // namespace fecl

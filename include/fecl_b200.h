@@ -205,6 +205,27 @@ int fecl_so_decode(fecl_codec_t codec, const fecl_so_io* io, uint64_t nframes, i
 
 void fecl_destroy(fecl_codec_t codec);
 
+/* ---- extensions (no counterpart in the reference) ------------------------ */
+
+/* Kernel selection: FECL_KERNEL_AUTO picks the fastest kernel that supports the
+ * code and options; FECL_KERNEL_GENERIC forces the generic kernels, which walk the
+ * reference's operation order in FP32 (one thread per turbo frame, one CTA per
+ * LDPC frame). */
+#define FECL_KERNEL_AUTO 0
+#define FECL_KERNEL_GENERIC 1
+int fecl_set_kernel(fecl_codec_t codec, int32_t kernel);
+
+/* Windowed turbo decoder: training steps run before each segment's forward and
+ * backward walk (a multiple of 8; -1 restores the default of 96).  Training only
+ * sets how often a segment boundary fails verification and is recomputed; results
+ * do not depend on it beyond FP32 rounding. */
+int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps);
+
+/* Windowed turbo decoder counters since the previous call (which resets them):
+ * constituent passes run, verification rounds that found a boundary to
+ * recompute, and segments recomputed. */
+int fecl_turbo_window_stats(fecl_codec_t codec, uint64_t* passes, uint64_t* fixup_rounds, uint64_t* recomputed);
+
 const char* fecl_strerror(int status);
 /* Message of the last failing call on this thread. */
 const char* fecl_last_error(void);
