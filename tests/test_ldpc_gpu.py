@@ -1,0 +1,195 @@
+"""LDPC belief propagation on the GPU, against the FP64 oracle and the reference's
+own property tests (test/Cpp/operations.h, test/Cpp/Ldpc.cpp), called through the
+C-ABI (fecl_b200's ctypes binding)."""
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+from goldens import ARRAYS, GOLDEN, case_inputs, check_matrix, hard
+from parity import assert_hard_parity, assert_soft_parity, frame_ok, soft_error
+
+pytestmark = pytest.mark.gpu
+
+LDPC_CASES = [n for n, c in GOLDEN["cases"].items() if c["kind"] == "ldpc"]
+
+
+def make_code(H, alg, iterations, scaling=1.0):
+    import fecl_b200 as F
+    return F.Ldpc(F.Ldpc.EncoderOptions(H), F.Ldpc.DecoderOptions().algorithm(alg).iterations(iterations).scalingFactor(scaling))
+
+
+def distort(bits, snrdb, seed):
+    """The reference's test channel (test/Cpp/operations.h:42-59): L = (+-1) * N(4 snr, 4 sqrt(snr/2))."""
+    snr = 10.0 ** (snrdb / 10.0)
+    rng = np.random.default_rng(seed)
+    return np.where(np.asarray(bits) > 0, 1.0, -1.0) * rng.normal(snr * 4.0, 4.0 * np.sqrt(snr / 2.0), size=len(bits))
+
+
+@pytest.mark.parametrize("name", LDPC_CASES)
+def test_golden_parity(name):
+    """Hard and soft outputs against the reference's on the golden cases."""
+    import fecl_b200 as F
+    c = GOLDEN["cases"][name]
+    code = make_code(check_matrix(c["code"]), c["algorithm"], c["iterations"], c["scaling"])
+    msg, cw, llr = case_inputs(name, code.encode)
+    K = c["msg_size"]
+    ref_hard = hard(name)
+    ref_msg = ARRAYS[name + "__msg"]
+    bits = code.decode(llr.astype(np.float32))
+    assert_hard_parity(bits, ref_hard, msg, K, ref_app=ref_msg)
+    out = code.soDecode(F.Codec.Input().parity(llr.astype(np.float32)), F.Codec.Output().msg().parity().state())
+    ok = frame_ok(ref_hard, msg, K)
+    ex = c["algorithm"] == F.Exact
+    assert_soft_parity(out.msg(), ref_msg, ok, K, what="msg", exact=ex)
+    assert_soft_parity(out.parity(), ARRAYS[name + "__parity"], ok, c["parity_size"], what="parity", exact=ex)
+    if name + "__state" in ARRAYS.files:
+        assert_soft_parity(out.state(), ARRAYS[name + "__state"], ok, c["state_size"], what="state", exact=ex)
+
+
+@pytest.mark.parametrize("alg", [0, 1, 2])
+def test_config1_scale_parity(alg):
+    """DVB-S2 short frame rate 1/2, 64 frames at Eb/N0 1.5 dB, 20 iterations,
+    against the oracle on the same FP32 L-values."""
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    from oracle import checker
+    H = F.Ldpc.DvbS2.matrix(16200, Fraction(1, 2))
+    code = make_code(H, alg, 20)
+    K, N = code.msgSize(), code.paritySize()
+    msg = ch.random_bits(64 * K, 11)
+    llr = ch.awgn_llr(code.encode(msg), 1.5, K / N, 11, np.float32)
+    bits, its = code.decode(llr, iterations=True)
+    ref_bits, ref_app = checker.ldpc_decode(H, alg, 20, 1.0, llr)
+    assert_hard_parity(bits, ref_bits, msg, K, ref_app=ref_app)
+    assert its.min() >= 1 and its.max() <= 20
+    out = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().msg())
+    assert_soft_parity(out.msg(), ref_app, frame_ok(ref_bits, msg, K), K, what="APP", exact=alg == F.Exact)
+
+
+@pytest.fixture(scope="module", params=[0, 1, 2], ids=["exact", "linear", "approximate"])
+def suite_code(request):
+    """The reference suite's code: Gallager(2048, 3, 5, seed 0), 30 iterations."""
+    import fecl_b200 as F
+    return make_code(F.Ldpc.Gallager.matrix(2048, 3, 5, 0), request.param, 30), request.param
+
+
+def test_decode(suite_code):
+    """test_decode (operations.h:113-127) at the suite SNR, n = 1 and 5."""
+    code, _ = suite_code
+    for n in (1, 5):
+        msg = np.ones(code.msgSize() * n, np.uint8)
+        p = code.encode(msg)
+        assert np.array_equal(code.decode(distort(p, 2.0, n)), msg)
+
+
+def test_soDecode_agrees_with_decode(suite_code):
+    """test_soDecode (operations.h:159-180) at -5 dB."""
+    import fecl_b200 as F
+    code, _ = suite_code
+    p = code.encode(np.ones(code.msgSize(), np.uint8))
+    llr = distort(p, -5.0, 3)
+    out = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().msg())
+    dec = code.decode(llr)
+    assert np.array_equal(dec, (out.msg() >= 0).astype(np.uint8))
+
+
+def test_soDecode_parityOut(suite_code):
+    """test_soDecode_parityOut (operations.h:210-235)."""
+    import fecl_b200 as F
+    code, _ = suite_code
+    msg = np.ones(code.msgSize(), np.uint8)
+    p = code.encode(msg)
+    llr = distort(p, 2.0, 4)
+    out = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().msg().parity())
+    assert np.array_equal(msg, (out.msg() > 0).astype(np.uint8))
+    assert np.array_equal(p, ((llr + out.parity()) > 0).astype(np.uint8))
+
+
+def test_zero_syst_and_zero_state_equal_none(suite_code):
+    """test_soDecode_0systIn / 0stateIn (operations.h:276-342): bit-exact."""
+    import fecl_b200 as F
+    code, _ = suite_code
+    p = code.encode(np.ones(code.msgSize(), np.uint8))
+    llr = distort(p, -5.0, 5)
+    a = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().msg().syst().parity())
+    b = code.soDecode(F.Codec.Input().parity(llr).syst(np.zeros(code.systSize())), F.Codec.Output().msg().syst().parity())
+    c = code.soDecode(F.Codec.Input().parity(llr).state(np.zeros(code.stateSize())), F.Codec.Output().msg().syst().parity())
+    for x in (b, c):
+        assert np.array_equal(a.msg(), x.msg()) and np.array_equal(a.syst(), x.syst()) and np.array_equal(a.parity(), x.parity())
+
+
+def test_two_phase_resume(suite_code):
+    """test_soDecode_2phases (operations.h:344-383): I iterations, then I more from the
+    state, equal 2I iterations in one go, bit for bit."""
+    import fecl_b200 as F
+    code, alg = suite_code
+    code2 = make_code(F.Ldpc.Gallager.matrix(2048, 3, 5, 0), alg, 60)
+    p = code.encode(np.ones(code.msgSize(), np.uint8))
+    assert np.array_equal(p, code2.encode(np.ones(code.msgSize(), np.uint8)))
+    llr = distort(p, -5.0, 6)
+    st = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().state()).state()
+    a = code.soDecode(F.Codec.Input().parity(llr).state(st), F.Codec.Output().msg().syst().parity())
+    b = code2.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().msg().syst().parity())
+    assert np.array_equal(a.msg(), b.msg()) and np.array_equal(a.syst(), b.syst()) and np.array_equal(a.parity(), b.parity())
+
+
+def test_systOut_is_parityOut_prefix(suite_code):
+    """test_ldpc_soDecode_systOut (test/Cpp/Ldpc.cpp:32-49)."""
+    import fecl_b200 as F
+    code, _ = suite_code
+    llr = distort(code.encode(np.ones(code.msgSize(), np.uint8)), -5.0, 7)
+    out = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().parity().syst())
+    assert np.array_equal(out.syst(), out.parity()[: code.systSize()])
+
+
+def test_systIn_does_not_hurt(suite_code):
+    """test_soDecode_systIn (operations.h:237-274)."""
+    import fecl_b200 as F
+    code, _ = suite_code
+    msg = np.ones(code.msgSize(), np.uint8)
+    p = code.encode(msg)
+    llr = distort(p, -5.0, 8)
+    syst = distort(msg, -5.0, 9)
+    a = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().msg())
+    b = code.soDecode(F.Codec.Input().parity(llr).syst(syst), F.Codec.Output().msg())
+    e1 = np.sum(msg != (a.msg() > 0))
+    e2 = np.sum(msg != (b.msg() > 0))
+    assert e2 <= e1
+
+
+def test_state_resume_matches_oracle_soft(suite_code):
+    """soDecode with a-priori and state inputs against the oracle (all four outputs)."""
+    import fecl_b200 as F
+    from oracle import restated as O
+    if not O.available():
+        pytest.skip("restated oracle not built")
+    code, alg = suite_code
+    H = F.Ldpc.Gallager.matrix(2048, 3, 5, 0)
+    o = O.Ldpc(H.rows(), H.cols(), H.row_ptr, H.col_idx)
+    msg = np.ones(code.msgSize() * 3, np.uint8)
+    llr = distort(code.encode(msg), 1.0, 10).astype(np.float32).astype(np.float64)
+    syst = (0.1 * distort(msg, -5.0, 11)).astype(np.float32).astype(np.float64)
+    st = o.so_decode(llr, alg, 30, outputs=("state",))["state"].astype(np.float32).astype(np.float64)
+    ref = o.so_decode(llr, alg, 30, syst=syst, state=st)
+    out = code.soDecode(F.Codec.Input().parity(llr).syst(syst).state(st), F.Codec.Output().msg().syst().parity().state())
+    ok = frame_ok((ref["msg"] >= 0).astype(np.uint8), msg, code.msgSize())
+    for k in ("msg", "syst", "parity", "state"):
+        size = {"msg": code.msgSize(), "syst": code.systSize(), "parity": code.paritySize(), "state": code.stateSize()}[k]
+        assert_soft_parity(getattr(out, k)(), ref[k], ok, size, what=k, exact=alg == F.Exact)
+
+
+def test_input_dtypes_and_device_memory():
+    """float64 / float32 / float16 L-values, host and device memory give the same bits."""
+    import torch
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    H = F.Ldpc.DvbS2.matrix(16200, Fraction(1, 2))
+    code = make_code(H, F.Approximate, 20, 0.75)
+    K, N = code.msgSize(), code.paritySize()
+    llr = ch.awgn_llr(code.encode(ch.random_bits(4 * K, 12)), 2.0, K / N, 12, np.float16)
+    a = code.decode(llr)
+    b = code.decode(llr.astype(np.float32))
+    c = code.decode(llr.astype(np.float64))
+    d = code.decode(torch.from_numpy(llr).cuda()).cpu().numpy()
+    assert np.array_equal(a, b) and np.array_equal(b, c) and np.array_equal(c, d)

@@ -1,0 +1,198 @@
+"""Turbo decoding on the GPU, against the FP64 oracle and the reference's own
+property tests (test/Cpp/operations.h, test/Cpp/Turbo.cpp), through the C-ABI."""
+import numpy as np
+import pytest
+
+from goldens import ARRAYS, GOLDEN, SUITE3, T17, case_inputs, hard, turbo_layout
+from parity import assert_hard_parity, assert_soft_parity, frame_ok
+
+pytestmark = pytest.mark.gpu
+
+TURBO_CASES = [n for n, c in GOLDEN["cases"].items() if c["kind"] == "turbo"]
+
+
+def distort(bits, snrdb, seed):
+    snr = 10.0 ** (snrdb / 10.0)
+    rng = np.random.default_rng(seed)
+    return np.where(np.asarray(bits) > 0, 1.0, -1.0) * rng.normal(snr * 4.0, 4.0 * np.sqrt(snr / 2.0), size=len(bits))
+
+
+def make_turbo(specs, perms, term, alg, iterations, sched, scaling=None):
+    import fecl_b200 as F
+    dec = F.Turbo.DecoderOptions().algorithm(alg).iterations(iterations).scheduling(sched)
+    if scaling is not None:
+        dec.scalingFactor(np.asarray(scaling).tolist())
+    return F.Turbo(F.Turbo.EncoderOptions([F.Trellis(*s) for s in specs], perms).termination(term), dec)
+
+
+@pytest.mark.parametrize("kernel", ["auto", "generic"])
+@pytest.mark.parametrize("name", TURBO_CASES)
+def test_golden_parity(name, kernel):
+    import fecl_b200 as F
+    c = GOLDEN["cases"][name]
+    specs, perms = turbo_layout(c["code"])
+    code = make_turbo(specs, perms, c["termination"], c["algorithm"], c["iterations"], c["scheduling"], c["scaling"])
+    code.setKernel(kernel)
+    msg, cw, llr = case_inputs(name, code.encode)
+    K = c["msg_size"]
+    ref_hard = hard(name)
+    ref_msg = ARRAYS[name + "__msg"]
+    bits = code.decode(llr.astype(np.float32))
+    assert_hard_parity(bits, ref_hard, msg, K, ref_app=ref_msg)
+    if c["scaling"] is None:  # soDecode ignores scaling (TurboDecoderImpl.cpp:75-150); decode applies it
+        out = code.soDecode(F.Codec.Input().parity(llr.astype(np.float32)), F.Codec.Output().msg().state())
+        ok = frame_ok(ref_hard, msg, K)
+        assert_soft_parity(out.msg(), ref_msg, ok, K, what="msg")
+        assert_soft_parity(out.state(), ARRAYS[name + "__state"], ok, c["state_size"], what="state")
+
+
+@pytest.mark.parametrize("alg", [2, 1, 0])
+def test_config2_scale_parity(alg):
+    """LTE K=6144, 6 iterations, serial, Eb/N0 0.7 dB, 128 frames: the windowed
+    kernel against the FP64 oracle on the same FP32 L-values."""
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    from oracle import checker
+    K, n = 6144, 128
+    code = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(alg).iterations(6).scheduling(F.Serial))
+    msg = ch.random_bits(n * K, 31)
+    llr = ch.awgn_llr(code.encode(msg), 0.7, K / code.paritySize(), 31, np.float32)
+    bits = code.decode(llr)
+    ref_bits, ref_app = checker.turbo_lte_decode(K, alg, 6, F.Serial, llr)
+    assert_hard_parity(bits, ref_bits, msg, K, ref_app=ref_app)
+    passes, rounds, recomputed = code.windowStats()
+    assert passes == n * 12
+
+
+def test_windowed_equals_generic_kernel():
+    """The windowed LTE kernel and the generic (reference-order) kernel agree bit for
+    bit on the hard decisions, whatever the training length."""
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    K, n = 2048, 48
+    code = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(6))
+    msg = ch.random_bits(n * K, 32)
+    llr = ch.awgn_llr(code.encode(msg), 0.6, K / code.paritySize(), 32, np.float32)
+    code.setKernel("generic")
+    ref = code.decode(llr)
+    code.setKernel("auto")
+    for train in (0, 32, 96, 256):
+        code.setWindowTraining(train)
+        assert np.array_equal(code.decode(llr), ref), train
+
+
+@pytest.mark.parametrize("K", [40, 1008, 4096, 6144])
+def test_lte_sizes(K):
+    """Every LTE block size the windowed kernel sees decodes like the generic kernel."""
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    code = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(4))
+    msg = ch.random_bits(8 * K, K)
+    llr = ch.awgn_llr(code.encode(msg), 1.0, K / code.paritySize(), K, np.float32)
+    a = code.decode(llr)
+    code.setKernel("generic")
+    b = code.decode(llr)
+    assert np.array_equal(a, b)
+
+
+SUITE_PARAMS = [(1, 0, 1), (0, 0, 1), (0, 1, 1), (0, 2, 1), (0, 2, 0)]  # (termination, algorithm, scheduling)
+
+
+@pytest.fixture(scope="module", params=SUITE_PARAMS, ids=["default", "tail", "table", "approximate", "serial"])
+def suite_code(request):
+    """test/Cpp/Turbo.cpp:89-161: K=1024 random interleaver, Trellis({4},{{017}},{015}), 4 iterations."""
+    term, alg, sched = request.param
+    perms = [np.arange(1024, dtype=np.uint32), ARRAYS["perm_1024"]]
+    mk = lambda it: make_turbo([T17], perms, term, alg, it, sched)
+    return mk(4), mk(8)
+
+
+def test_decode(suite_code):
+    code, _ = suite_code
+    for n in (1, 5):
+        msg = np.ones(code.msgSize() * n, np.uint8)
+        assert np.array_equal(code.decode(distort(code.encode(msg), -2.0, n)), msg)
+
+
+def test_soDecode_agrees_with_decode(suite_code):
+    import fecl_b200 as F
+    code, _ = suite_code
+    llr = distort(code.encode(np.ones(code.msgSize(), np.uint8)), -5.0, 3)
+    out = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().msg())
+    assert np.array_equal(code.decode(llr), (out.msg() > 0).astype(np.uint8))
+
+
+def test_soDecode_parityOut(suite_code):
+    import fecl_b200 as F
+    code, _ = suite_code
+    msg = np.ones(code.msgSize(), np.uint8)
+    p = code.encode(msg)
+    llr = distort(p, -2.0, 4)
+    out = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().msg().parity())
+    assert np.array_equal(msg, (out.msg() > 0).astype(np.uint8))
+    assert np.array_equal(p, ((llr + out.parity()) > 0).astype(np.uint8))
+
+
+def test_zero_syst_and_zero_state_equal_none(suite_code):
+    import fecl_b200 as F
+    code, _ = suite_code
+    llr = distort(code.encode(np.ones(code.msgSize(), np.uint8)), -5.0, 5)
+    a = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().msg().syst().parity())
+    b = code.soDecode(F.Codec.Input().parity(llr).syst(np.zeros(code.systSize())), F.Codec.Output().msg().syst().parity())
+    c = code.soDecode(F.Codec.Input().parity(llr).state(np.zeros(code.stateSize())), F.Codec.Output().msg().syst().parity())
+    for x in (b, c):
+        assert np.array_equal(a.msg(), x.msg()) and np.array_equal(a.syst(), x.syst()) and np.array_equal(a.parity(), x.parity())
+
+
+def test_two_phase_resume(suite_code):
+    import fecl_b200 as F
+    code, code2 = suite_code
+    llr = distort(code.encode(np.ones(code.msgSize(), np.uint8)), -5.0, 6)
+    st = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().state()).state()
+    a = code.soDecode(F.Codec.Input().parity(llr).state(st), F.Codec.Output().msg().syst().parity())
+    b = code2.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().msg().syst().parity())
+    assert np.array_equal(a.msg(), b.msg()) and np.array_equal(a.syst(), b.syst()) and np.array_equal(a.parity(), b.parity())
+
+
+def test_systOut_is_parityOut_prefix(suite_code):
+    import fecl_b200 as F
+    code, _ = suite_code
+    llr = distort(code.encode(np.ones(code.msgSize(), np.uint8)), -5.0, 7)
+    out = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().parity().syst())
+    assert np.array_equal(out.syst(), out.parity()[: code.systSize()])
+
+
+@pytest.mark.parametrize("term", [1, 0])
+@pytest.mark.parametrize("sched", [0, 1])
+def test_three_variable_length_constituents(term, sched):
+    """test/Cpp/Turbo.cpp:143-161: three constituents, one with a 2-input trellis,
+    interleavers of lengths 1024, 512 and 512 (even positions)."""
+    import fecl_b200 as F
+    from oracle import restated as O
+    perms = [ARRAYS["perm_1024"], ARRAYS["perm_512"], ARRAYS["perm_even_512"]]
+    code = make_turbo(SUITE3, perms, term, F.Exact, 4, sched)
+    msg = np.ones(code.msgSize() * 2, np.uint8)
+    llr = distort(code.encode(msg), 0.0, 8)
+    assert np.array_equal(code.decode(llr), msg)
+    if O.available():
+        o = O.Turbo([O.trellis(*s) for s in SUITE3], perms, term)
+        x = llr.astype(np.float32).astype(np.float64)
+        ref = o.so_decode(x, F.Exact, 4, sched)
+        out = code.soDecode(F.Codec.Input().parity(x), F.Codec.Output().msg().syst().parity().state())
+        ok = frame_ok((ref["msg"] > 0).astype(np.uint8), msg, code.msgSize())
+        for k, size in (("msg", code.msgSize()), ("syst", code.systSize()), ("parity", code.paritySize()),
+                        ("state", code.stateSize())):
+            assert_soft_parity(getattr(out, k)(), ref[k], ok, size, what=k)
+
+
+def test_device_memory_decode_matches_host():
+    import torch
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    K = 6144
+    code = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(6))
+    llr = ch.awgn_llr(code.encode(ch.random_bits(16 * K, 40)), 0.8, K / code.paritySize(), 40, np.float32)
+    a = code.decode(llr)
+    b = code.decode(torch.from_numpy(llr).cuda()).cpu().numpy()
+    c = code.decode(torch.from_numpy(llr).pin_memory()).numpy()
+    assert np.array_equal(a, b) and np.array_equal(a, c)
