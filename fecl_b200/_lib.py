@@ -89,6 +89,7 @@ SIGNATURES = [
     ("fecl_set_kernel", C.c_int, [C.c_void_p, C.c_int32]),
     ("fecl_turbo_set_window_training", C.c_int, [C.c_void_p, C.c_int32]),
     ("fecl_turbo_window_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("fecl_lte_turbo_decode_noalloc", C.c_int, [C.c_uint32, C.c_int32, C.c_uint32, C.c_void_p, C.c_int32, C.c_uint64, C.c_void_p, C.c_void_p]),
     ("fecl_strerror", C.c_char_p, [C.c_int]),
     ("fecl_last_error", C.c_char_p, []),
     ("fecl_version", C.c_char_p, []),

@@ -119,6 +119,11 @@ size_t dsize(int dtype) {
 
 }  // namespace
 
+namespace fecl {
+// Lets entry points in other translation units report errors through fecl_last_error().
+void set_last_error(const std::string& msg) { g_error = msg; }
+}  // namespace fecl
+
 struct fecl_codec_s {
   int kind = 0;  // 0 LDPC, 1 turbo
   int device = 0;

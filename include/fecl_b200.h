@@ -226,6 +226,27 @@ int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps);
  * recompute, and segments recomputed. */
 int fecl_turbo_window_stats(fecl_codec_t codec, uint64_t* passes, uint64_t* fixup_rounds, uint64_t* recomputed);
 
+/* Allocation-free LTE turbo decode.  No counterpart in the reference.  For callers
+ * that cannot allocate device memory once running -- a pipeline that reserves its
+ * whole memory budget at start-up, a real-time thread that must not block in
+ * cudaMalloc, a plug-in host that owns the memory pool -- this decodes `nframes`
+ * LTE turbo frames (the code of fecl_turbo_create_lte, Serial scheduling, scaling
+ * 1.0) with the windowed kernel of fecl_decode, bit-identical to it, but calls no
+ * cudaMalloc, cudaFree or allocating library routine.  Its scratch, interleaver and
+ * scaling tables are fixed-size static device arrays (8 MiB of scratch, K <= 6144,
+ * iterations <= 64) that every GPU loading the library holds until process exit;
+ * a batch needing more scratch than 8 MiB (more than 68 frames at K = 6144) is
+ * rejected with FECL_EINVAL.  llr ([nframes][3K+12]) and msg ([nframes][K] bytes)
+ * are device memory of the current device; the call is asynchronous on `stream`.
+ * The first call on a device looks up the arrays' device addresses there, so make
+ * it once with each device current before relying on the call being cheap.  All
+ * calls on a device share the arrays and overwrite them: calls that overlap on the
+ * GPU (different streams, or different host threads) race and must be serialised
+ * by the caller.  Every scratch element a call reads it first writes itself, so no
+ * state carries over from one call to the next. */
+int fecl_lte_turbo_decode_noalloc(uint32_t K, int32_t algorithm, uint32_t iterations, const void* llr,
+                                  int32_t llr_dtype, uint64_t nframes, uint8_t* msg, void* stream);
+
 const char* fecl_strerror(int status);
 /* Message of the last failing call on this thread. */
 const char* fecl_last_error(void);
