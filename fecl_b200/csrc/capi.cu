@@ -130,7 +130,8 @@ struct fecl_codec_s {
   std::unique_ptr<fecl::LdpcCode> ldpc;
   std::unique_ptr<fecl::TurboCode> turbo;
   std::mutex mu;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;   // host-memory calls: first pipeline stream
+  cudaStream_t stream2 = nullptr;  // host-memory calls: second pipeline stream
   cudaEvent_t done = nullptr;
   bool pending = false;
   // device description
@@ -145,6 +146,10 @@ struct fecl_codec_s {
     if (stream) {
       cudaStreamSynchronize(stream);
       cudaStreamDestroy(stream);
+    }
+    if (stream2) {
+      cudaStreamSynchronize(stream2);
+      cudaStreamDestroy(stream2);
     }
     if (done) cudaEventDestroy(done);
   }
@@ -162,6 +167,7 @@ struct fecl_codec_s {
     }
     cuda_check(cudaGetDevice(&device), "cudaGetDevice");
     cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "cudaEventCreate");
   }
 
@@ -359,99 +365,62 @@ fecl_codec_s* checked(fecl_codec_t c) {
   return c;
 }
 
-// Runs a decode.  Host-memory calls stage buffers through the workspace on the
-// codec's stream and wait; device-memory calls launch on the caller's stream.
-void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard, int32_t* iters, bool soft,
-                int32_t flags, cudaStream_t user_stream) {
-  c->ensure_device();
-  DeviceGuard dg(c->device);
-  const bool host = (flags == FECL_HOST_MEMORY);
-  if (flags != FECL_HOST_MEMORY && flags != FECL_DEVICE_MEMORY) fail(FECL_EINVAL, "Invalid memory flag");
-  cudaStream_t s = host ? c->stream : user_stream;
-  const size_t isz = dsize(io->in_dtype);
-  const size_t osz = soft ? dsize(io->out_dtype) : 4;
-  const uint64_t P = c->parity(), S = c->syst(), M = c->msg(), X = c->state();
+// Device pointers of one decode launch (inputs, outputs, scratch).
+struct Launch {
+  const void *llr = nullptr, *syst = nullptr, *state = nullptr;
+  uint8_t* hard = nullptr;
+  int32_t* iters = nullptr;
+  void *msg = nullptr, *syst_out = nullptr, *parity_out = nullptr, *state_out = nullptr;
+  char* scratch = nullptr;
+};
 
+// Scratch of the decoder kernels for n frames, with the offsets of its parts.
+struct ScratchPlan {
+  size_t bytes = 0, o1 = 0, o2 = 0, o3 = 0, o4 = 0, o5 = 0;
+};
+
+ScratchPlan plan_scratch(const fecl_codec_s* c, uint64_t n, bool lte_fast) {
   Carver cv;
-  size_t o_llr = 0, o_syst = 0, o_state = 0, o_hard = 0, o_iters = 0, o_msg = 0, o_so = 0, o_po = 0, o_sto = 0;
-  if (host) {
-    o_llr = cv.take(n * P * isz);
-    if (io->syst) o_syst = cv.take(n * S * isz);
-    if (io->state) o_state = cv.take(n * X * isz);
-    if (hard) o_hard = cv.take(n * M);
-    if (iters) o_iters = cv.take(n * 4);
-    if (io->msg) o_msg = cv.take(n * M * osz);
-    if (io->syst_out) o_so = cv.take(n * S * osz);
-    if (io->parity_out) o_po = cv.take(n * P * osz);
-    if (io->state_out) o_sto = cv.take(n * X * osz);
-  }
-  size_t o_s1 = 0, o_s2 = 0, o_s3 = 0, o_s4 = 0, o_s5 = 0;
-  const bool lte_fast = c->kind == 1 && !soft && c->lte_fast_ok();
+  ScratchPlan sp;
+  const uint64_t P = c->parity(), X = c->state();
   if (lte_fast) {
-    o_s1 = cv.take(fecl::turbo_lte_scratch_bytes(int(c->msg()), int64_t(n)));
+    sp.o1 = cv.take(fecl::turbo_lte_scratch_bytes(int(c->msg()), int64_t(n)));
   } else if (c->kind == 0) {
-    o_s1 = cv.take(n * c->ldev.E * 4);
-    o_s2 = cv.take(n * P * 4);
-    o_s3 = cv.take(n * P * 4);
+    sp.o1 = cv.take(n * c->ldev.E * 4);
+    sp.o2 = cv.take(n * P * 4);
+    sp.o3 = cv.take(n * P * 4);
   } else {
-    o_s1 = cv.take(n * P * 4);
-    o_s2 = cv.take(n * P * 4);
-    o_s3 = cv.take(n * X * 4);
-    o_s4 = cv.take(n * X * 4);
-    o_s5 = cv.take(n * uint64_t(c->tdev.max_steps) * c->tdev.max_states * 4);
+    sp.o1 = cv.take(n * P * 4);
+    sp.o2 = cv.take(n * P * 4);
+    sp.o3 = cv.take(n * X * 4);
+    sp.o4 = cv.take(n * X * 4);
+    sp.o5 = cv.take(n * uint64_t(c->tdev.max_steps) * c->tdev.max_states * 4);
   }
-  c->wait_previous(s);
-  if (c->ws.bytes < cv.off) {
-    // the old workspace may still be read by earlier work on other streams
-    if (c->pending) cuda_check(cudaEventSynchronize(c->done), "cudaEventSynchronize");
-    c->ws.reserve(cv.off);
-  }
-  char* base = c->ws.as<char>();
-  auto dptr = [&](size_t off) -> void* { return base + off; };
+  sp.bytes = cv.off;
+  return sp;
+}
 
-  const void* d_llr = io->parity;
-  const void* d_syst = io->syst;
-  const void* d_state = io->state;
-  uint8_t* d_hard = hard;
-  int32_t* d_iters = iters;
-  void *d_msg = io->msg, *d_so = io->syst_out, *d_po = io->parity_out, *d_sto = io->state_out;
-  if (host) {
-    d_llr = dptr(o_llr);
-    cuda_check(cudaMemcpyAsync(dptr(o_llr), io->parity, n * P * isz, cudaMemcpyHostToDevice, s), "copy in");
-    if (io->syst) {
-      d_syst = dptr(o_syst);
-      cuda_check(cudaMemcpyAsync(dptr(o_syst), io->syst, n * S * isz, cudaMemcpyHostToDevice, s), "copy in");
-    }
-    if (io->state) {
-      d_state = dptr(o_state);
-      cuda_check(cudaMemcpyAsync(dptr(o_state), io->state, n * X * isz, cudaMemcpyHostToDevice, s), "copy in");
-    }
-    if (hard) d_hard = static_cast<uint8_t*>(dptr(o_hard));
-    if (iters) d_iters = static_cast<int32_t*>(dptr(o_iters));
-    if (io->msg) d_msg = dptr(o_msg);
-    if (io->syst_out) d_so = dptr(o_so);
-    if (io->parity_out) d_po = dptr(o_po);
-    if (io->state_out) d_sto = dptr(o_sto);
-  }
-
+void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint64_t n, int32_t in_dtype,
+                   int32_t out_dtype, bool soft, bool lte_fast, cudaStream_t s) {
   cudaError_t e;
+  auto at = [&](size_t off) { return d.scratch + off; };
   if (c->kind == 0) {
     fecl::LdpcRun r;
     r.nframes = int64_t(n);
-    r.llr = d_llr;
-    r.llr_dtype = io->in_dtype;
-    r.syst_in = d_syst;
-    r.state_in = d_state;
-    r.hard = d_hard;
-    r.iters = d_iters;
-    r.msg_out = d_msg;
-    r.syst_out = d_so;
-    r.parity_out = d_po;
-    r.state_out = d_sto;
-    r.out_dtype = io->out_dtype;
-    r.c2v = static_cast<float*>(dptr(o_s1));
-    r.app = static_cast<float*>(dptr(o_s2));
-    r.chan = static_cast<float*>(dptr(o_s3));
+    r.llr = d.llr;
+    r.llr_dtype = in_dtype;
+    r.syst_in = d.syst;
+    r.state_in = d.state;
+    r.hard = d.hard;
+    r.iters = d.iters;
+    r.msg_out = d.msg;
+    r.syst_out = d.syst_out;
+    r.parity_out = d.parity_out;
+    r.state_out = d.state_out;
+    r.out_dtype = out_dtype;
+    r.c2v = reinterpret_cast<float*>(at(sp.o1));
+    r.app = reinterpret_cast<float*>(at(sp.o2));
+    r.chan = reinterpret_cast<float*>(at(sp.o3));
     e = fecl::launch_ldpc_flood(c->ldev, r, s);
   } else if (lte_fast) {
     fecl::TurboLteParams r;
@@ -463,14 +432,14 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
     r.perm[0] = c->tdev.c[0].perm;
     r.perm[1] = c->tdev.c[1].perm;
     r.sf = c->tdev.sf;
-    r.llr = d_llr;
-    r.llr_dtype = io->in_dtype;
-    r.hard = d_hard;
-    r.iters = d_iters;
-    r.scratch = static_cast<float*>(dptr(o_s1));
+    r.llr = d.llr;
+    r.llr_dtype = in_dtype;
+    r.hard = d.hard;
+    r.iters = d.iters;
+    r.scratch = reinterpret_cast<float*>(at(sp.o1));
     if (!c->stats.ptr) {
       c->stats.reserve(3 * sizeof(unsigned long long));
-      cuda_check(cudaMemsetAsync(c->stats.ptr, 0, 3 * sizeof(unsigned long long), s), "cudaMemset");
+      cuda_check(cudaMemset(c->stats.ptr, 0, 3 * sizeof(unsigned long long)), "cudaMemset");
     }
     r.stats = c->stats.as<unsigned long long>();
     e = fecl::launch_turbo_lte(r, s);
@@ -478,41 +447,142 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
     fecl::TurboRun r;
     r.nframes = int64_t(n);
     r.soft = soft ? 1 : 0;
-    r.llr = d_llr;
-    r.llr_dtype = io->in_dtype;
-    r.syst_in = d_syst;
-    r.state_in = d_state;
-    r.hard = d_hard;
-    r.iters = d_iters;
-    r.msg_out = d_msg;
-    r.syst_out = d_so;
-    r.parity_out = d_po;
-    r.state_out = d_sto;
-    r.out_dtype = io->out_dtype;
-    r.parity_in = static_cast<float*>(dptr(o_s1));
-    r.parity_buf = static_cast<float*>(dptr(o_s2));
-    r.ext = static_cast<float*>(dptr(o_s3));
-    r.ext_buf = static_cast<float*>(dptr(o_s4));
-    r.alpha = static_cast<float*>(dptr(o_s5));
+    r.llr = d.llr;
+    r.llr_dtype = in_dtype;
+    r.syst_in = d.syst;
+    r.state_in = d.state;
+    r.hard = d.hard;
+    r.iters = d.iters;
+    r.msg_out = d.msg;
+    r.syst_out = d.syst_out;
+    r.parity_out = d.parity_out;
+    r.state_out = d.state_out;
+    r.out_dtype = out_dtype;
+    r.parity_in = reinterpret_cast<float*>(at(sp.o1));
+    r.parity_buf = reinterpret_cast<float*>(at(sp.o2));
+    r.ext = reinterpret_cast<float*>(at(sp.o3));
+    r.ext_buf = reinterpret_cast<float*>(at(sp.o4));
+    r.alpha = reinterpret_cast<float*>(at(sp.o5));
     e = fecl::launch_turbo_generic(c->tdev, r, s);
   }
   if (e == cudaErrorInvalidValue) fail(FECL_EUNSUPPORTED, "code shape not supported by the device decoder");
   cuda_check(e, "kernel launch");
+}
 
-  if (host) {
-    if (hard) cuda_check(cudaMemcpyAsync(hard, d_hard, n * M, cudaMemcpyDeviceToHost, s), "copy out");
-    if (iters) cuda_check(cudaMemcpyAsync(iters, d_iters, n * 4, cudaMemcpyDeviceToHost, s), "copy out");
-    if (io->msg) cuda_check(cudaMemcpyAsync(io->msg, d_msg, n * M * osz, cudaMemcpyDeviceToHost, s), "copy out");
-    if (io->syst_out) cuda_check(cudaMemcpyAsync(io->syst_out, d_so, n * S * osz, cudaMemcpyDeviceToHost, s), "copy out");
-    if (io->parity_out)
-      cuda_check(cudaMemcpyAsync(io->parity_out, d_po, n * P * osz, cudaMemcpyDeviceToHost, s), "copy out");
-    if (io->state_out)
-      cuda_check(cudaMemcpyAsync(io->state_out, d_sto, n * X * osz, cudaMemcpyDeviceToHost, s), "copy out");
-    cuda_check(cudaStreamSynchronize(s), "decode");
-    c->pending = false;
-  } else {
-    c->mark(s);
+// Grows the workspace to `bytes`; the old one may still be read by queued work.
+void reserve_workspace(fecl_codec_s* c, size_t bytes) {
+  if (c->ws.bytes >= bytes) return;
+  if (c->pending) cuda_check(cudaEventSynchronize(c->done), "cudaEventSynchronize");
+  cuda_check(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  cuda_check(cudaStreamSynchronize(c->stream2), "cudaStreamSynchronize");
+  c->ws.reserve(bytes);
+}
+
+// Runs a decode.  Device-memory calls launch on the caller's stream.  Host-memory
+// calls pipeline the batch in chunks over two streams of the codec -- copy in,
+// decode, copy out -- so that the copies of one chunk overlap the decode of the
+// other, and return when every result is on the host.
+void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard, int32_t* iters, bool soft,
+                int32_t flags, cudaStream_t user_stream) {
+  if (flags != FECL_HOST_MEMORY && flags != FECL_DEVICE_MEMORY) fail(FECL_EINVAL, "Invalid memory flag");
+  c->ensure_device();
+  DeviceGuard dg(c->device);
+  const bool host = (flags == FECL_HOST_MEMORY);
+  const size_t isz = dsize(io->in_dtype);
+  const size_t osz = soft ? dsize(io->out_dtype) : 4;
+  const uint64_t P = c->parity(), S = c->syst(), M = c->msg(), X = c->state();
+  const bool lte_fast = c->kind == 1 && !soft && c->lte_fast_ok();
+
+  if (!host) {
+    const ScratchPlan sp = plan_scratch(c, n, lte_fast);
+    c->wait_previous(user_stream);
+    reserve_workspace(c, sp.bytes);
+    Launch d;
+    d.llr = io->parity;
+    d.syst = io->syst;
+    d.state = io->state;
+    d.hard = hard;
+    d.iters = iters;
+    d.msg = io->msg;
+    d.syst_out = io->syst_out;
+    d.parity_out = io->parity_out;
+    d.state_out = io->state_out;
+    d.scratch = c->ws.as<char>();
+    launch_decode(c, d, sp, n, io->in_dtype, io->out_dtype, soft, lte_fast, user_stream);
+    c->mark(user_stream);
+    return;
   }
+
+  // Chunks of at least kMinChunk frames, at most 4 chunks per call.
+  constexpr uint64_t kMinChunk = 128;
+  const uint64_t nchunks = std::max<uint64_t>(1, std::min<uint64_t>(4, n / kMinChunk));
+  const uint64_t chunk = (n + nchunks - 1) / nchunks;
+  const int nslots = nchunks > 1 ? 2 : 1;
+  Carver cv;
+  const size_t o_llr = cv.take(chunk * P * isz);
+  const size_t o_syst = io->syst ? cv.take(chunk * S * isz) : 0;
+  const size_t o_state = io->state ? cv.take(chunk * X * isz) : 0;
+  const size_t o_hard = hard ? cv.take(chunk * M) : 0;
+  const size_t o_iters = iters ? cv.take(chunk * 4) : 0;
+  const size_t o_msg = io->msg ? cv.take(chunk * M * osz) : 0;
+  const size_t o_so = io->syst_out ? cv.take(chunk * S * osz) : 0;
+  const size_t o_po = io->parity_out ? cv.take(chunk * P * osz) : 0;
+  const size_t o_sto = io->state_out ? cv.take(chunk * X * osz) : 0;
+  const ScratchPlan sp = plan_scratch(c, chunk, lte_fast);
+  const size_t o_scr = cv.take(sp.bytes);
+  const size_t slot_bytes = cv.off;
+  if (c->pending) {
+    cuda_check(cudaStreamWaitEvent(c->stream, c->done, 0), "cudaStreamWaitEvent");
+    cuda_check(cudaStreamWaitEvent(c->stream2, c->done, 0), "cudaStreamWaitEvent");
+  }
+  reserve_workspace(c, slot_bytes * nslots);
+  const char* hp = static_cast<const char*>(io->parity);
+  for (uint64_t k = 0; k < nchunks; ++k) {
+    const uint64_t f0 = k * chunk;
+    if (f0 >= n) break;
+    const uint64_t nk = std::min(chunk, n - f0);
+    const int slot = int(k % nslots);
+    cudaStream_t st = slot == 0 ? c->stream : c->stream2;
+    char* base = c->ws.as<char>() + slot * slot_bytes;
+    Launch d;
+    cuda_check(cudaMemcpyAsync(base + o_llr, hp + f0 * P * isz, nk * P * isz, cudaMemcpyHostToDevice, st), "copy in");
+    d.llr = base + o_llr;
+    if (io->syst) {
+      cuda_check(cudaMemcpyAsync(base + o_syst, static_cast<const char*>(io->syst) + f0 * S * isz, nk * S * isz,
+                                 cudaMemcpyHostToDevice, st), "copy in");
+      d.syst = base + o_syst;
+    }
+    if (io->state) {
+      cuda_check(cudaMemcpyAsync(base + o_state, static_cast<const char*>(io->state) + f0 * X * isz, nk * X * isz,
+                                 cudaMemcpyHostToDevice, st), "copy in");
+      d.state = base + o_state;
+    }
+    if (hard) d.hard = reinterpret_cast<uint8_t*>(base + o_hard);
+    if (iters) d.iters = reinterpret_cast<int32_t*>(base + o_iters);
+    if (io->msg) d.msg = base + o_msg;
+    if (io->syst_out) d.syst_out = base + o_so;
+    if (io->parity_out) d.parity_out = base + o_po;
+    if (io->state_out) d.state_out = base + o_sto;
+    d.scratch = base + o_scr;
+    launch_decode(c, d, sp, nk, io->in_dtype, io->out_dtype, soft, lte_fast, st);
+    if (hard) cuda_check(cudaMemcpyAsync(hard + f0 * M, d.hard, nk * M, cudaMemcpyDeviceToHost, st), "copy out");
+    if (iters) cuda_check(cudaMemcpyAsync(iters + f0, d.iters, nk * 4, cudaMemcpyDeviceToHost, st), "copy out");
+    if (io->msg)
+      cuda_check(cudaMemcpyAsync(static_cast<char*>(io->msg) + f0 * M * osz, d.msg, nk * M * osz,
+                                 cudaMemcpyDeviceToHost, st), "copy out");
+    if (io->syst_out)
+      cuda_check(cudaMemcpyAsync(static_cast<char*>(io->syst_out) + f0 * S * osz, d.syst_out, nk * S * osz,
+                                 cudaMemcpyDeviceToHost, st), "copy out");
+    if (io->parity_out)
+      cuda_check(cudaMemcpyAsync(static_cast<char*>(io->parity_out) + f0 * P * osz, d.parity_out, nk * P * osz,
+                                 cudaMemcpyDeviceToHost, st), "copy out");
+    if (io->state_out)
+      cuda_check(cudaMemcpyAsync(static_cast<char*>(io->state_out) + f0 * X * osz, d.state_out, nk * X * osz,
+                                 cudaMemcpyDeviceToHost, st), "copy out");
+  }
+  cuda_check(cudaStreamSynchronize(c->stream), "decode");
+  cuda_check(cudaStreamSynchronize(c->stream2), "decode");
+  c->pending = false;
 }
 
 }  // namespace
