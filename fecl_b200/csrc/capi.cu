@@ -269,6 +269,18 @@ struct fecl_codec_s {
   int lte_train = -1;
   bool force_generic = false;
   DeviceBuffer stats;  // windowed turbo counters
+  // The lane-batched LDPC kernel needs check degrees <= 32 and, unless the iteration
+  // count is fixed, a scaling that does not change across iterations (its stop test
+  // runs inside the check update of the next iteration).
+  bool ldpc_lanes_ok() const {
+    if (kind != 0 || force_generic) return false;
+    if (ldpc->max_check_degree() > 32) return false;
+    const auto& d = ldpc->decoder();
+    if (d.fixed_iterations) return true;
+    for (const auto& row : d.scaling)
+      if (row != d.scaling[0]) return false;
+    return true;
+  }
   // The windowed kernel covers the LTE RSC pair with serial scheduling and FP32 messages
   // for any K whose two exchange arrays fit in shared memory.
   bool lte_fast_ok() const {
@@ -383,7 +395,9 @@ ScratchPlan plan_scratch(const fecl_codec_s* c, uint64_t n, bool lte_fast) {
   Carver cv;
   ScratchPlan sp;
   const uint64_t P = c->parity(), X = c->state();
-  if (lte_fast) {
+  if (c->kind == 0 && c->ldpc_lanes_ok()) {
+    sp.o1 = cv.take(fecl::ldpc_lanes_scratch_bytes(int64_t(P), int64_t(X), int64_t(n), c->ldpc->decoder().precision));
+  } else if (lte_fast) {
     sp.o1 = cv.take(fecl::turbo_lte_scratch_bytes(int(c->msg()), int64_t(n)));
   } else if (c->kind == 0) {
     sp.o1 = cv.take(n * c->ldev.E * 4);
@@ -404,7 +418,41 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
                    int32_t out_dtype, bool soft, bool lte_fast, cudaStream_t s) {
   cudaError_t e;
   auto at = [&](size_t off) { return d.scratch + off; };
-  if (c->kind == 0) {
+  if (c->kind == 0 && c->ldpc_lanes_ok()) {
+    fecl::LdpcLanesParams r;
+    const auto& L = c->ldev;
+    r.M = L.M;
+    r.N = L.N;
+    r.msg = L.msg;
+    r.d_max = L.d_max;
+    r.E = L.E;
+    r.row_ptr = L.row_ptr;
+    r.col_idx = L.col_idx;
+    r.col_ptr = L.col_ptr;
+    r.col_edges = L.col_edges;
+    r.sf = L.sf;
+    r.n_sf = L.n_sf;
+    r.sf_stride = L.sf_stride;
+    r.algorithm = L.algorithm;
+    r.iterations = L.iterations;
+    r.fixed_iterations = L.fixed_iterations;
+    r.msg_type = c->ldpc->decoder().precision;
+    r.nframes = int64_t(n);
+    r.llr = d.llr;
+    r.llr_dtype = in_dtype;
+    r.syst_in = d.syst;
+    r.state_in = d.state;
+    r.hard = d.hard;
+    r.iters = d.iters;
+    r.msg_out = d.msg;
+    r.syst_out = d.syst_out;
+    r.parity_out = d.parity_out;
+    r.state_out = d.state_out;
+    r.out_dtype = out_dtype;
+    e = fecl::launch_ldpc_lanes(r, at(sp.o1), s);
+  } else if (c->kind == 0) {
+    if (c->ldpc->decoder().precision != 0)
+      fail(FECL_EUNSUPPORTED, "FP16 / int8 messages need check degrees <= 32 and a scaling constant across iterations");
     fecl::LdpcRun r;
     r.nframes = int64_t(n);
     r.llr = d.llr;

@@ -46,6 +46,45 @@ struct LdpcRun {
 
 cudaError_t launch_ldpc_flood(const LdpcDeviceCode& code, const LdpcRun& run, cudaStream_t stream);
 
+// Batched decoder with 32 frames per warp (one per lane), lane-minor scratch.
+struct LdpcLanesParams {
+  // code
+  int32_t M = 0, N = 0, msg = 0, d_max = 0;
+  int64_t E = 0;
+  const uint32_t* row_ptr = nullptr;
+  const uint32_t* col_idx = nullptr;
+  const uint32_t* col_ptr = nullptr;
+  const uint32_t* col_edges = nullptr;
+  const float* sf = nullptr;
+  int32_t n_sf = 1, sf_stride = 1;
+  int32_t algorithm = 2, iterations = 1, fixed_iterations = 0;
+  int32_t msg_type = 0;  // 0 FP32, 1 FP16, 2 saturated int8 (Q5.2)
+  // batch, frame-major caller buffers
+  int64_t nframes = 0;
+  const void* llr = nullptr;
+  int32_t llr_dtype = 1;
+  const void* syst_in = nullptr;
+  const void* state_in = nullptr;
+  uint8_t* hard = nullptr;
+  int32_t* iters = nullptr;
+  void* msg_out = nullptr;
+  void* syst_out = nullptr;
+  void* parity_out = nullptr;
+  void* state_out = nullptr;
+  int32_t out_dtype = 1;
+  // filled by the launcher from the scratch buffer
+  int32_t groups = 0;
+  float* chan = nullptr;
+  float* app = nullptr;
+  void* c2v = nullptr;
+  uint32_t* active = nullptr;
+  uint32_t* fail = nullptr;
+  int32_t* iters_ws = nullptr;
+};
+
+size_t ldpc_lanes_scratch_bytes(int64_t N, int64_t E, int64_t nframes, int msg_type);
+cudaError_t launch_ldpc_lanes(LdpcLanesParams p, void* scratch, cudaStream_t stream);
+
 // ---- Turbo ---------------------------------------------------------------
 
 constexpr int kMaxConstituents = 8;
