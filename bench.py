@@ -199,18 +199,229 @@ def run_reference_arm(args):
     return 0
 
 
+# ---- LDPC workloads (--workload ldpc-short | ldpc-normal) ----------------------------
+
+LDPC_WORKLOADS = {
+    # DVB-S2 short frame, nominal rate 1/2 (K = 7200), Exact BP, at most 20 iterations
+    # with the syndrome stop, FP64 L-values; outputs hard bits and a-posteriori L-values.
+    "ldpc-short": {"codes": [(16200, (1, 2), 64, 1.5)], "algorithm": "Exact", "iterations": 20, "scaling": 1.0,
+                   "llr": "f64", "soft": True,
+                   "text": "DVB-S2 short n=16200 r=1/2 x 64 frames, Exact BP, <=20 iterations with syndrome stop, "
+                           "Eb/N0 1.5 dB, FP64 L-values, hard bits + a-posteriori L-values"},
+    # DVB-S2 normal frames at rates 1/2, 3/4, 9/10, 512 frames each, normalised min-sum
+    # (0.75), at most 50 iterations; message storage set by --precision.
+    "ldpc-normal": {"codes": [(64800, (1, 2), 512, 1.5), (64800, (3, 4), 512, 2.75), (64800, (9, 10), 512, 3.75)],
+                    "algorithm": "Approximate", "iterations": 50, "scaling": 0.75, "llr": "f32", "soft": False,
+                    "text": "DVB-S2 normal n=64800 r=1/2, 3/4, 9/10 x 512 frames each (Eb/N0 1.5, 2.75, 3.75 dB), "
+                            "normalised min-sum 0.75, <=50 iterations with syndrome stop, FP32 L-values"},
+}
+PRECISIONS = {"f32": 0, "f16": 1, "i8": 2}
+
+
+def ldpc_algorithmic_bytes(N, E, K, iterations_run, s_llr, s_msg, soft):
+    """Flooding BP with message state in memory: the L-values once; per iteration each
+    check-to-bit message read and written once and each bit posterior read and written
+    once (FP32); the decoded bits (or a-posteriori values) once."""
+    return N * s_llr + iterations_run * (2 * E * s_msg + 2 * N * 4) + (K * 8 if soft else K)
+
+
+def run_ldpc(args):
+    import numpy as np
+    import torch
+    from fractions import Fraction
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+
+    w = LDPC_WORKLOADS[args.workload]
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    prec = PRECISIONS[args.precision]
+    np_llr = {"f64": np.float64, "f32": np.float32, "f16": np.float16}[w["llr"]]
+    alg = getattr(F, w["algorithm"])
+    jobs = []
+    for n, (num, den), frames, ebn0 in w["codes"]:
+        frames = args.frames or frames
+        H = F.Ldpc.DvbS2.matrix(n, Fraction(num, den))
+        code = F.Ldpc(F.Ldpc.EncoderOptions(H), F.Ldpc.DecoderOptions().algorithm(alg).iterations(w["iterations"])
+                      .scalingFactor(w["scaling"]).precision(prec))
+        Kc, Nc = code.msgSize(), code.paritySize()
+        msg = ch.random_bits(frames * Kc, SEED + rank)
+        llr = ch.awgn_llr(code.encode(msg), ebn0, Kc / Nc, SEED + rank, np_llr)
+        d_llr = torch.from_numpy(llr).cuda()
+        out = torch.empty(frames * Kc, dtype=torch.float64 if w["soft"] else torch.uint8, device="cuda")
+        jobs.append({"H": H, "code": code, "K": Kc, "N": Nc, "E": code.stateSize(), "frames": frames, "msg": msg,
+                     "llr": llr, "d_llr": d_llr, "out": out, "rate": "%d/%d" % (num, den), "ebn0": ebn0})
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step(j, host=False):
+        src = j["h_llr"] if host else j["d_llr"]
+        dst = j["h_out"] if host else j["out"]
+        if w["soft"]:
+            j["code"].soDecode(F.Codec.Input().parity(src), F.Codec.Output().msg(), out={"msg": dst})
+        else:
+            j["code"].decode(src, out=dst)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    if args.profile_decodes:
+        for _ in range(args.profile_decodes):
+            for j in jobs:
+                step(j)
+        torch.cuda.synchronize()
+        return 0
+    for _ in range(max(args.warmup, 3)):
+        for j in jobs:
+            step(j)
+    barrier()
+    times = []
+    with ClockSampler(local) as clk:
+        barrier()
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for j in jobs:
+                step(j)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        barrier()
+    clocks = clk.summary()
+    ms = statistics.mean(times)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    info_bits = sum(j["frames"] * j["K"] for j in jobs)
+    value = world * info_bits / (ms * 1e-3) / 1e6
+
+    # per-code FER and iterations, and the algorithmic bytes of one step
+    alg_bytes = 0
+    per_code = []
+    s_llr = np.dtype(np_llr).itemsize
+    s_msg = {0: 4, 1: 2, 2: 1}[prec]
+    for j in jobs:
+        bits, its = j["code"].decode(j["d_llr"], iterations=True)
+        bits = bits.cpu().numpy().reshape(j["frames"], j["K"])
+        its = its.cpu().numpy()
+        fer = float(np.mean(np.any(bits != j["msg"].reshape(j["frames"], j["K"]), axis=1)))
+        alg_bytes += j["frames"] * (j["N"] * s_llr + (j["K"] * 8 if w["soft"] else j["K"])) + \
+            int(its.sum()) * (2 * j["E"] * s_msg + 2 * j["N"] * 4)
+        per_code.append({"n": j["N"], "rate": j["rate"], "frames": j["frames"], "ebn0_db": j["ebn0"], "fer": fer,
+                         "iterations_mean": round(float(its.mean()), 2), "iterations_max": int(its.max())})
+        j["bits"] = bits
+
+    # end to end with pinned host buffers
+    for j in jobs:
+        j["h_llr"] = torch.from_numpy(j["llr"]).pin_memory()
+        j["h_out"] = torch.empty(j["out"].shape, dtype=j["out"].dtype).pin_memory()
+        step(j, host=True)
+    e2e = []
+    barrier()
+    for _ in range(max(2, args.steps // 2)):
+        t0 = time.perf_counter()
+        for j in jobs:
+            step(j, host=True)
+        e2e.append(time.perf_counter() - t0)
+    barrier()
+    e2e_s = statistics.mean(e2e)
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "Mbit/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {0: "f32", 1: "f16", 2: "i8"}[prec], "data": "synthetic",
+        "config": {"workload": w["text"], "message_storage": args.precision, "codes": per_code,
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": "frame shards, replicas per GPU" if world > 1 else "single GPU"},
+        "latency_ms": {"p50": round(statistics.median(times), 4),
+                       "p99": round(sorted(times)[min(len(times) - 1, int(0.99 * len(times)))], 4)},
+        "e2e": {"value": round(world * info_bits / e2e_s / 1e6, 2), "unit": "Mbit/s",
+                "h2d_bytes_per_step": int(sum(j["llr"].nbytes for j in jobs)),
+                "d2h_bytes_per_step": int(sum(j["out"].numel() * j["out"].element_size() for j in jobs))},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                     "kernel": "lane-batched BP (check, bit and update kernels) per step",
+                     "algorithmic_bytes_per_step": int(alg_bytes)},
+        "gpu_launches": None,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"], line["matched_hard_decisions_vs_reference"] = ldpc_cpu_reference(w, jobs)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def ldpc_cpu_reference(w, jobs, sample_frames=16):
+    """The reference BP decoder (oracle/_ref, else the C restatement) on the first
+    `sample_frames` frames of each code of the workload, all host threads."""
+    import numpy as np
+    import fecl_b200 as F
+    from oracle import ref
+    cores = os.cpu_count() or 1
+    alg = getattr(F, w["algorithm"])
+    total_bits, total_s, match = 0, 0.0, True
+    kind = "reference" if ref.available() else "port"
+    for j in jobs:
+        n = min(sample_frames, j["frames"])
+        x = np.ascontiguousarray(j["llr"][: n * j["N"]], dtype=np.float64)
+        H = j["H"]
+        if kind == "reference":
+            rc = ref.RefCodec.ldpc(H.rows(), H.cols(), H.row_ptr, H.col_idx, alg, w["iterations"], (w["scaling"],),
+                                   workgroup=cores)
+            t = time.perf_counter()
+            bits = rc.decode(x)
+            total_s += time.perf_counter() - t
+        else:
+            from oracle import restated
+            t = time.perf_counter()
+            bits, _ = restated.ldpc_decode(H, alg, w["iterations"], w["scaling"], x, threads=cores)
+            total_s += time.perf_counter() - t
+        total_bits += n * j["K"]
+        match = match and bool(np.array_equal(np.asarray(bits).ravel(), j["bits"][:n].ravel()))
+    return ({"value": total_bits / total_s / 1e6, "unit": "Mbit/s", "cores": cores, "kind": kind,
+             "sample": "first %d frames of each code, one decode each, %d threads, %.2f s wall"
+                       % (sample_frames, cores, total_s)}, match)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="lte-turbo", choices=["lte-turbo"] + sorted(LDPC_WORKLOADS),
+                    help="lte-turbo is the headline workload; the LDPC workloads print the same line for BP")
+    ap.add_argument("--frames", type=int, default=0,
+                    help="LDPC workloads: frames per code instead of the workload's (small cases for ncu)")
+    ap.add_argument("--precision", default="f32", choices=sorted(PRECISIONS),
+                    help="LDPC message storage (f32 is the reference-parity mode)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-decodes", type=int, default=0,
                     help="only run this many decodes of the workload (for ncu captures) and exit")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload in LDPC_WORKLOADS:
+        return run_ldpc(args)
 
     import numpy as np
     import torch

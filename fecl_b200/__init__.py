@@ -133,6 +133,12 @@ def _is_device(x):
     return hasattr(x, "is_cuda") and x.is_cuda
 
 
+def _contiguous(x):
+    if hasattr(x, "is_contiguous"):
+        return x.is_contiguous()
+    return np.asarray(x).flags["C_CONTIGUOUS"]
+
+
 def _dtype_code(a):
     if hasattr(a, "data_ptr"):
         import torch
@@ -299,8 +305,10 @@ class Codec:
                               _lib.HOST_MEMORY, None))
         return (msg, it) if iterations else msg
 
-    def soDecode(self, input, output):
-        """Codec::soDecode -- src/Codec.h:249-307."""
+    def soDecode(self, input, output, out=None):
+        """Codec::soDecode -- src/Codec.h:249-307.  `out` optionally maps output names
+        to preallocated buffers (numpy arrays or torch tensors in the input's kind of
+        memory, of the output dtype and size) that receive them."""
         v = input._v
         if "parity" not in v:
             raise ValueError("Input must contains parity")
@@ -322,7 +330,8 @@ class Codec:
             dt = par.dtype
             ins = {k: v[k].contiguous().view(-1).to(dt) for k in ("parity", "syst", "state") if k in v}
             odt = torch.float64 if output.dtype == np.float64 else torch.float32
-            outs = {k: torch.empty(n * sizes[k], dtype=odt, device=par.device) for k in output._want}
+            outs = {k: torch.empty(n * sizes[k], dtype=odt, device=par.device) for k in output._want
+                    if not (out and k in out)}
             ptr = lambda t: t.data_ptr()
             flags = _lib.DEVICE_MEMORY
             stream = C.c_void_p(torch.cuda.current_stream(par.device).cuda_stream)
@@ -332,12 +341,19 @@ class Codec:
             dt = x.dtype if x.dtype in (np.float64, np.float32, np.float16) else np.float64
             ins = {k: np.ascontiguousarray(np.asarray(v[k], dtype=dt).ravel()) for k in ("parity", "syst", "state") if k in v}
             odt = np.float64 if output.dtype == np.float64 else np.float32
-            outs = {k: np.zeros(n * sizes[k], dtype=odt) for k in output._want}
-            ptr = lambda a: a.ctypes.data
+            outs = {k: np.zeros(n * sizes[k], dtype=odt) for k in output._want if not (out and k in out)}
+            ptr = lambda a: a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
             flags = _lib.HOST_MEMORY
             stream = None
             io.in_dtype = _dtype_code(ins["parity"])
         io.out_dtype = _lib.F64 if output.dtype == np.float64 else _lib.F32
+        for k in output._want:
+            if out and k in out:
+                t = out[k]
+                nbytes = t.numel() * t.element_size() if hasattr(t, "data_ptr") else np.asarray(t).nbytes
+                if nbytes != n * sizes[k] * (8 if io.out_dtype == _lib.F64 else 4) or not _contiguous(t):
+                    raise ValueError("Invalid size for " + k)
+                outs[k] = t
         for k, t in ins.items():
             setattr(io, k, ptr(t))
             keep.append(t)
