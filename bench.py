@@ -249,6 +249,11 @@ def run_ldpc(args):
         H = F.Ldpc.DvbS2.matrix(n, Fraction(num, den))
         code = F.Ldpc(F.Ldpc.EncoderOptions(H), F.Ldpc.DecoderOptions().algorithm(alg).iterations(w["iterations"])
                       .scalingFactor(w["scaling"]).precision(prec))
+        code.setKernel(args.kernel)
+        if args.cluster or args.threads:
+            code.setClusterShape(args.cluster, args.threads)
+        if args.wave:
+            code.setWave(args.wave)
         Kc, Nc = code.msgSize(), code.paritySize()
         msg = ch.random_bits(frames * Kc, SEED + rank)
         llr = ch.awgn_llr(code.encode(msg), ebn0, Kc / Nc, SEED + rank, np_llr)
@@ -345,7 +350,7 @@ def run_ldpc(args):
         "metric": METRIC, "value": round(value, 2), "unit": "Mbit/s", "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": {0: "f32", 1: "f16", 2: "i8"}[prec], "data": "synthetic",
-        "config": {"workload": w["text"], "message_storage": args.precision, "codes": per_code,
+        "config": {"workload": w["text"], "message_storage": args.precision, "kernel": args.kernel, "codes": per_code,
                    "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": "frame shards, replicas per GPU" if world > 1 else "single GPU"},
         "latency_ms": {"p50": round(statistics.median(times), 4),
@@ -355,7 +360,9 @@ def run_ldpc(args):
                 "d2h_bytes_per_step": int(sum(j["out"].numel() * j["out"].element_size() for j in jobs))},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
-                     "kernel": "lane-batched BP (check, bit and update kernels) per step",
+                     "kernel": {"auto": "lane-batched BP (check and bit kernels) per step",
+                                "cluster": "cluster-resident BP (ldpc_cluster_kernel) per step",
+                                "lanes": "lane-batched BP (check and bit kernels) per step"}[args.kernel],
                      "algorithmic_bytes_per_step": int(alg_bytes)},
         "gpu_launches": None,
         "clocks": clocks,
@@ -414,6 +421,11 @@ def main():
                     help="LDPC workloads: frames per code instead of the workload's (small cases for ncu)")
     ap.add_argument("--precision", default="f32", choices=sorted(PRECISIONS),
                     help="LDPC message storage (f32 is the reference-parity mode)")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "cluster", "lanes"],
+                    help="LDPC workloads: decoder kernel (auto: the lane-batched one where it applies)")
+    ap.add_argument("--cluster", type=int, default=0, help="LDPC: CTAs per frame of the cluster kernel (0: built-in)")
+    ap.add_argument("--threads", type=int, default=0, help="LDPC: threads per CTA of the cluster kernel (0: built-in)")
+    ap.add_argument("--wave", type=int, default=0, help="LDPC: frame groups of 32 decoded together (0: built-in)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-decodes", type=int, default=0,
                     help="only run this many decodes of the workload (for ncu captures) and exit")

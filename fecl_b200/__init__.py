@@ -232,9 +232,14 @@ class Codec:
         return self._sizes[3]
 
     def setKernel(self, kernel):
-        """Extension: 'auto' (fastest kernel for the code) or 'generic' (the kernels that
-        walk the reference's operation order in FP32)."""
-        _check(_L.fecl_set_kernel(self._h, {"auto": _lib.KERNEL_AUTO, "generic": _lib.KERNEL_GENERIC}[kernel]))
+        """Extension: 'auto' (fastest kernel for the code), 'generic' (the kernels that
+        walk the reference's operation order in FP32), and for LDPC 'lanes' (32 frames
+        per warp, messages in device memory) or 'cluster' (each frame's messages in the
+        shared memory of a thread-block cluster)."""
+        sel = {"auto": 0, "generic": 1, "lanes": 2, "cluster": 3}
+        if kernel not in sel:
+            raise ValueError("Invalid kernel selection")
+        _check(_L.fecl_set_kernel(self._h, sel[kernel]))
 
     # Codec::getWorkGroupSize / setWorkGroupSize (src/Codec.h:65-66): a CPU thread count
     # in the reference; kept for API compatibility, the device decoder ignores it.
@@ -504,6 +509,18 @@ class Ldpc(Codec):
 
     def getDecoderOptions(self):
         return self._decoder
+
+    def setClusterShape(self, cluster=0, threads=0):
+        """Extension: CTAs per frame (1, 2, 4, 8, 16) and threads per CTA (256, 512,
+        1024) of the cluster-resident decoder; 0 restores the built-in choice."""
+        _check(_L.fecl_ldpc_set_cluster_shape(self._h, int(cluster), int(threads)))
+        return self
+
+    def setWave(self, groups=0):
+        """Extension: frame groups of 32 the lane-batched decoder runs together through
+        every iteration (0 restores the built-in choice)."""
+        _check(_L.fecl_ldpc_set_wave(self._h, int(groups)))
+        return self
 
     def checks(self):
         """The transformed check matrix (detail::Ldpc::Structure::checks); its edge

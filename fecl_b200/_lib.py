@@ -87,6 +87,8 @@ SIGNATURES = [
     ("fecl_so_decode", C.c_int, [C.c_void_p, C.POINTER(fecl_so_io), C.c_uint64, C.c_int32, C.c_void_p]),
     ("fecl_destroy", None, [C.c_void_p]),
     ("fecl_set_kernel", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fecl_ldpc_set_cluster_shape", C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    ("fecl_ldpc_set_wave", C.c_int, [C.c_void_p, C.c_int32]),
     ("fecl_turbo_set_window_training", C.c_int, [C.c_void_p, C.c_int32]),
     ("fecl_turbo_window_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("fecl_lte_turbo_decode_noalloc", C.c_int, [C.c_uint32, C.c_int32, C.c_uint32, C.c_void_p, C.c_int32, C.c_uint64, C.c_void_p, C.c_void_p]),

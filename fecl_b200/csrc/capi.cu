@@ -9,6 +9,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -17,6 +18,7 @@
 #include "../../include/fecl_b200.h"
 #include "device/kernels.hpp"
 #include "host/codes.hpp"
+#include "host/ldpc_plan.hpp"
 
 namespace {
 
@@ -169,6 +171,8 @@ struct fecl_codec_s {
     cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "cudaEventCreate");
+    cuda_check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attribute");
+    cuda_check(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device), "attribute");
   }
 
   void upload_ldpc() {
@@ -267,13 +271,79 @@ struct fecl_codec_s {
 
   bool on_device = false;
   int lte_train = -1;
-  bool force_generic = false;
+  int kernel_sel = FECL_KERNEL_AUTO;
+  bool force_generic_() const { return kernel_sel == FECL_KERNEL_GENERIC; }
+
+  // Cluster-resident LDPC decoder: partition tables per cluster size, uploaded on use.
+  struct ClusterDev {
+    fecl::LdpcClusterPlan plan;
+    bool uploaded = false;
+    DeviceBuffer row_split, bit_split, chk_addr, bit_ptr, bit_addr;
+    std::map<int, int> max_active;  // threads -> resident clusters
+  };
+  std::map<uint32_t, std::unique_ptr<ClusterDev>> cplans;
+  int cluster_size_sel = 0, cluster_threads_sel = 0;  // 0: chosen by the heuristic
+  int lanes_wave = 0;                                 // 0: chosen by the launcher
+  int smem_optin = 0, sm_count = 0;
+
+  ClusterDev& cluster_plan(uint32_t C) {
+    auto& slot = cplans[C];
+    if (!slot) {
+      slot.reset(new ClusterDev);
+      slot->plan = fecl::build_ldpc_cluster_plan(ldpc->checks(), C);
+    }
+    return *slot;
+  }
+  size_t cluster_smem(uint32_t C) {
+    auto& d = cluster_plan(C);
+    return fecl::ldpc_cluster_smem_bytes(int64_t(d.plan.max_edges), int64_t(d.plan.max_bits), ldpc->decoder().precision);
+  }
+  // Shape of the cluster decoder for a batch of n frames: the cluster size and the
+  // threads per CTA, or false when the code's messages do not fit a cluster.  The
+  // smallest cluster whose shares fit in shared memory is doubled while the batch
+  // would leave more than half of the SMs idle (up to 8 CTAs).
+  bool ldpc_cluster_shape(uint64_t n, uint32_t* C_out, int* threads_out) {
+    if (kind != 0 || kernel_sel == FECL_KERNEL_GENERIC || kernel_sel == FECL_KERNEL_LANES) return false;
+    if (ldpc->max_check_degree() > 32) return false;
+    const size_t limit = size_t(smem_optin) - 1024;  // static shared memory of the kernel
+    uint32_t C = 0;
+    for (uint32_t c = 1; c <= 16; c *= 2) {
+      if (cluster_size_sel && c != uint32_t(cluster_size_sel)) continue;
+      try {
+        if (cluster_smem(c) <= limit) {
+          C = c;
+          break;
+        }
+      } catch (const std::invalid_argument&) {
+        return false;
+      }
+    }
+    if (C == 0) return false;
+    if (!cluster_size_sel)
+      while (C < 8 && n * C * 2 <= uint64_t(sm_count) && cluster_smem(C * 2) <= limit) C *= 2;
+    int threads = cluster_threads_sel;
+    if (!threads) threads = ldpc->max_check_degree() <= 16 ? 1024 : 512;
+    if ((threads == 1024 && ldpc->max_check_degree() > 16) || (threads == 256 && ldpc->max_check_degree() <= 16))
+      threads = 512;
+    *C_out = C;
+    *threads_out = threads;
+    return true;
+  }
+  void upload_cluster(ClusterDev& d) {
+    if (d.uploaded) return;
+    d.row_split.upload(d.plan.row_split);
+    d.bit_split.upload(d.plan.bit_split);
+    d.chk_addr.upload(d.plan.chk_addr);
+    d.bit_ptr.upload(d.plan.bit_ptr);
+    d.bit_addr.upload(d.plan.bit_addr);
+    d.uploaded = true;
+  }
   DeviceBuffer stats;  // windowed turbo counters
   // The lane-batched LDPC kernel needs check degrees <= 32 and, unless the iteration
   // count is fixed, a scaling that does not change across iterations (its stop test
   // runs inside the check update of the next iteration).
   bool ldpc_lanes_ok() const {
-    if (kind != 0 || force_generic) return false;
+    if (kind != 0 || force_generic_()) return false;
     if (ldpc->max_check_degree() > 32) return false;
     const auto& d = ldpc->decoder();
     if (d.fixed_iterations) return true;
@@ -284,7 +354,7 @@ struct fecl_codec_s {
   // The windowed kernel covers the LTE RSC pair with serial scheduling and FP32 messages
   // for any K whose two exchange arrays fit in shared memory.
   bool lte_fast_ok() const {
-    if (force_generic || kind != 1 || !turbo->is_lte_shape()) return false;
+    if (force_generic_() || kind != 1 || !turbo->is_lte_shape()) return false;
     const auto& d = turbo->decoder();
     if (d.scheduling != 0 || d.precision != 0 || d.iterations == 0) return false;
     static const fecl::Trellis lte = fecl::lte_trellis();
@@ -389,12 +459,43 @@ struct Launch {
 // Scratch of the decoder kernels for n frames, with the offsets of its parts.
 struct ScratchPlan {
   size_t bytes = 0, o1 = 0, o2 = 0, o3 = 0, o4 = 0, o5 = 0;
+  uint32_t cluster = 0;  // > 0: the cluster-resident LDPC decoder with this many CTAs per frame
+  int threads = 0, clusters = 0;
 };
 
-ScratchPlan plan_scratch(const fecl_codec_s* c, uint64_t n, bool lte_fast) {
+ScratchPlan plan_scratch(fecl_codec_s* c, uint64_t n, bool lte_fast) {
   Carver cv;
   ScratchPlan sp;
   const uint64_t P = c->parity(), X = c->state();
+  uint32_t C = 0;
+  int threads = 0;
+  // LDPC kernel choice under FECL_KERNEL_AUTO: the lane-batched decoder where it
+  // applies, else the cluster-resident one where the code fits, else the generic one.
+  const bool want_cluster = c->kind == 0 && (c->kernel_sel == FECL_KERNEL_CLUSTER ||
+                                             (c->kernel_sel == FECL_KERNEL_AUTO && !c->ldpc_lanes_ok()));
+  if (want_cluster && c->ldpc_cluster_shape(n, &C, &threads)) {
+    auto& d = c->cluster_plan(C);
+    auto it = d.max_active.find(threads);
+    if (it == d.max_active.end()) {
+      fecl::LdpcClusterParams q;
+      q.cluster = int32_t(C);
+      q.threads = threads;
+      q.max_edges = int64_t(d.plan.max_edges);
+      q.max_bits = int64_t(d.plan.max_bits);
+      q.msg_type = c->ldpc->decoder().precision;
+      it = d.max_active.emplace(threads, fecl::ldpc_cluster_max_active(q)).first;
+    }
+    if (it->second > 0) {
+      sp.cluster = C;
+      sp.threads = threads;
+      sp.clusters = it->second;
+      sp.o1 = cv.take(256);  // frame counter
+      sp.bytes = cv.off;
+      return sp;
+    }
+  }
+  if (c->kind == 0 && c->kernel_sel == FECL_KERNEL_CLUSTER)
+    fail(FECL_EUNSUPPORTED, "the code's messages do not fit a thread-block cluster");
   if (c->kind == 0 && c->ldpc_lanes_ok()) {
     sp.o1 = cv.take(fecl::ldpc_lanes_scratch_bytes(int64_t(P), int64_t(X), int64_t(n), c->ldpc->decoder().precision));
   } else if (lte_fast) {
@@ -418,7 +519,52 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
                    int32_t out_dtype, bool soft, bool lte_fast, cudaStream_t s) {
   cudaError_t e;
   auto at = [&](size_t off) { return d.scratch + off; };
-  if (c->kind == 0 && c->ldpc_lanes_ok()) {
+  if (c->kind == 0 && sp.cluster) {
+    auto& cd = c->cluster_plan(sp.cluster);
+    c->upload_cluster(cd);
+    fecl::LdpcClusterParams r;
+    const auto& L = c->ldev;
+    r.M = L.M;
+    r.N = L.N;
+    r.msg = L.msg;
+    r.d_max = L.d_max;
+    r.E = L.E;
+    r.row_ptr = L.row_ptr;
+    r.chk_addr = cd.chk_addr.as<uint32_t>();
+    r.bit_ptr = cd.bit_ptr.as<uint32_t>();
+    r.bit_addr = cd.bit_addr.as<uint32_t>();
+    r.row_split = cd.row_split.as<uint32_t>();
+    r.bit_split = cd.bit_split.as<uint32_t>();
+    r.sf = L.sf;
+    r.n_sf = L.n_sf;
+    r.sf_stride = L.sf_stride;
+    r.algorithm = L.algorithm;
+    r.iterations = L.iterations;
+    r.fixed_iterations = L.fixed_iterations;
+    r.separate_syndrome = 0;
+    for (const auto& row : c->ldpc->decoder().scaling)
+      if (row != c->ldpc->decoder().scaling[0]) r.separate_syndrome = 1;
+    r.msg_type = c->ldpc->decoder().precision;
+    r.cluster = int32_t(sp.cluster);
+    r.threads = sp.threads;
+    r.clusters = sp.clusters;
+    r.max_edges = int64_t(cd.plan.max_edges);
+    r.max_bits = int64_t(cd.plan.max_bits);
+    r.counter = reinterpret_cast<int32_t*>(at(sp.o1));
+    r.nframes = int64_t(n);
+    r.llr = d.llr;
+    r.llr_dtype = in_dtype;
+    r.syst_in = d.syst;
+    r.state_in = d.state;
+    r.hard = d.hard;
+    r.iters = d.iters;
+    r.msg_out = d.msg;
+    r.syst_out = d.syst_out;
+    r.parity_out = d.parity_out;
+    r.state_out = d.state_out;
+    r.out_dtype = out_dtype;
+    e = fecl::launch_ldpc_cluster(r, s);
+  } else if (c->kind == 0 && c->ldpc_lanes_ok()) {
     fecl::LdpcLanesParams r;
     const auto& L = c->ldev;
     r.M = L.M;
@@ -437,6 +583,7 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
     r.iterations = L.iterations;
     r.fixed_iterations = L.fixed_iterations;
     r.msg_type = c->ldpc->decoder().precision;
+    r.wave_groups = c->lanes_wave;
     r.nframes = int64_t(n);
     r.llr = d.llr;
     r.llr_dtype = in_dtype;
@@ -871,9 +1018,37 @@ int fecl_so_decode(fecl_codec_t codec, const fecl_so_io* io, uint64_t nframes, i
 int fecl_set_kernel(fecl_codec_t codec, int32_t kernel) {
   return guarded([&] {
     auto c = checked(codec);
-    if (kernel != FECL_KERNEL_AUTO && kernel != FECL_KERNEL_GENERIC) fail(FECL_EINVAL, "Invalid kernel selection");
+    if (kernel != FECL_KERNEL_AUTO && kernel != FECL_KERNEL_GENERIC && kernel != FECL_KERNEL_LANES &&
+        kernel != FECL_KERNEL_CLUSTER)
+      fail(FECL_EINVAL, "Invalid kernel selection");
+    if ((kernel == FECL_KERNEL_LANES || kernel == FECL_KERNEL_CLUSTER) && c->kind != 0)
+      fail(FECL_EINVAL, "kernel selection applies to LDPC codecs");
     std::lock_guard<std::mutex> lk(c->mu);
-    c->force_generic = (kernel == FECL_KERNEL_GENERIC);
+    c->kernel_sel = kernel;
+  });
+}
+
+int fecl_ldpc_set_cluster_shape(fecl_codec_t codec, int32_t cluster, int32_t threads) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 0) fail(FECL_EINVAL, "not an LDPC codec");
+    if (cluster != 0 && cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16)
+      fail(FECL_EINVAL, "cluster size must be 1, 2, 4, 8 or 16");
+    if (threads != 0 && threads != 256 && threads != 512 && threads != 1024)
+      fail(FECL_EINVAL, "threads per CTA must be 256, 512 or 1024");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->cluster_size_sel = cluster;
+    c->cluster_threads_sel = threads;
+  });
+}
+
+int fecl_ldpc_set_wave(fecl_codec_t codec, int32_t groups) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 0) fail(FECL_EINVAL, "not an LDPC codec");
+    if (groups < 0 || groups > 65535) fail(FECL_EINVAL, "wave must be 0..65535 groups");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->lanes_wave = groups;
   });
 }
 

@@ -59,6 +59,7 @@ struct LdpcLanesParams {
   int32_t n_sf = 1, sf_stride = 1;
   int32_t algorithm = 2, iterations = 1, fixed_iterations = 0;
   int32_t msg_type = 0;  // 0 FP32, 1 FP16, 2 saturated int8 (Q5.2)
+  int32_t wave_groups = 0;  // groups decoded together (0: as many as fit in 64 MiB of L2)
   // batch, frame-major caller buffers
   int64_t nframes = 0;
   const void* llr = nullptr;
@@ -84,6 +85,49 @@ struct LdpcLanesParams {
 
 size_t ldpc_lanes_scratch_bytes(int64_t N, int64_t E, int64_t nframes, int msg_type);
 cudaError_t launch_ldpc_lanes(LdpcLanesParams p, void* scratch, cudaStream_t stream);
+
+// Flooding BP with each frame's messages resident in the shared memory of a
+// thread-block cluster of `cluster` CTAs (ldpc_cluster.cu).  The address tables are
+// built per (code, cluster) by build_ldpc_cluster_plan (host/ldpc_plan.hpp).
+struct LdpcClusterParams {
+  // code
+  int32_t M = 0, N = 0, msg = 0, d_max = 0;
+  int64_t E = 0;
+  const uint32_t* row_ptr = nullptr;    // [M+1] CSR by check
+  const uint32_t* chk_addr = nullptr;   // [E]   CSR order: (rank << 28) | offset of the edge's bit
+  const uint32_t* bit_ptr = nullptr;    // [N]   start (multiple of 4) | degree << 26 into bit_addr
+  const uint32_t* bit_addr = nullptr;   // [..]  bit-major: (rank << 28) | offset of the edge
+  const uint32_t* row_split = nullptr;  // [cluster+1] rows owned by each rank
+  const uint32_t* bit_split = nullptr;  // [cluster+1] bits owned by each rank
+  const float* sf = nullptr;
+  int32_t n_sf = 1, sf_stride = 1;
+  int32_t algorithm = 2, iterations = 1, fixed_iterations = 0;
+  int32_t separate_syndrome = 0;  // scaling changes across iterations
+  int32_t msg_type = 0;           // 0 FP32, 1 FP16, 2 saturated int8 (Q5.2)
+  // shape
+  int32_t cluster = 1, threads = 512, clusters = 1;  // CTAs per cluster, threads per CTA, clusters in the grid
+  int64_t max_edges = 0, max_bits = 0;                // largest share of one rank
+  int64_t app_offset = 0;                             // filled by the launcher
+  int32_t* counter = nullptr;                         // device int, frames handed out
+  // batch, frame-major caller buffers
+  int64_t nframes = 0;
+  const void* llr = nullptr;
+  int32_t llr_dtype = 1;
+  const void* syst_in = nullptr;
+  const void* state_in = nullptr;
+  uint8_t* hard = nullptr;
+  int32_t* iters = nullptr;
+  void* msg_out = nullptr;
+  void* syst_out = nullptr;
+  void* parity_out = nullptr;
+  void* state_out = nullptr;
+  int32_t out_dtype = 1;
+};
+
+// Dynamic shared memory of one CTA for the given largest shares.
+size_t ldpc_cluster_smem_bytes(int64_t max_edges, int64_t max_bits, int msg_type);
+cudaError_t launch_ldpc_cluster(LdpcClusterParams p, cudaStream_t stream);
+int ldpc_cluster_max_active(const LdpcClusterParams& p);
 
 // ---- Turbo ---------------------------------------------------------------
 

@@ -53,7 +53,7 @@ __device__ __forceinline__ void check_row(const LdpcDeviceCode& c, float* __rest
                                           const float* __restrict__ app, int r, const float* sf_row) {
   const uint32_t e0 = c.row_ptr[r];
   const int d = int(c.row_ptr[r + 1] - e0);
-  const float sf = sf_row[d - 2];
+  const float sf = sf_row[d >= 2 ? d - 2 : 0];
   float v[DMAX];
 #pragma unroll
   for (int j = 0; j < DMAX; ++j)

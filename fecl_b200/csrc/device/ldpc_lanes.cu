@@ -2,20 +2,23 @@
 // lane.
 //
 // Same decoder as ldpc_flood.cu (BpDecoderImpl, src/detail/BpDecoder/BpDecoderImpl.cpp:37-179),
-// laid out for HBM streaming instead of one CTA per frame.  Frames are grouped by 32;
+// laid out for streaming instead of one CTA per frame.  Frames are grouped by 32;
 // within a group every per-bit and per-edge array is stored lane-minor,
 //     chan[g][n][32], app[g][n][32] (FP32), c2v[g][e][32] (FP32, FP16 or int8),
 // so when a warp works on one check row (or one bit) for its 32 frames, every load
 // and store is one contiguous 128-byte (or 64- / 32-byte) line, and the column
-// indices are the same for all lanes.  Each iteration is three launches:
+// indices are the same for all lanes.  Each iteration is two launches:
 //   check: warp per (group, row): v = app - c2v, the reference's forward/backward
 //          boxplus order (min-sum, whose chain is exact, as two minima and a sign
 //          parity), scaled c2v out; for iteration >= 1 it also folds the row's
 //          syndrome bit of the previous APP into a per-group failure mask (ballot +
 //          one atomicOr), which is the reference's stop test (:53-59);
-//   bit:   warp per (group, bit): app = chan + sum c2v in edge order;
-//   update: per group, frames whose syndrome held stop (their lanes are masked from
-//          then on) with the iteration count recorded.
+//   bit:   warp per (group, bit): app = chan + sum c2v in edge order; one block per
+//          group retires the frames whose syndrome held (their lanes are masked from
+//          then on) and records their iteration counts.
+// Groups are decoded in waves whose working set (chan, app, c2v) fits in L2: every
+// iteration of a wave runs before the next wave starts, so the messages of a wave
+// stay on chip and HBM sees each group's data about once per decode.
 // A frame that stops at iteration i has had exactly the reference's sequence: its
 // last check update ran with the scaling of iteration i, which equals that of
 // iteration I-1 because this kernel is used only when the scaling does not change
@@ -28,337 +31,266 @@
 
 #include "common.cuh"
 #include "kernels.hpp"
+#include "ldpc_math.cuh"
 
 namespace fecl {
 namespace {
 
-constexpr int kExact = 0, kLinear = 1, kApproximate = 2;
+using ldpc::kApproximate;
+using ldpc::kExact;
+using ldpc::kLinear;
+using ldpc::Msg;
 constexpr int kLanes = 32;
 constexpr int kWarpsPerBlock = 8;
 
 __constant__ LinearLut c_lut;
 
-__device__ __forceinline__ bool neg(float x) { return (__float_as_uint(x) >> 31) != 0; }
-
-__device__ __forceinline__ float box_linear(float a, float b) {
-  const float m = fminf(fabsf(a), fabsf(b));
-  const float s = (neg(a) != neg(b)) ? m : -m;
-  return s - lut_log1pexpm(c_lut, fabsf(a + b)) + lut_log1pexpm(c_lut, fabsf(a - b));
-}
-
-__device__ __forceinline__ float phi(float x) { return log1pf(2.0f / expm1f(x)); }
-
-// Message storage.
-template <int MSG>
-struct Msg;
-template <>
-struct Msg<0> {
-  using T = float;
-  __device__ static float load(const T* p) { return *p; }
-  __device__ static void store(T* p, float v) { *p = v; }
-};
-template <>
-struct Msg<1> {
-  using T = __half;
-  __device__ static float load(const T* p) { return __half2float(*p); }
-  __device__ static void store(T* p, float v) { *p = __float2half_rn(v); }
-};
-template <>
-struct Msg<2> {
-  using T = int8_t;
-  __device__ static float load(const T* p) { return float(*p) * 0.25f; }
-  __device__ static void store(T* p, float v) {
-    const float q = fminf(fmaxf(rintf(v * 4.0f), -127.0f), 127.0f);
-    *p = int8_t(q);
-  }
-};
-
-// One check row for this lane's frame: v[] in, c2v out (scaled), in the forward /
-// backward order of BpDecoderImpl::checkUpdate (:132-159).
-template <int ALG, int DMAX>
-__device__ __forceinline__ void row_update(const float v[DMAX], float out[DMAX], int d, float sf) {
-  if (ALG == kExact) {
-    float m[DMAX], fs[DMAX];
-    unsigned fn[DMAX];
-#pragma unroll
-    for (int j = 0; j < DMAX; ++j)
-      if (j < d) m[j] = phi(fminf(fabsf(v[j]), 80.0f));
-    fs[0] = m[0];
-    fn[0] = neg(v[0]);
-#pragma unroll
-    for (int j = 1; j < DMAX; ++j)
-      if (j < d - 1) {
-        fs[j] = fs[j - 1] + m[j];
-        fn[j] = fn[j - 1] ^ unsigned(neg(v[j]));
-      }
-    float bs = 0.0f;
-    unsigned bn = 0;
-    const unsigned odd = unsigned(d & 1);
-#pragma unroll
-    for (int j = DMAX - 1; j >= 0; --j) {
-      if (j < d) {
-        const int jp = j > 0 ? j - 1 : 0;
-        float s;
-        unsigned n;
-        if (j == d - 1) {
-          s = fs[jp];
-          n = fn[jp];
-        } else if (j == 0) {
-          s = bs;
-          n = bn;
-        } else {
-          s = fs[jp] + bs;
-          n = fn[jp] ^ bn;
-        }
-        const float mag = phi(s);
-        out[j] = sf * ((n ^ odd) ? -mag : mag);
-        if (j == d - 1) {
-          bs = m[j];
-          bn = unsigned(neg(v[j]));
-        } else {
-          bs = bs + m[j];
-          bn = bn ^ unsigned(neg(v[j]));
-        }
-      }
-    }
-  } else if (ALG == kApproximate) {
-    // Min-sum: the chain of MinBoxSum::sum over the other inputs is exact (a minimum
-    // and a sign parity: each pairwise sum is negative iff its operands' sign bits
-    // agree), so the two smallest magnitudes and the sign-bit parity give the same
-    // values bit for bit with a handful of registers.
-    float m1 = INFINITY, m2 = INFINITY;
-    int i1 = 0;
-    unsigned par = 0;
-#pragma unroll
-    for (int j = 0; j < DMAX; ++j) {
-      if (j < d) {
-        const float a = fabsf(v[j]);
-        par ^= unsigned(neg(v[j]));
-        if (a < m1) {
-          m2 = m1;
-          m1 = a;
-          i1 = j;
-        } else if (a < m2) {
-          m2 = a;
-        }
-      }
-    }
-    // d - 1 inputs: the result's sign bit is (d - 2) xor the parity of the others' sign bits.
-    const unsigned base = unsigned((d - 2) & 1);
-#pragma unroll
-    for (int j = 0; j < DMAX; ++j) {
-      if (j < d) {
-        const float m = (j == i1) ? m2 : m1;
-        const unsigned nb = base ^ par ^ unsigned(neg(v[j]));
-        out[j] = sf * (nb ? -m : m);
-      }
-    }
-  } else {
-    float fwd[DMAX];
-    fwd[0] = v[0];
-#pragma unroll
-    for (int j = 1; j < DMAX; ++j)
-      if (j < d - 1) fwd[j] = box_linear(fwd[j - 1], v[j]);
-    float bwd = 0.0f;
-#pragma unroll
-    for (int j = DMAX - 1; j >= 0; --j) {
-      if (j < d) {
-        const int jp = j > 0 ? j - 1 : 0;
-        float o;
-        if (j == d - 1) o = fwd[jp];
-        else if (j == 0) o = bwd;
-        else o = box_linear(fwd[jp], bwd);
-        out[j] = sf * o;
-        if (j == d - 1) bwd = v[j];
-        else bwd = box_linear(bwd, v[j]);
-      }
-    }
-  }
-}
-
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
+// Lane masks of a group at iteration `it`: active[it & 1][g] holds the frames still
+// decoding, fail[it & 1][g] collects the rows whose syndrome bit is set.  The bit pass
+// of iteration it retires frames and writes the masks of iteration it + 1, so a
+// kernel never reads a mask that the same launch writes.
+__device__ __forceinline__ uint32_t* active_of(const LdpcLanesParams& p, int it) { return p.active + (it & 1) * p.groups; }
+__device__ __forceinline__ uint32_t* fail_of(const LdpcLanesParams& p, int it) { return p.fail + (it & 1) * p.groups; }
+
+// One check row r of group g for this lane's frame: loads of v, the row update, the
+// stores of c2v for active lanes; returns the row's parity of the hard decision.
 template <int ALG, int MSG, int DMAX>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_check(LdpcLanesParams p, int it) {
+__device__ __forceinline__ void load_row(const LdpcLanesParams& p, int g, int r, int lane, uint32_t& e0, int& d,
+                                         float v[DMAX], unsigned& parity) {
   using M = Msg<MSG>;
-  auto* c2v = static_cast<typename M::T*>(p.c2v);
-  const int lane = lane_id();
-  const int64_t warps = int64_t(gridDim.x) * kWarpsPerBlock;
-  const int64_t tasks = int64_t(p.groups) * p.M;
-  const bool check_syndrome = it > 0 && !p.fixed_iterations;
-  const float* sf_row = p.sf + size_t(it % p.n_sf) * p.sf_stride;
-  for (int64_t t = int64_t(blockIdx.x) * kWarpsPerBlock + (threadIdx.x >> 5); t < tasks; t += warps) {
-    const int g = int(t / p.M);
-    const int r = int(t - int64_t(g) * p.M);
-    const uint32_t active = p.active[g];
-    if (active == 0) continue;
-    const bool mine = (active >> lane) & 1;
-    const uint32_t e0 = __ldg(p.row_ptr + r);
-    const int d = int(__ldg(p.row_ptr + r + 1) - e0);
-    typename M::T* cg = c2v + (int64_t(g) * p.E + e0) * kLanes + lane;
-    const float* ag = p.app + int64_t(g) * p.N * kLanes + lane;
-    float v[DMAX];
-    unsigned parity = 0;
+  const auto* c2v = static_cast<const typename M::T*>(p.c2v);
+  e0 = __ldg(p.row_ptr + r);
+  d = int(__ldg(p.row_ptr + r + 1) - e0);
+  const typename M::T* cg = c2v + (int64_t(g) * p.E + e0) * kLanes + lane;
+  const float* ag = p.app + int64_t(g) * p.N * kLanes + lane;
+  parity = 0;
 #pragma unroll
-    for (int j = 0; j < DMAX; ++j) {
-      if (j < d) {
-        const uint32_t col = __ldg(p.col_idx + e0 + j);
-        const float a = ag[int64_t(col) * kLanes];
-        parity ^= unsigned(a >= 0.0f);
-        v[j] = a - M::load(cg + j * kLanes);
-      }
-    }
-    if (check_syndrome) {
-      const uint32_t bad = __ballot_sync(0xffffffffu, parity != 0) & active;
-      if (bad && lane == 0) atomicOr(p.fail + g, bad);
-    }
-    float out[DMAX];
-    row_update<ALG, DMAX>(v, out, d, sf_row[d - 2]);
-    if (mine) {
-#pragma unroll
-      for (int j = 0; j < DMAX; ++j)
-        if (j < d) M::store(cg + j * kLanes, out[j]);
+  for (int j = 0; j < DMAX; ++j) {
+    if (j < d) {
+      const uint32_t col = __ldg(p.col_idx + e0 + j);
+      const float a = ag[int64_t(col) * kLanes];
+      parity ^= unsigned(a >= 0.0f);
+      v[j] = a - M::load(cg + j * kLanes);
     }
   }
 }
 
-// app = chan + sum of c2v over the bit's edges, in increasing edge order.
+template <int ALG, int MSG, int DMAX>
+__device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, uint32_t e0, int d, int lane, const float* sf_row,
+                                          const float v[DMAX], bool mine) {
+  using M = Msg<MSG>;
+  auto* c2v = static_cast<typename M::T*>(p.c2v);
+  float out[DMAX];
+  ldpc::row_update<ALG, DMAX>(c_lut, v, out, d, sf_row[d >= 2 ? d - 2 : 0]);
+  if (mine) {
+    typename M::T* cg = c2v + (int64_t(g) * p.E + e0) * kLanes + lane;
+#pragma unroll
+    for (int j = 0; j < DMAX; ++j)
+      if (j < d) M::store(cg + j * kLanes, out[j]);
+  }
+}
+
+// Check pass of iteration `it` over groups [g0, g0 + gridDim.y): a warp per row, two
+// rows at a time for short rows so that twice the loads are in flight.
+template <int ALG, int MSG, int DMAX>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_check(LdpcLanesParams p, int it, int g0) {
+  constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  const int lane = lane_id();
+  const int warps = int(gridDim.x) * kWarpsPerBlock;
+  const bool check_syndrome = it > 0 && !p.fixed_iterations;
+  const float* sf_row = p.sf + size_t(it % p.n_sf) * p.sf_stride;
+  const int g = g0 + int(blockIdx.y);
+  const uint32_t active = active_of(p, it)[g];
+  if (active == 0) return;
+  const bool mine = (active >> lane) & 1;
+  uint32_t bad = 0;
+  const int w0 = int(blockIdx.x) * kWarpsPerBlock + (threadIdx.x >> 5);
+  for (int r = w0 * kRows; r < p.M; r += warps * kRows) {
+    float v[kRows][DMAX];
+    uint32_t e0[kRows];
+    int d[kRows];
+    unsigned parity[kRows];
+#pragma unroll
+    for (int q = 0; q < kRows; ++q) {
+      d[q] = 0;
+      parity[q] = 0;
+      if (r + q < p.M) load_row<ALG, MSG, DMAX>(p, g, r + q, lane, e0[q], d[q], v[q], parity[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < kRows; ++q) {
+      if (d[q] > 0) {
+        if (check_syndrome) bad |= __ballot_sync(0xffffffffu, parity[q] != 0);
+        store_row<ALG, MSG, DMAX>(p, g, e0[q], d[q], lane, sf_row, v[q], mine);
+      }
+    }
+  }
+  bad &= active;
+  if (bad && lane == 0) atomicOr(fail_of(p, it) + g, bad);
+}
+
+// Bit pass of iteration `it` (or, with it < 0, the initial APP from chan and the
+// staged c2v for every lane): app = chan + sum of c2v over the bit's edges, in
+// increasing edge order.  Block (0, y) of each group retires the frames whose
+// syndrome held at this iteration, or all of them at the last one, records their
+// iteration counts and writes the group's masks for iteration it + 1.
 template <int MSG>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_bit(LdpcLanesParams p, int all_lanes) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_bit(LdpcLanesParams p, int it, int g0) {
   using M = Msg<MSG>;
   const auto* c2v = static_cast<const typename M::T*>(p.c2v);
   const int lane = lane_id();
-  const int64_t warps = int64_t(gridDim.x) * kWarpsPerBlock;
-  const int64_t tasks = int64_t(p.groups) * p.N;
-  for (int64_t t = int64_t(blockIdx.x) * kWarpsPerBlock + (threadIdx.x >> 5); t < tasks; t += warps) {
-    const int g = int(t / p.N);
-    const int b = int(t - int64_t(g) * p.N);
-    const uint32_t active = all_lanes ? 0xffffffffu : p.active[g];
-    if (!((active >> lane) & 1)) continue;
+  const int warps = int(gridDim.x) * kWarpsPerBlock;
+  const int g = g0 + int(blockIdx.y);
+  const uint32_t active = it < 0 ? 0xffffffffu : active_of(p, it)[g];
+  if (it >= 0 && blockIdx.x == 0 && threadIdx.x == 0) {
+    uint32_t done = 0;
+    if (it == p.iterations - 1) done = active;
+    else if (it > 0 && !p.fixed_iterations) done = active & ~fail_of(p, it)[g];
+    for (uint32_t m = done; m; m &= m - 1) p.iters_ws[int64_t(g) * kLanes + (__ffs(m) - 1)] = it + 1;
+    active_of(p, it + 1)[g] = active & ~done;
+    fail_of(p, it + 1)[g] = 0;
+  }
+  if (!((active >> lane) & 1)) return;
+  const typename M::T* cg = c2v + int64_t(g) * p.E * kLanes + lane;
+  for (int b = int(blockIdx.x) * kWarpsPerBlock + (threadIdx.x >> 5); b < p.N; b += warps) {
     const int64_t base = (int64_t(g) * p.N + b) * kLanes + lane;
+    const uint32_t k0 = __ldg(p.col_ptr + b), k1 = __ldg(p.col_ptr + b + 1);
     float acc = p.chan[base];
-    const uint32_t k1 = __ldg(p.col_ptr + b + 1);
-    const typename M::T* cg = c2v + int64_t(g) * p.E * kLanes + lane;
-    for (uint32_t k = __ldg(p.col_ptr + b); k < k1; ++k) acc += M::load(cg + int64_t(__ldg(p.col_edges + k)) * kLanes);
+    uint32_t k = k0;
+    for (; k + 4 <= k1; k += 4) {
+      const uint32_t e_0 = __ldg(p.col_edges + k), e_1 = __ldg(p.col_edges + k + 1);
+      const uint32_t e_2 = __ldg(p.col_edges + k + 2), e_3 = __ldg(p.col_edges + k + 3);
+      const float x0 = M::load(cg + int64_t(e_0) * kLanes), x1 = M::load(cg + int64_t(e_1) * kLanes);
+      const float x2 = M::load(cg + int64_t(e_2) * kLanes), x3 = M::load(cg + int64_t(e_3) * kLanes);
+      acc += x0;
+      acc += x1;
+      acc += x2;
+      acc += x3;
+    }
+    for (; k < k1; ++k) acc += M::load(cg + int64_t(__ldg(p.col_edges + k)) * kLanes);
     p.app[base] = acc;
   }
 }
 
-// Frames whose syndrome held at this iteration (or every frame at the last one) stop.
-__global__ void lanes_update(LdpcLanesParams p, int it) {
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < p.groups; g += gridDim.x * blockDim.x) {
-    const uint32_t active = p.active[g];
-    uint32_t done = 0;
-    if (it == p.iterations - 1) done = active;
-    else if (it > 0 && !p.fixed_iterations) done = active & ~p.fail[g];
-    for (uint32_t m = done; m; m &= m - 1) {
-      const int l = __ffs(m) - 1;
-      p.iters_ws[int64_t(g) * kLanes + l] = it + 1;
-    }
-    p.active[g] = active & ~done;
-    p.fail[g] = 0;
-  }
-}
-
-// Frame-major inputs -> lane-minor scratch: chan (+ a-priori on systematic bits),
-// c2v (state or zero), lane masks.  One thread per (group, position, lane).
+// Frame-major inputs -> lane-minor scratch for group blockIdx.y: chan (+ a-priori on
+// systematic bits), c2v (state or zero), lane masks.
 template <int MSG>
 __global__ void lanes_stage(LdpcLanesParams p) {
   using M = Msg<MSG>;
   auto* c2v = static_cast<typename M::T*>(p.c2v);
-  const int64_t tot_bits = int64_t(p.groups) * p.N * kLanes;
-  const int64_t tot_edges = int64_t(p.groups) * p.E * kLanes;
-  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < tot_bits; i += stride) {
-    const int lane = int(i % kLanes);
-    const int64_t gb = i / kLanes;
-    const int g = int(gb / p.N);
-    const int b = int(gb - int64_t(g) * p.N);
+  const int g = int(blockIdx.y);
+  const int stride = int(gridDim.x) * blockDim.x;
+  const int t0 = int(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (int i = t0; i < p.N * kLanes; i += stride) {
+    const int lane = i % kLanes, b = i / kLanes;
     const int64_t f = int64_t(g) * kLanes + lane;
     float x = 0.0f;
     if (f < p.nframes) {
       x = load_llr(p.llr, p.llr_dtype, f * p.N + b);
       if (p.syst_in && b < p.msg) x += load_llr(p.syst_in, p.llr_dtype, f * p.msg + b);
     }
-    p.chan[i] = x;
+    p.chan[int64_t(g) * p.N * kLanes + i] = x;
   }
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < tot_edges; i += stride) {
+  for (int64_t i = t0; i < p.E * kLanes; i += stride) {
     const int lane = int(i % kLanes);
-    const int64_t ge = i / kLanes;
-    const int g = int(ge / p.E);
-    const int64_t e = ge - int64_t(g) * p.E;
+    const int64_t e = i / kLanes;
     const int64_t f = int64_t(g) * kLanes + lane;
     float v = 0.0f;
     if (p.state_in && f < p.nframes) v = load_llr(p.state_in, p.llr_dtype, f * p.E + e);
-    M::store(c2v + i, v);
+    M::store(c2v + int64_t(g) * p.E * kLanes + i, v);
   }
-  for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < p.groups; g += stride) {
-    const int64_t left = p.nframes - g * kLanes;
+  if (t0 == 0) {
+    const int64_t left = p.nframes - int64_t(g) * kLanes;
     p.active[g] = left >= kLanes ? 0xffffffffu : ((1u << left) - 1u);
+    p.active[p.groups + g] = 0;
     p.fail[g] = 0;
+    p.fail[p.groups + g] = 0;
   }
 }
 
-// Outputs: hard bits from app >= 0 (:67-69), or the soft outputs of :111-129.
+// Outputs of group blockIdx.y: hard bits from app >= 0 (:67-69), or the soft outputs
+// of :111-129.
 template <int MSG>
 __global__ void lanes_finish(LdpcLanesParams p) {
   using M = Msg<MSG>;
   const auto* c2v = static_cast<const typename M::T*>(p.c2v);
-  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-  const int64_t tot_bits = int64_t(p.groups) * p.N * kLanes;
+  const int g = int(blockIdx.y);
+  const int stride = int(gridDim.x) * blockDim.x;
+  const int t0 = int(blockIdx.x) * blockDim.x + threadIdx.x;
   const bool soft = p.msg_out || p.syst_out || p.parity_out;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < tot_bits; i += stride) {
-    const int lane = int(i % kLanes);
-    const int64_t gb = i / kLanes;
-    const int g = int(gb / p.N);
-    const int b = int(gb - int64_t(g) * p.N);
+  const typename M::T* cg = c2v + int64_t(g) * p.E * kLanes;
+  for (int i = t0; i < p.N * kLanes; i += stride) {
+    const int lane = i % kLanes, b = i / kLanes;
     const int64_t f = int64_t(g) * kLanes + lane;
     if (f >= p.nframes) continue;
-    if (p.hard && b < p.msg) p.hard[f * p.msg + b] = uint8_t(p.app[i] >= 0.0f);
+    const int64_t at = int64_t(g) * p.N * kLanes + i;
+    if (p.hard && b < p.msg) p.hard[f * p.msg + b] = uint8_t(p.app[at] >= 0.0f);
     if (soft) {
       float ext = 0.0f;
-      const typename M::T* cg = c2v + int64_t(g) * p.E * kLanes + lane;
       for (uint32_t k = __ldg(p.col_ptr + b); k < __ldg(p.col_ptr + b + 1); ++k)
-        ext += M::load(cg + int64_t(__ldg(p.col_edges + k)) * kLanes);
+        ext += M::load(cg + int64_t(__ldg(p.col_edges + k)) * kLanes + lane);
       if (p.parity_out) store_llr(p.parity_out, p.out_dtype, f * p.N + b, ext);
       if (b < p.msg) {
         if (p.syst_out) store_llr(p.syst_out, p.out_dtype, f * p.msg + b, ext);
-        if (p.msg_out) store_llr(p.msg_out, p.out_dtype, f * p.msg + b, p.chan[i] + ext);
+        if (p.msg_out) store_llr(p.msg_out, p.out_dtype, f * p.msg + b, p.chan[at] + ext);
       }
     }
   }
   if (p.state_out) {
-    const int64_t tot_edges = int64_t(p.groups) * p.E * kLanes;
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < tot_edges; i += stride) {
+    for (int64_t i = t0; i < p.E * kLanes; i += stride) {
       const int lane = int(i % kLanes);
-      const int64_t ge = i / kLanes;
-      const int g = int(ge / p.E);
-      const int64_t e = ge - int64_t(g) * p.E;
+      const int64_t e = i / kLanes;
       const int64_t f = int64_t(g) * kLanes + lane;
-      if (f < p.nframes) store_llr(p.state_out, p.out_dtype, f * p.E + e, M::load(c2v + i));
+      if (f < p.nframes) store_llr(p.state_out, p.out_dtype, f * p.E + e, M::load(cg + i));
     }
   }
-  for (int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; f < p.nframes; f += stride)
-    if (p.iters) p.iters[f] = p.iters_ws[f];
+  if (p.iters && t0 < kLanes) {
+    const int64_t f = int64_t(g) * kLanes + t0;
+    if (f < p.nframes) p.iters[f] = p.iters_ws[f];
+  }
 }
 
-int grid_for(int64_t tasks_warps) {
-  const int64_t blocks = (tasks_warps + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  return int(blocks < 148 * 16 ? (blocks > 0 ? blocks : 1) : 148 * 16);
+// Grid of a per-row or per-bit pass over `groups` groups: y = group, x strides over
+// `per_group` rows or bits with one warp each, about 16 blocks per SM over the grid.
+dim3 grid_for(int64_t per_group, int groups) {
+  const int64_t need = (per_group + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const int64_t share = (148 * 16 + groups - 1) / groups;
+  const int64_t x = need < share ? need : share;
+  return dim3(unsigned(x > 0 ? x : 1), unsigned(groups));
 }
+
+// Working set of one group in bytes: chan, app and c2v, the arrays every iteration
+// touches.
+int64_t group_bytes(const LdpcLanesParams& p) {
+  const int64_t mb = p.msg_type == 1 ? 2 : (p.msg_type == 2 ? 1 : 4);
+  return int64_t(kLanes) * (2 * 4 * int64_t(p.N) + mb * p.E);
+}
+
+// Groups decoded together: all iterations of a wave run before the next wave starts,
+// so that a wave whose working set fits in L2 never goes back to HBM for its messages.
+constexpr int64_t kWaveBytes = 64ll << 20;
 
 template <int ALG, int MSG, int DMAX>
 cudaError_t run(const LdpcLanesParams& p, cudaStream_t s) {
-  const int gb = grid_for(int64_t(p.groups) * p.N);
-  const int gc = grid_for(int64_t(p.groups) * p.M);
-  lanes_stage<MSG><<<1184, 256, 0, s>>>(p);
-  lanes_bit<MSG><<<gb, kWarpsPerBlock * 32, 0, s>>>(p, 1);
-  for (int it = 0; it < p.iterations; ++it) {
-    lanes_check<ALG, MSG, DMAX><<<gc, kWarpsPerBlock * 32, 0, s>>>(p, it);
-    lanes_bit<MSG><<<gb, kWarpsPerBlock * 32, 0, s>>>(p, 0);
-    lanes_update<<<(p.groups + 127) / 128, 128, 0, s>>>(p, it);
+  if (p.groups > 65535) return cudaErrorInvalidValue;
+  const int64_t gb = group_bytes(p);
+  int wave = int(p.wave_groups > 0 ? p.wave_groups : (kWaveBytes + gb - 1) / gb);
+  if (wave < 1) wave = 1;
+  if (wave > p.groups) wave = p.groups;
+  const dim3 gs((148 * 8 + p.groups - 1) / p.groups, p.groups);
+  lanes_stage<MSG><<<gs, 256, 0, s>>>(p);
+  for (int w0 = 0; w0 < p.groups; w0 += wave) {
+    const int nw = p.groups - w0 < wave ? p.groups - w0 : wave;
+    const dim3 gbit = grid_for(p.N, nw);
+    const dim3 gchk = grid_for((p.M + (DMAX <= 8 ? 1 : 0)) / (DMAX <= 8 ? 2 : 1), nw);
+    lanes_bit<MSG><<<gbit, kWarpsPerBlock * 32, 0, s>>>(p, -1, w0);
+    for (int it = 0; it < p.iterations; ++it) {
+      lanes_check<ALG, MSG, DMAX><<<gchk, kWarpsPerBlock * 32, 0, s>>>(p, it, w0);
+      lanes_bit<MSG><<<gbit, kWarpsPerBlock * 32, 0, s>>>(p, it, w0);
+    }
   }
-  lanes_finish<MSG><<<1184, 256, 0, s>>>(p);
+  lanes_finish<MSG><<<gs, 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 
@@ -386,14 +318,13 @@ size_t ldpc_lanes_scratch_bytes(int64_t N, int64_t E, int64_t nframes, int msg_t
   const size_t msg_bytes = msg_type == 1 ? 2 : (msg_type == 2 ? 1 : 4);
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   return al(size_t(groups) * N * kLanes * 4) * 2 + al(size_t(groups) * E * kLanes * msg_bytes) +
-         al(size_t(groups) * 8) + al(size_t(groups) * kLanes * 4);
+         al(size_t(groups) * 16) + al(size_t(groups) * kLanes * 4);
 }
 
 cudaError_t launch_ldpc_lanes(LdpcLanesParams p, void* scratch, cudaStream_t s) {
   static bool lut_ready = false;
   if (!lut_ready) {
-    LinearLut l;
-    for (int i = 0; i < 8; ++i) l.y[i] = float(log(1.0 + exp(-(double(i) / 2.0))));
+    const LinearLut l = ldpc::linear_lut();
     cudaError_t e = cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
     if (e != cudaSuccess) return e;
     lut_ready = true;
@@ -409,9 +340,9 @@ cudaError_t launch_ldpc_lanes(LdpcLanesParams p, void* scratch, cudaStream_t s) 
   q += al(size_t(p.groups) * p.N * kLanes * 4);
   p.c2v = q;
   q += al(size_t(p.groups) * p.E * kLanes * msg_bytes);
-  p.active = reinterpret_cast<uint32_t*>(q);
-  p.fail = p.active + p.groups;
-  q += al(size_t(p.groups) * 8);
+  p.active = reinterpret_cast<uint32_t*>(q);  // [2][groups]
+  p.fail = p.active + 2 * p.groups;          // [2][groups]
+  q += al(size_t(p.groups) * 16);
   p.iters_ws = reinterpret_cast<int32_t*>(q);
   switch (p.algorithm) {
     case kExact: return run_m<kExact>(p, s);

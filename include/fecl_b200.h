@@ -213,7 +213,23 @@ void fecl_destroy(fecl_codec_t codec);
  * LDPC frame). */
 #define FECL_KERNEL_AUTO 0
 #define FECL_KERNEL_GENERIC 1
+/* LDPC only: the lane-batched decoder (32 frames per warp, messages in device
+ * memory) or the cluster-resident decoder (each frame's messages in the shared
+ * memory of a thread-block cluster).  Both compute the same values bit for bit. */
+#define FECL_KERNEL_LANES 2
+#define FECL_KERNEL_CLUSTER 3
 int fecl_set_kernel(fecl_codec_t codec, int32_t kernel);
+
+/* Shape of the cluster-resident LDPC decoder: CTAs per frame (1, 2, 4, 8 or 16) and
+ * threads per CTA (256, 512 or 1024).  0 for either restores the built-in choice.
+ * Shapes whose shares of the code do not fit in shared memory fall back to the
+ * lane-batched decoder (or fail with FECL_EUNSUPPORTED under FECL_KERNEL_CLUSTER). */
+int fecl_ldpc_set_cluster_shape(fecl_codec_t codec, int32_t cluster, int32_t threads);
+
+/* Lane-batched LDPC decoder: frame groups (32 frames each) decoded together, every
+ * iteration of one wave of groups before the next; 0 restores the built-in choice
+ * (the groups whose messages fit in 64 MiB of L2). */
+int fecl_ldpc_set_wave(fecl_codec_t codec, int32_t groups);
 
 /* Windowed turbo decoder: training steps run before each segment's forward and
  * backward walk (a multiple of 8; -1 restores the default of 96).  Training only
