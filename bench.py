@@ -409,13 +409,258 @@ def ldpc_cpu_reference(w, jobs, sample_frames=16):
                        % (sample_frames, cores, total_s)}, match)
 
 
+# ---- mixed batch (--workload mixed) ---------------------------------------------------
+
+MIXED_RATES = [(1, 2), (3, 5), (2, 3), (3, 4), (4, 5), (5, 6)]
+
+
+def mixed_requests(total, seed):
+    """The mixed batch of 4096 frames: 50 % LTE turbo frames with K uniform over the 188
+    QPP sizes, 40 % DVB-S2 short and 10 % DVB-S2 normal LDPC frames with the rate
+    uniform over MIXED_RATES; Eb/N0 uniform in 0.5-3.0 dB per frame (seeded)."""
+    import numpy as np
+    import fecl_b200 as F
+    rng = np.random.default_rng(seed)
+    sizes = F.Turbo.Lte3Gpp.sizes()
+    kinds = rng.choice(3, size=total, p=[0.5, 0.4, 0.1])
+    reqs = []
+    for k in kinds:
+        ebn0 = float(rng.uniform(0.5, 3.0))
+        if k == 0:
+            reqs.append(("turbo", int(sizes[rng.integers(len(sizes))]), ebn0))
+        else:
+            reqs.append(("ldpc", (16200 if k == 1 else 64800, MIXED_RATES[rng.integers(len(MIXED_RATES))]), ebn0))
+    return reqs
+
+
+class MixedCodes:
+    """One codec per code of the mix: LTE turbo (max-log-MAP, 6 iterations) and DVB-S2
+    LDPC (normalised min-sum 0.75, at most 50 iterations with the syndrome stop) with the
+    given LDPC message precision."""
+
+    def __init__(self, precision):
+        self.precision = precision
+        self.codes = {}
+
+    def get(self, key):
+        import fecl_b200 as F
+        from fractions import Fraction
+        if key not in self.codes:
+            kind, p = key
+            if kind == "turbo":
+                self.codes[key] = F.Turbo.lte(p, F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(6)
+                                              .scheduling(F.Serial))
+            else:
+                n, (a, b) = p
+                H = F.Ldpc.DvbS2.matrix(n, Fraction(a, b))
+                self.codes[key] = F.Ldpc(F.Ldpc.EncoderOptions(H), F.Ldpc.DecoderOptions().algorithm(F.Approximate)
+                                         .iterations(50).scalingFactor(0.75).precision(self.precision))
+        return self.codes[key]
+
+
+def mixed_inputs(reqs, codes, seed):
+    """Per request: codec key, message bits and FP16 L-values (seeded per request)."""
+    import numpy as np
+    from fecl_b200 import channel as ch
+    out = []
+    for i, (kind, p, ebn0) in enumerate(reqs):
+        key = (kind, p)
+        code = codes.get(key)
+        msg = ch.random_bits(code.msgSize(), seed * 100003 + i)
+        llr = ch.awgn_llr(code.encode(msg), ebn0, code.msgSize() / code.paritySize(), seed * 100003 + i, np.float16)
+        out.append((key, msg, llr))
+    return out
+
+
+def run_mixed(args):
+    import numpy as np
+    import torch
+    import fecl_b200 as F
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    total = args.frames or 4096
+    prec = PRECISIONS[args.precision if args.precision != "f32" else "f16"]
+    reqs = mixed_requests(total, SEED + rank)
+    codes = MixedCodes(prec)
+    inputs = mixed_inputs(reqs, codes, SEED + rank)
+    # one job per code: its frames' L-values contiguous in one device buffer
+    by_key = {}
+    for idx, (key, msg, llr) in enumerate(inputs):
+        by_key.setdefault(key, []).append(idx)
+    keys = sorted(by_key, key=str)
+    llr_host = np.concatenate([inputs[i][2] for k in keys for i in by_key[k]])
+    msg_ref = [np.concatenate([inputs[i][1] for i in by_key[k]]) for k in keys]
+    d_llr = torch.from_numpy(llr_host).cuda()
+    n_bits_out = sum(codes.get(k).msgSize() * len(by_key[k]) for k in keys)
+    d_msg = torch.zeros(n_bits_out, dtype=torch.uint8, device="cuda")
+    d_its = torch.zeros(total, dtype=torch.int32, device="cuda")
+    jobs, lo, mo, fo = [], 0, 0, 0
+    for k in keys:
+        c, n = codes.get(k), len(by_key[k])
+        jobs.append((c, d_llr[lo:lo + n * c.paritySize()], d_msg[mo:mo + n * c.msgSize()], d_its[fo:fo + n]))
+        lo += n * c.paritySize()
+        mo += n * c.msgSize()
+        fo += n
+    t0 = time.perf_counter()
+    batch = F.Batch(jobs, autotune=not args.no_autotune)
+    build_s = time.perf_counter() - t0
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    if args.profile_decodes:
+        for _ in range(args.profile_decodes):
+            batch.run()
+        torch.cuda.synchronize()
+        return 0
+    for _ in range(max(args.warmup, 3)):
+        batch.run()
+    barrier()
+    times = []
+    with ClockSampler(local) as clk:
+        barrier()
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            batch.run()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        barrier()
+    clocks = clk.summary()
+    ms = statistics.mean(times)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    info_bits = sum(codes.get(k).msgSize() * len(by_key[k]) for k in keys)
+    value = world * info_bits / (ms * 1e-3) / 1e6
+
+    # FER per family and the algorithmic bytes of one step (iterations as run)
+    bits = d_msg.cpu().numpy()
+    its = d_its.cpu().numpy()
+    fam = {"turbo": [0, 0], "ldpc16200": [0, 0], "ldpc64800": [0, 0]}
+    alg_bytes = 0
+    mo = fo = 0
+    s_msg = {0: 4, 1: 2, 2: 1}[prec]
+    for k, ref in zip(keys, msg_ref):
+        c, n = codes.get(k), len(by_key[k])
+        K = c.msgSize()
+        got = bits[mo:mo + n * K].reshape(n, K)
+        bad = np.any(got != ref.reshape(n, K), axis=1)
+        name = "turbo" if k[0] == "turbo" else "ldpc%d" % k[1][0]
+        fam[name][0] += int(bad.sum())
+        fam[name][1] += n
+        if k[0] == "turbo":
+            alg_bytes += n * algorithmic_bytes_per_frame(K, 6, 2, 4)
+        else:
+            alg_bytes += n * (c.paritySize() * 2 + K) + int(its[fo:fo + n].sum()) * (2 * c.stateSize() * s_msg + 2 * c.paritySize() * 4)
+        mo += n * K
+        fo += n
+
+    # end to end: pinned host L-values in, decisions out, every step
+    h_llr = torch.from_numpy(llr_host).pin_memory()
+    h_msg = torch.empty(n_bits_out, dtype=torch.uint8).pin_memory()
+    e2e = []
+    barrier()
+    for _ in range(max(3, args.steps // 2)):
+        t1 = time.perf_counter()
+        d_llr.copy_(h_llr, non_blocking=True)
+        batch.run()
+        h_msg.copy_(d_msg, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        e2e.append(time.perf_counter() - t1)
+    barrier()
+    e2e_s = statistics.mean(e2e)
+
+    # the plain per-request FP32 GPU decoder on a sample of the same requests: one
+    # decode call per frame, FP32 messages, device-resident L-values
+    plain = None
+    if rank == 0 and not args.no_plain:
+        sample = inputs[: min(len(inputs), args.plain_sample)]
+        pcodes = MixedCodes(0)
+        d_in = [torch.from_numpy(llr).cuda() for _, _, llr in sample]
+        torch.cuda.synchronize()
+        for (key, _, _), x in zip(sample[:8], d_in[:8]):
+            pcodes.get(key).decode(x)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        outs = [pcodes.get(key).decode(x) for (key, _, _), x in zip(sample, d_in)]
+        torch.cuda.synchronize()
+        pt = time.perf_counter() - t1
+        perr = sum(int(np.any(o.cpu().numpy() != m)) for o, (_, m, _) in zip(outs, sample))
+        sbits = sum(m.size for _, m, _ in sample)
+        # the batch's errors on the same requests
+        berr = 0
+        pos = {}
+        mo = 0
+        for k in keys:
+            K = codes.get(k).msgSize()
+            for j, i in enumerate(by_key[k]):
+                pos[i] = mo + j * K
+            mo += len(by_key[k]) * K
+        for i, (key, m, _) in enumerate(sample):
+            berr += int(np.any(bits[pos[i]:pos[i] + m.size] != m))
+        plain = {"value": round(sbits / pt / 1e6, 2), "unit": "Mbit/s", "frames": len(sample), "fer": perr / len(sample),
+                 "batch_fer_same_frames": berr / len(sample),
+                 "what": "one decode call per frame, FP32 messages, L-values in device memory, same requests"}
+
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "Mbit/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f16", "data": "synthetic",
+        "config": {"workload": "mixed batch of %d frames: 50%% LTE turbo (K uniform over the 188 QPP sizes, max-log-MAP, "
+                               "6 iterations), 40%% DVB-S2 short and 10%% DVB-S2 normal LDPC (rates 1/2..5/6, "
+                               "normalised min-sum 0.75, <=50 iterations), Eb/N0 U(0.5, 3.0) dB per frame, FP16 L-values, "
+                               "one CUDA graph" % total,
+                   "ldpc_message_storage": {0: "f32", 1: "f16", 2: "i8"}[prec], "codes": len(keys),
+                   "autotune": not args.no_autotune, "build_s": round(build_s, 3),
+                   "fer": {k: (v[0] / v[1] if v[1] else None) for k, v in fam.items()},
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": "frame shards, replicas per GPU" if world > 1 else "single GPU"},
+        "latency_ms": {"p50": round(statistics.median(times), 4),
+                       "p99": round(sorted(times)[min(len(times) - 1, int(0.99 * len(times)))], 4)},
+        "e2e": {"value": round(world * info_bits / e2e_s / 1e6, 2), "unit": "Mbit/s",
+                "h2d_bytes_per_step": int(llr_host.nbytes), "d2h_bytes_per_step": int(n_bits_out)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                     "kernel": "mixed batch graph (turbo_lte_batch_kernel + LDPC kernels) per step",
+                     "algorithmic_bytes_per_step": int(alg_bytes)},
+        "plain_per_request_fp32": plain,
+        "gpu_launches": None,
+        "clocks": clocks,
+    }
+    if plain:
+        line["speedup_vs_plain_per_request"] = round(value / plain["value"], 1)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lte-turbo", choices=["lte-turbo"] + sorted(LDPC_WORKLOADS),
+    ap.add_argument("--workload", default="lte-turbo", choices=["lte-turbo", "mixed"] + sorted(LDPC_WORKLOADS),
                     help="lte-turbo is the headline workload; the LDPC workloads print the same line for BP")
     ap.add_argument("--frames", type=int, default=0,
                     help="LDPC workloads: frames per code instead of the workload's (small cases for ncu)")
@@ -427,6 +672,9 @@ def main():
     ap.add_argument("--threads", type=int, default=0, help="LDPC: threads per CTA of the cluster kernel (0: built-in)")
     ap.add_argument("--wave", type=int, default=0, help="LDPC: frame groups of 32 decoded together (0: built-in)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="mixed: build the batch without autotuning")
+    ap.add_argument("--no-plain", action="store_true", help="mixed: skip the per-request FP32 comparison")
+    ap.add_argument("--plain-sample", type=int, default=256, help="mixed: requests decoded one by one for the comparison")
     ap.add_argument("--profile-decodes", type=int, default=0,
                     help="only run this many decodes of the workload (for ncu captures) and exit")
     args = ap.parse_args()
@@ -434,6 +682,8 @@ def main():
         return run_reference_arm(args)
     if args.workload in LDPC_WORKLOADS:
         return run_ldpc(args)
+    if args.workload == "mixed":
+        return run_mixed(args)
 
     import numpy as np
     import torch

@@ -26,7 +26,7 @@ from ._lib import lib as _L
 
 __all__ = [
     "Exact", "Linear", "Approximate", "Serial", "Parallel", "Custom",
-    "SparseBitMatrix", "Trellis", "Codec", "Ldpc", "Turbo", "FeclError", "lib_path",
+    "SparseBitMatrix", "Trellis", "Codec", "Ldpc", "Turbo", "Batch", "FeclError", "lib_path",
 ]
 
 # DecoderAlgorithm (src/DecoderAlgorithm.h:30-34) and SchedulingType (src/SchedulingType.h:32-39)
@@ -544,6 +544,13 @@ class Turbo(Codec):
             _check(_L.fecl_lte_interleaver(int(length), _ptr(p)))
             return p
 
+        @staticmethod
+        def sizes():
+            """The 188 message lengths of the LTE QPP table (3GPP TS 36.212 Table 5.1.3-3):
+            40..512 step 8, 528..1024 step 16, 1056..2048 step 32, 2112..6144 step 64."""
+            return (list(range(40, 513, 8)) + list(range(528, 1025, 16)) + list(range(1056, 2049, 32))
+                    + list(range(2112, 6145, 64)))
+
     class EncoderOptions:
         """Turbo::EncoderOptions -- src/detail/Turbo.h:59-72."""
 
@@ -651,3 +658,59 @@ class Turbo(Codec):
 
     def getDecoderOptions(self):
         return self._decoder
+
+
+class Batch:
+    """Extension: frames of several codecs decoded by one CUDA graph launch
+    (fecl_batch_create in include/fecl_b200.h).
+
+    jobs is a list of (codec, llr, msg) or (codec, llr, msg, iterations) with torch
+    CUDA tensors: llr [nframes * paritySize] (float16/32/64), msg [nframes * msgSize]
+    uint8, iterations [nframes] int32.  The tensors stay bound to the batch: write new
+    L-values into them and call run() again.  Results equal each codec's decode()
+    bit for bit.  autotune=True times the equivalent LDPC kernel shapes on these
+    inputs at creation and keeps the fastest."""
+
+    def __init__(self, jobs, autotune=False):
+        self._keep = []
+        arr = (_lib.fecl_batch_job * len(jobs))()
+        for i, job in enumerate(jobs):
+            codec, llr, msg = job[:3]
+            it = job[3] if len(job) > 3 else None
+            if not (_is_device(llr) and _is_device(msg) and (it is None or _is_device(it))):
+                raise ValueError("batch buffers must be CUDA tensors")
+            n = codec._frames(llr.numel(), codec.paritySize(), "parity")
+            if msg.numel() != n * codec.msgSize():
+                raise ValueError("Invalid size for message")
+            if it is not None and it.numel() != n:
+                raise ValueError("Invalid size for iterations")
+            arr[i].codec = codec._h
+            arr[i].nframes = n
+            arr[i].llr = llr.data_ptr()
+            arr[i].llr_dtype = _dtype_code(llr)
+            arr[i].msg = msg.data_ptr()
+            arr[i].iterations = it.data_ptr() if it is not None else None
+            self._keep.append((codec, llr, msg, it))
+        h = C.c_void_p()
+        _check(_L.fecl_batch_create(arr, len(jobs), _lib.BATCH_AUTOTUNE if autotune else 0, C.byref(h)))
+        self._h = h
+        self._device = jobs[0][1].device
+
+    def run(self, stream=None):
+        """Launches the batch on `stream` (default: torch's current stream)."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(self._device)
+        _check(_L.fecl_batch_run(self._h, C.c_void_p(s.cuda_stream)))
+
+    def describe(self):
+        """One line per job: the kernel it runs."""
+        buf = C.create_string_buffer(1 << 16)
+        _check(_L.fecl_batch_describe(self._h, buf, len(buf)))
+        return buf.value.decode()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and h.value:
+            _L.fecl_batch_destroy(h)
+            self._h = None
+

@@ -68,6 +68,20 @@ class fecl_so_io(C.Structure):
     ]
 
 
+class fecl_batch_job(C.Structure):
+    _fields_ = [
+        ("codec", C.c_void_p),
+        ("nframes", C.c_uint64),
+        ("llr", C.c_void_p),
+        ("llr_dtype", C.c_int32),
+        ("msg", C.c_void_p),
+        ("iterations", C.c_void_p),
+    ]
+
+
+BATCH_AUTOTUNE = 1
+
+
 # (name, restype, argtypes) for every symbol include/fecl_b200.h declares.
 SIGNATURES = [
     ("fecl_ldpc_create", C.c_int, [C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.POINTER(fecl_ldpc_options), C.POINTER(C.c_void_p)]),
@@ -92,6 +106,10 @@ SIGNATURES = [
     ("fecl_turbo_set_window_training", C.c_int, [C.c_void_p, C.c_int32]),
     ("fecl_turbo_window_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("fecl_lte_turbo_decode_noalloc", C.c_int, [C.c_uint32, C.c_int32, C.c_uint32, C.c_void_p, C.c_int32, C.c_uint64, C.c_void_p, C.c_void_p]),
+    ("fecl_batch_create", C.c_int, [C.POINTER(fecl_batch_job), C.c_uint32, C.c_int32, C.POINTER(C.c_void_p)]),
+    ("fecl_batch_run", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fecl_batch_describe", C.c_int, [C.c_void_p, C.c_char_p, C.c_uint64]),
+    ("fecl_batch_destroy", None, [C.c_void_p]),
     ("fecl_strerror", C.c_char_p, [C.c_int]),
     ("fecl_last_error", C.c_char_p, []),
     ("fecl_version", C.c_char_p, []),

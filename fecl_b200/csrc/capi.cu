@@ -15,28 +15,11 @@
 #include <string>
 #include <vector>
 
-#include "../../include/fecl_b200.h"
-#include "device/kernels.hpp"
-#include "host/codes.hpp"
-#include "host/ldpc_plan.hpp"
+#include "codec.hpp"
 
 namespace {
 
 thread_local std::string g_error;
-
-struct Error {
-  int code;
-  std::string msg;
-};
-
-[[noreturn]] void fail(int code, const std::string& msg) { throw Error{code, msg}; }
-
-void cuda_check(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    fail(e == cudaErrorMemoryAllocation ? FECL_ENOMEM : FECL_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
-  }
-}
 
 template <class F>
 int guarded(F&& f) {
@@ -58,67 +41,6 @@ int guarded(F&& f) {
   }
 }
 
-// A device allocation owned by a codec.
-struct DeviceBuffer {
-  void* ptr = nullptr;
-  size_t bytes = 0;
-  DeviceBuffer() = default;
-  DeviceBuffer(const DeviceBuffer&) = delete;
-  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-  ~DeviceBuffer() {
-    if (ptr) cudaFree(ptr);
-  }
-  void reserve(size_t n) {
-    if (n <= bytes) return;
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    bytes = 0;
-    cuda_check(cudaMalloc(&ptr, n), "cudaMalloc");
-    bytes = n;
-  }
-  template <class T>
-  void upload(const std::vector<T>& v) {
-    reserve(std::max<size_t>(v.size() * sizeof(T), 16));
-    if (!v.empty()) cuda_check(cudaMemcpy(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
-  }
-  template <class T>
-  T* as() const {
-    return static_cast<T*>(ptr);
-  }
-};
-
-// Carves aligned slices out of one workspace allocation.
-struct Carver {
-  size_t off = 0;
-  size_t take(size_t bytes) {
-    size_t o = off;
-    off += (bytes + 255) & ~size_t(255);
-    return o;
-  }
-};
-
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cuda_check(cudaSetDevice(dev), "cudaSetDevice");
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
-
-size_t dsize(int dtype) {
-  switch (dtype) {
-    case FECL_F64: return 8;
-    case FECL_F32: return 4;
-    case FECL_F16: return 2;
-  }
-  fail(FECL_EINVAL, "Invalid element type");
-}
-
 }  // namespace
 
 namespace fecl {
@@ -126,261 +48,6 @@ namespace fecl {
 void set_last_error(const std::string& msg) { g_error = msg; }
 }  // namespace fecl
 
-struct fecl_codec_s {
-  int kind = 0;  // 0 LDPC, 1 turbo
-  int device = 0;
-  std::unique_ptr<fecl::LdpcCode> ldpc;
-  std::unique_ptr<fecl::TurboCode> turbo;
-  std::mutex mu;
-  cudaStream_t stream = nullptr;   // host-memory calls: first pipeline stream
-  cudaStream_t stream2 = nullptr;  // host-memory calls: second pipeline stream
-  cudaEvent_t done = nullptr;
-  bool pending = false;
-  // device description
-  DeviceBuffer row_ptr, col_idx, col_ptr, col_edges, sf;
-  std::vector<std::unique_ptr<DeviceBuffer>> tables;
-  fecl::LdpcDeviceCode ldev;
-  fecl::TurboDeviceCode tdev;
-  // workspace
-  DeviceBuffer ws;
-
-  ~fecl_codec_s() {
-    if (stream) {
-      cudaStreamSynchronize(stream);
-      cudaStreamDestroy(stream);
-    }
-    if (stream2) {
-      cudaStreamSynchronize(stream2);
-      cudaStreamDestroy(stream2);
-    }
-    if (done) cudaEventDestroy(done);
-  }
-
-  uint64_t msg() const { return kind == 0 ? ldpc->msg_size() : turbo->msg_size(); }
-  uint64_t syst() const { return kind == 0 ? ldpc->syst_size() : turbo->syst_size(); }
-  uint64_t parity() const { return kind == 0 ? ldpc->parity_size() : turbo->parity_size(); }
-  uint64_t state() const { return kind == 0 ? ldpc->state_size() : turbo->state_size(); }
-
-  void init_runtime() {
-    int n = 0;
-    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
-      cudaGetLastError();
-      fail(FECL_ENODEV, "no CUDA device is visible");
-    }
-    cuda_check(cudaGetDevice(&device), "cudaGetDevice");
-    cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    cuda_check(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking), "cudaStreamCreate");
-    cuda_check(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "cudaEventCreate");
-    cuda_check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attribute");
-    cuda_check(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device), "attribute");
-  }
-
-  void upload_ldpc() {
-    const fecl::Csr& H = ldpc->checks();
-    row_ptr.upload(H.row_ptr);
-    col_idx.upload(H.col_idx);
-    // per-bit edge lists in increasing edge order
-    std::vector<uint32_t> cp(H.cols + 1, 0), ce(H.nnz());
-    for (auto c : H.col_idx) cp[c + 1]++;
-    for (uint32_t b = 0; b < H.cols; ++b) cp[b + 1] += cp[b];
-    std::vector<uint32_t> fill(cp.begin(), cp.end() - 1);
-    for (uint64_t e = 0; e < H.nnz(); ++e) ce[fill[H.col_idx[e]]++] = uint32_t(e);
-    col_ptr.upload(cp);
-    col_edges.upload(ce);
-    ldev.M = int32_t(H.rows);
-    ldev.N = int32_t(H.cols);
-    ldev.E = int64_t(H.nnz());
-    ldev.msg = int32_t(ldpc->msg_size());
-    ldev.d_max = int32_t(ldpc->max_check_degree());
-    ldev.row_ptr = row_ptr.as<uint32_t>();
-    ldev.col_idx = col_idx.as<uint32_t>();
-    ldev.col_ptr = col_ptr.as<uint32_t>();
-    ldev.col_edges = col_edges.as<uint32_t>();
-    upload_ldpc_options();
-  }
-
-  void upload_ldpc_options() {
-    const auto& d = ldpc->decoder();
-    const int stride = int(ldpc->max_check_degree()) - 1;
-    std::vector<float> t;
-    for (auto& row : d.scaling)
-      for (int k = 0; k < stride; ++k) t.push_back(float(row[k]));
-    sf.upload(t);
-    ldev.sf = sf.as<float>();
-    ldev.n_sf = int32_t(d.scaling.size());
-    ldev.sf_stride = stride;
-    ldev.algorithm = d.algorithm;
-    ldev.iterations = int32_t(d.iterations);
-    ldev.fixed_iterations = d.fixed_iterations;
-  }
-
-  void upload_turbo() {
-    const auto& cs = turbo->constituents();
-    if (cs.size() > size_t(fecl::kMaxConstituents)) fail(FECL_EUNSUPPORTED, "too many constituents for the device decoder");
-    tables.clear();
-    tdev.n = int32_t(cs.size());
-    tdev.msg = int32_t(turbo->msg_size());
-    tdev.syst = int32_t(turbo->syst_size());
-    tdev.parity = int32_t(turbo->parity_size());
-    tdev.state = int32_t(turbo->state_size());
-    tdev.tail = int32_t(turbo->syst_tail_size());
-    tdev.max_steps = 0;
-    tdev.max_states = 0;
-    for (size_t j = 0; j < cs.size(); ++j) {
-      const auto& c = cs[j];
-      auto& k = tdev.c[j];
-      k.state_count = int32_t(c.trellis.state_count);
-      k.input_count = int32_t(c.trellis.input_count);
-      k.input_size = int32_t(c.trellis.input_size);
-      k.output_size = int32_t(c.trellis.output_size);
-      k.length = int32_t(c.length);
-      k.tail = int32_t(c.tail);
-      k.termination = c.termination;
-      k.msg_size = int32_t(c.msg_size());
-      k.syst_size = int32_t(c.syst_size());
-      k.syst_tail_size = int32_t(c.syst_tail_size());
-      k.parity_size = int32_t(c.parity_size());
-      // interleavers are padded with zeros so that 8-entry vector loads never leave them
-      std::vector<uint32_t> padded_perm(c.perm);
-      padded_perm.resize(c.perm.size() + 16, 0);
-      for (const std::vector<uint32_t>* v : {&c.trellis.next_state, &c.trellis.output,
-                                             static_cast<const std::vector<uint32_t>*>(&padded_perm)}) {
-        tables.emplace_back(new DeviceBuffer);
-        tables.back()->upload(*v);
-      }
-      k.next_state = tables[tables.size() - 3]->as<uint32_t>();
-      k.output = tables[tables.size() - 2]->as<uint32_t>();
-      k.perm = tables[tables.size() - 1]->as<uint32_t>();
-      tdev.max_steps = std::max(tdev.max_steps, int32_t(c.length + c.tail));
-      tdev.max_states = std::max(tdev.max_states, int32_t(c.trellis.state_count));
-    }
-    upload_turbo_options();
-  }
-
-  void upload_turbo_options() {
-    const auto& d = turbo->decoder();
-    std::vector<float> t;
-    for (size_t j = 0; j < turbo->constituents().size(); ++j)
-      for (uint32_t i = 0; i < std::max<uint32_t>(d.iterations, 1); ++i) t.push_back(float(turbo->scaling_factor(i, j)));
-    sf.upload(t);
-    tdev.sf = sf.as<float>();
-    tdev.algorithm = d.algorithm;
-    tdev.iterations = int32_t(d.iterations);
-    tdev.scheduling = d.scheduling;
-  }
-
-  bool on_device = false;
-  int lte_train = -1;
-  int kernel_sel = FECL_KERNEL_AUTO;
-  bool force_generic_() const { return kernel_sel == FECL_KERNEL_GENERIC; }
-
-  // Cluster-resident LDPC decoder: partition tables per cluster size, uploaded on use.
-  struct ClusterDev {
-    fecl::LdpcClusterPlan plan;
-    bool uploaded = false;
-    DeviceBuffer row_split, bit_split, chk_addr, bit_ptr, bit_addr;
-    std::map<int, int> max_active;  // threads -> resident clusters
-  };
-  std::map<uint32_t, std::unique_ptr<ClusterDev>> cplans;
-  int cluster_size_sel = 0, cluster_threads_sel = 0;  // 0: chosen by the heuristic
-  int lanes_wave = 0;                                 // 0: chosen by the launcher
-  int smem_optin = 0, sm_count = 0;
-
-  ClusterDev& cluster_plan(uint32_t C) {
-    auto& slot = cplans[C];
-    if (!slot) {
-      slot.reset(new ClusterDev);
-      slot->plan = fecl::build_ldpc_cluster_plan(ldpc->checks(), C);
-    }
-    return *slot;
-  }
-  size_t cluster_smem(uint32_t C) {
-    auto& d = cluster_plan(C);
-    return fecl::ldpc_cluster_smem_bytes(int64_t(d.plan.max_edges), int64_t(d.plan.max_bits), ldpc->decoder().precision);
-  }
-  // Shape of the cluster decoder for a batch of n frames: the cluster size and the
-  // threads per CTA, or false when the code's messages do not fit a cluster.  The
-  // smallest cluster whose shares fit in shared memory is doubled while the batch
-  // would leave more than half of the SMs idle (up to 8 CTAs).
-  bool ldpc_cluster_shape(uint64_t n, uint32_t* C_out, int* threads_out) {
-    if (kind != 0 || kernel_sel == FECL_KERNEL_GENERIC || kernel_sel == FECL_KERNEL_LANES) return false;
-    if (ldpc->max_check_degree() > 32) return false;
-    const size_t limit = size_t(smem_optin) - 1024;  // static shared memory of the kernel
-    uint32_t C = 0;
-    for (uint32_t c = 1; c <= 16; c *= 2) {
-      if (cluster_size_sel && c != uint32_t(cluster_size_sel)) continue;
-      try {
-        if (cluster_smem(c) <= limit) {
-          C = c;
-          break;
-        }
-      } catch (const std::invalid_argument&) {
-        return false;
-      }
-    }
-    if (C == 0) return false;
-    if (!cluster_size_sel)
-      while (C < 8 && n * C * 2 <= uint64_t(sm_count) && cluster_smem(C * 2) <= limit) C *= 2;
-    int threads = cluster_threads_sel;
-    if (!threads) threads = ldpc->max_check_degree() <= 16 ? 1024 : 512;
-    if ((threads == 1024 && ldpc->max_check_degree() > 16) || (threads == 256 && ldpc->max_check_degree() <= 16))
-      threads = 512;
-    *C_out = C;
-    *threads_out = threads;
-    return true;
-  }
-  void upload_cluster(ClusterDev& d) {
-    if (d.uploaded) return;
-    d.row_split.upload(d.plan.row_split);
-    d.bit_split.upload(d.plan.bit_split);
-    d.chk_addr.upload(d.plan.chk_addr);
-    d.bit_ptr.upload(d.plan.bit_ptr);
-    d.bit_addr.upload(d.plan.bit_addr);
-    d.uploaded = true;
-  }
-  DeviceBuffer stats;  // windowed turbo counters
-  // The lane-batched LDPC kernel needs check degrees <= 32 and, unless the iteration
-  // count is fixed, a scaling that does not change across iterations (its stop test
-  // runs inside the check update of the next iteration).
-  bool ldpc_lanes_ok() const {
-    if (kind != 0 || force_generic_()) return false;
-    if (ldpc->max_check_degree() > 32) return false;
-    const auto& d = ldpc->decoder();
-    if (d.fixed_iterations) return true;
-    for (const auto& row : d.scaling)
-      if (row != d.scaling[0]) return false;
-    return true;
-  }
-  // The windowed kernel covers the LTE RSC pair with serial scheduling and FP32 messages
-  // for any K whose two exchange arrays fit in shared memory.
-  bool lte_fast_ok() const {
-    if (force_generic_() || kind != 1 || !turbo->is_lte_shape()) return false;
-    const auto& d = turbo->decoder();
-    if (d.scheduling != 0 || d.precision != 0 || d.iterations == 0) return false;
-    static const fecl::Trellis lte = fecl::lte_trellis();
-    for (const auto& c : turbo->constituents())
-      if (c.trellis.next_state != lte.next_state || c.trellis.output != lte.output) return false;
-    return turbo->msg_size() <= 12288;
-  }
-  // Device resources are created at the first decode, so that host-side operations
-  // (encode, check, the transformed matrix) work without a GPU.
-  void ensure_device() {
-    if (on_device) return;
-    init_runtime();
-    if (kind == 0) upload_ldpc();
-    else upload_turbo();
-    on_device = true;
-  }
-
-  // Orders this call after the previous device-memory call on the codec.
-  void wait_previous(cudaStream_t s) {
-    if (pending) cuda_check(cudaStreamWaitEvent(s, done, 0), "cudaStreamWaitEvent");
-  }
-  void mark(cudaStream_t s) {
-    cuda_check(cudaEventRecord(done, s), "cudaEventRecord");
-    pending = true;
-  }
-};
 
 namespace {
 
@@ -447,21 +114,12 @@ fecl_codec_s* checked(fecl_codec_t c) {
   return c;
 }
 
-// Device pointers of one decode launch (inputs, outputs, scratch).
-struct Launch {
-  const void *llr = nullptr, *syst = nullptr, *state = nullptr;
-  uint8_t* hard = nullptr;
-  int32_t* iters = nullptr;
-  void *msg = nullptr, *syst_out = nullptr, *parity_out = nullptr, *state_out = nullptr;
-  char* scratch = nullptr;
-};
 
-// Scratch of the decoder kernels for n frames, with the offsets of its parts.
-struct ScratchPlan {
-  size_t bytes = 0, o1 = 0, o2 = 0, o3 = 0, o4 = 0, o5 = 0;
-  uint32_t cluster = 0;  // > 0: the cluster-resident LDPC decoder with this many CTAs per frame
-  int threads = 0, clusters = 0;
-};
+
+}  // namespace
+
+namespace fecl {
+namespace capi {
 
 ScratchPlan plan_scratch(fecl_codec_s* c, uint64_t n, bool lte_fast) {
   Carver cv;
@@ -664,6 +322,11 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
   cuda_check(e, "kernel launch");
 }
 
+}  // namespace capi
+}  // namespace fecl
+
+namespace {
+
 // Grows the workspace to `bytes`; the old one may still be read by queued work.
 void reserve_workspace(fecl_codec_s* c, size_t bytes) {
   if (c->ws.bytes >= bytes) return;
@@ -832,6 +495,7 @@ int fecl_ldpc_set_options(fecl_codec_t codec, const fecl_ldpc_options* options) 
     if (c->kind != 0) fail(FECL_EINVAL, "not an LDPC codec");
     std::lock_guard<std::mutex> lk(c->mu);
     c->ldpc->set_decoder(ldpc_config(options, c->ldpc->max_check_degree()));
+    c->generation.fetch_add(1);
     if (c->on_device) {
       DeviceGuard dg(c->device);
       if (c->pending) cuda_check(cudaEventSynchronize(c->done), "cudaEventSynchronize");
@@ -927,6 +591,7 @@ int fecl_turbo_set_options(fecl_codec_t codec, const fecl_turbo_options* options
     if (c->kind != 1) fail(FECL_EINVAL, "not a turbo codec");
     std::lock_guard<std::mutex> lk(c->mu);
     c->turbo->set_decoder(turbo_config(options));
+    c->generation.fetch_add(1);
     if (c->on_device) {
       DeviceGuard dg(c->device);
       if (c->pending) cuda_check(cudaEventSynchronize(c->done), "cudaEventSynchronize");

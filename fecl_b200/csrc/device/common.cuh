@@ -3,7 +3,10 @@
 
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
+
+#include <atomic>
 
 namespace fecl {
 
@@ -33,6 +36,28 @@ inline size_t dtype_size(int dtype) { return dtype == kF64 ? 8 : (dtype == kF16 
 struct LinearLut {
   float y[8];
 };
+
+// The table's values, computed on the host.
+inline LinearLut make_linear_lut() {
+  LinearLut l;
+  for (int i = 0; i < 8; ++i) l.y[i] = float(log(1.0 + exp(-(double(i) / 2.0))));
+  return l;
+}
+
+// Runs `upload` (which fills a translation unit's __constant__ tables) once per
+// device, with that device current.  __constant__ memory is per device, so a
+// process that decodes on several GPUs needs one upload on each.
+template <class F>
+inline cudaError_t once_per_device(std::atomic<unsigned long long>& done, F&& upload) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load() & bit) return cudaSuccess;
+  e = upload();
+  if (e == cudaSuccess) done.fetch_or(bit);
+  return e;
+}
 
 __device__ __forceinline__ float lut_log1pexpm(const LinearLut& t, float x) {
   x *= 2.0f;

@@ -199,4 +199,45 @@ struct TurboLteParams {
 size_t turbo_lte_scratch_bytes(int K, int64_t nframes);
 cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s);
 
+// The same windowed decoder over a batch of frames of different K (any K <= 12288),
+// one descriptor per frame, in one persistent launch (plus one staging launch).
+struct TurboLteBatchFrame {
+  const void* llr = nullptr;       // [3K+12] L-values of llr_dtype, FeCl's turbo layout
+  uint8_t* hard = nullptr;         // [K]
+  int32_t* iters = nullptr;        // nullable
+  float* scratch = nullptr;        // turbo_lte_frame_floats(K) floats, 16-byte aligned
+  const uint32_t* perm = nullptr;  // interleaver of constituent 1, padded by 16 entries
+  const float* sf = nullptr;       // [2][iterations] scaling of the extrinsic values
+  int32_t K = 0, iterations = 0, llr_dtype = 1, pad = 0;
+};
+struct TurboLteBatchParams {
+  const TurboLteBatchFrame* frames = nullptr;  // device array; frames are taken in this order
+  int64_t nframes = 0;
+  int32_t* counter = nullptr;  // device int, zeroed by the launcher
+  int32_t max_K = 0;           // largest K in the batch (sizes shared memory)
+  int32_t algorithm = 2;       // one algorithm per launch
+  int32_t train = -1;          // training steps (-1: default)
+  int32_t ctas = 0;            // persistent CTAs (0: as many as are resident at once)
+  unsigned long long* stats = nullptr;
+};
+size_t turbo_lte_frame_floats(int K);
+int turbo_lte_batch_max_ctas(int max_K, int algorithm);
+cudaError_t launch_turbo_lte_batch(const TurboLteBatchParams& p, cudaStream_t s);
+
+// Uploads of every translation unit's __constant__ tables to the current device
+// (each launcher calls its own; a stream capture must run them before it starts).
+cudaError_t ldpc_flood_init();
+cudaError_t ldpc_lanes_init();
+cudaError_t ldpc_cluster_init();
+cudaError_t turbo_generic_init();
+cudaError_t turbo_lte_init();
+inline cudaError_t init_device_constants() {
+  cudaError_t e;
+  if ((e = ldpc_flood_init()) != cudaSuccess) return e;
+  if ((e = ldpc_lanes_init()) != cudaSuccess) return e;
+  if ((e = ldpc_cluster_init()) != cudaSuccess) return e;
+  if ((e = turbo_generic_init()) != cudaSuccess) return e;
+  return turbo_lte_init();
+}
+
 }  // namespace fecl

@@ -348,19 +348,22 @@ size_t msg_bytes(int msg_type) { return msg_type == 1 ? 2 : (msg_type == 2 ? 1 :
 
 }  // namespace
 
+cudaError_t ldpc_cluster_init() {
+  static std::atomic<unsigned long long> done{0};
+  return once_per_device(done, [] {
+    const LinearLut l = make_linear_lut();
+    return cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
+  });
+}
+
 size_t ldpc_cluster_smem_bytes(int64_t max_edges, int64_t max_bits, int msg_type) {
   const size_t c2v = (size_t(max_edges) * msg_bytes(msg_type) + 15) & ~size_t(15);
   return c2v + size_t(max_bits) * 8;
 }
 
 cudaError_t launch_ldpc_cluster(LdpcClusterParams p, cudaStream_t s) {
-  static bool lut_ready = false;
-  if (!lut_ready) {
-    const LinearLut l = ldpc::linear_lut();
-    cudaError_t e = cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
-    if (e != cudaSuccess) return e;
-    lut_ready = true;
-  }
+  cudaError_t e0 = ldpc_cluster_init();
+  if (e0 != cudaSuccess) return e0;
   if (p.nframes <= 0) return cudaSuccess;
   if (p.cluster < 1 || p.cluster > 16 || (p.cluster & (p.cluster - 1))) return cudaErrorInvalidValue;
   const size_t smem = ldpc_cluster_smem_bytes(p.max_edges, p.max_bits, p.msg_type);

@@ -209,15 +209,17 @@ cudaError_t launch_alg(const LdpcDeviceCode& c, const LdpcRun& p, cudaStream_t s
 
 }  // namespace
 
+cudaError_t ldpc_flood_init() {
+  static std::atomic<unsigned long long> done{0};
+  return once_per_device(done, [] {
+    const LinearLut l = make_linear_lut();
+    return cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
+  });
+}
+
 cudaError_t launch_ldpc_flood(const LdpcDeviceCode& c, const LdpcRun& p, cudaStream_t s) {
-  static bool lut_ready = false;
-  if (!lut_ready) {
-    LinearLut l;
-    for (int i = 0; i < 8; ++i) l.y[i] = float(log(1.0 + exp(-(double(i) / 2.0))));
-    cudaError_t e = cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
-    if (e != cudaSuccess) return e;
-    lut_ready = true;
-  }
+  cudaError_t e0 = ldpc_flood_init();
+  if (e0 != cudaSuccess) return e0;
   if (p.nframes <= 0) return cudaSuccess;
   switch (c.algorithm) {
     case kExact: return launch_alg<kExact>(c, p, s);

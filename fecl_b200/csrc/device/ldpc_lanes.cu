@@ -313,6 +313,14 @@ cudaError_t run_m(const LdpcLanesParams& p, cudaStream_t s) {
 
 }  // namespace
 
+cudaError_t ldpc_lanes_init() {
+  static std::atomic<unsigned long long> done{0};
+  return once_per_device(done, [] {
+    const LinearLut l = make_linear_lut();
+    return cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
+  });
+}
+
 size_t ldpc_lanes_scratch_bytes(int64_t N, int64_t E, int64_t nframes, int msg_type) {
   const int64_t groups = (nframes + kLanes - 1) / kLanes;
   const size_t msg_bytes = msg_type == 1 ? 2 : (msg_type == 2 ? 1 : 4);
@@ -322,13 +330,8 @@ size_t ldpc_lanes_scratch_bytes(int64_t N, int64_t E, int64_t nframes, int msg_t
 }
 
 cudaError_t launch_ldpc_lanes(LdpcLanesParams p, void* scratch, cudaStream_t s) {
-  static bool lut_ready = false;
-  if (!lut_ready) {
-    const LinearLut l = ldpc::linear_lut();
-    cudaError_t e = cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
-    if (e != cudaSuccess) return e;
-    lut_ready = true;
-  }
+  cudaError_t e0 = ldpc_lanes_init();
+  if (e0 != cudaSuccess) return e0;
   if (p.nframes <= 0) return cudaSuccess;
   p.groups = int32_t((p.nframes + kLanes - 1) / kLanes);
   const size_t msg_bytes = p.msg_type == 1 ? 2 : (p.msg_type == 2 ? 1 : 4);

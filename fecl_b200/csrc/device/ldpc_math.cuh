@@ -166,12 +166,5 @@ __device__ __forceinline__ void row_update(const LinearLut& lut, const float v[D
   }
 }
 
-// The reference's 8-point table of log(1 + exp(-x)) at x = i/2 (src/detail/LinearTable.h:56-81).
-inline LinearLut linear_lut() {
-  LinearLut l;
-  for (int i = 0; i < 8; ++i) l.y[i] = float(log(1.0 + exp(-(double(i) / 2.0))));
-  return l;
-}
-
 }  // namespace ldpc
 }  // namespace fecl

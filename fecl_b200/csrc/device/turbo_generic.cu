@@ -336,15 +336,17 @@ __global__ void __launch_bounds__(64) turbo_generic_f32(TurboDeviceCode c, Turbo
 
 }  // namespace
 
+cudaError_t turbo_generic_init() {
+  static std::atomic<unsigned long long> done{0};
+  return once_per_device(done, [] {
+    const LinearLut l = make_linear_lut();
+    return cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
+  });
+}
+
 cudaError_t launch_turbo_generic(const TurboDeviceCode& c, const TurboRun& p, cudaStream_t s) {
-  static bool lut_ready = false;
-  if (!lut_ready) {
-    LinearLut l;
-    for (int i = 0; i < 8; ++i) l.y[i] = float(log(1.0 + exp(-(double(i) / 2.0))));
-    cudaError_t e = cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
-    if (e != cudaSuccess) return e;
-    lut_ready = true;
-  }
+  cudaError_t e0 = turbo_generic_init();
+  if (e0 != cudaSuccess) return e0;
   if (p.nframes <= 0) return cudaSuccess;
   if (c.max_states > kMaxS) return cudaErrorInvalidValue;
   for (int j = 0; j < c.n; ++j)

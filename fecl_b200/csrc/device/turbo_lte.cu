@@ -315,28 +315,39 @@ __device__ __forceinline__ bool close8(const float* x, const float* y) {
   return ok;
 }
 
+// One frame's geometry and buffers, as the decode loop below sees them.
+struct LteJob {
+  int32_t K = 0, Kp = 0, Tp = 0, seg_len = 0, train = 0, iterations = 0;
+  const float* sf = nullptr;            // [2][iterations]
+  const uint32_t* perm = nullptr;       // interleaver of constituent 1, padded by 16 entries
+  const float* scratch = nullptr;       // staged L-values: Ls [Kp] | Lp0 [Tp] | Lp1 [Tp] | tail [8]
+  float* ck = nullptr;                  // checkpoints [2][nblk + 1][8]
+  uint8_t* hard = nullptr;              // [K]
+  int32_t* iters = nullptr;             // nullable
+  unsigned long long* stats = nullptr;  // nullable
+};
+
+// Decodes one frame with the whole CTA; smem holds 2 * Kp floats + Shared.
 template <int ALG>
-__global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p) {
-  extern __shared__ float smem[];
-  const int K = p.K, T = p.K + 3;
+__device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
+  const int K = q.K, T = q.K + 3;
   const int nblk = (T + kBlk - 1) / kBlk;
   float* X = smem;
-  float* Y = smem + p.Kp;
-  Shared& sh = *reinterpret_cast<Shared*>(smem + 2 * p.Kp);
-  const int64_t f = blockIdx.x;
+  float* Y = smem + q.Kp;
+  Shared& sh = *reinterpret_cast<Shared*>(smem + 2 * q.Kp);
   Frame fr;
-  const float* base = p.scratch + f * p.frame_stride;
+  const float* base = q.scratch;
   fr.Ls = base;
-  fr.Lp0 = base + p.Kp;
-  fr.Lp1 = base + p.Kp + p.Tp;
-  fr.ts = base + p.Kp + 2 * p.Tp;
-  fr.cka = p.ck + f * int64_t(2 * (nblk + 1) * 8);
+  fr.Lp0 = base + q.Kp;
+  fr.Lp1 = base + q.Kp + q.Tp;
+  fr.ts = base + q.Kp + 2 * q.Tp;
+  fr.cka = q.ck;
   fr.ckb = fr.cka + (nblk + 1) * 8;
   const int tid = threadIdx.x;
-  const int L = p.seg_len;
+  const int L = q.seg_len;
   const int S = (T + L - 1) / L;
 
-  for (int k = tid; k < p.Kp; k += kThreads) {
+  for (int k = tid; k < q.Kp; k += kThreads) {
     X[k] = 0.0f;
     Y[k] = 0.0f;
   }
@@ -346,9 +357,9 @@ __global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p
   }
   __syncthreads();
 
-  for (int it = 0; it < p.iterations; ++it) {
+  for (int it = 0; it < q.iterations; ++it) {
     for (int j = 0; j < 2; ++j) {
-      const uint32_t* perm = j == 0 ? p.perm[0] : p.perm[1];
+      const uint32_t* perm = q.perm;
       // ---- A: segments with training starts
       {
         const bool fwd = tid < kSegs;
@@ -358,12 +369,12 @@ __global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p
           int t_train;
           const float* vin;
           if (fwd) {
-            const bool exact = (w == 0 || a0 - p.train <= 0);
-            t_train = exact ? 0 : a0 - p.train;
+            const bool exact = (w == 0 || a0 - q.train <= 0);
+            t_train = exact ? 0 : a0 - q.train;
             vin = exact ? sh.term : sh.flat;
           } else {
-            const bool exact = (w == S - 1 || a1 + p.train >= T);
-            t_train = exact ? T : a1 + p.train;
+            const bool exact = (w == S - 1 || a1 + q.train >= T);
+            t_train = exact ? T : a1 + q.train;
             vin = exact ? sh.term : sh.flat;
           }
           segment_walk<ALG>(fwd, j, t_train, a0, a1, vin, sh.sv[fwd ? 0 : 1][w], sh.ev[fwd ? 0 : 1][w], K, T, fr, X,
@@ -404,7 +415,7 @@ __global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p
           }
           __syncthreads();
           if (mine) {
-            if (p.stats) atomicAdd(p.stats + 2, 1ull);
+            if (q.stats) atomicAdd(q.stats + 2, 1ull);
             const int a0 = w * L, a1 = min(T, a0 + L);
             segment_walk<ALG>(fwd, j, fwd ? a0 : a1, a0, a1, sh.in[fwd ? 0 : 1][w], sh.sv[fwd ? 0 : 1][w],
                               sh.ev[fwd ? 0 : 1][w], K, T, fr, X, Y, perm);
@@ -412,12 +423,12 @@ __global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p
         }
         __syncthreads();
       }
-      if (p.stats && tid == 0) {
-        atomicAdd(p.stats + 0, 1ull);
-        atomicAdd(p.stats + 1, (unsigned long long)rounds);
+      if (q.stats && tid == 0) {
+        atomicAdd(q.stats + 0, 1ull);
+        atomicAdd(q.stats + 1, (unsigned long long)rounds);
       }
       // ---- B: 8-step blocks, extrinsic output
-      const float sf = p.sf[j * p.iterations + it];
+      const float sf = q.sf[j * q.iterations + it];
       float* out = j == 0 ? X : Y;
       for (int b = tid; b < nblk; b += kThreads) {
         const int t0 = b * kBlk;
@@ -476,9 +487,32 @@ __global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p
     }
   }
   // a-posteriori and hard decision, TurboDecoderImpl.cpp:64-71
-  for (int k = tid; k < K; k += kThreads) p.hard[f * K + k] = uint8_t((X[k] + Y[k]) > 0.0f);
-  if (p.iters && tid == 0) p.iters[f] = p.iterations;
+  for (int k = tid; k < K; k += kThreads) q.hard[k] = uint8_t((X[k] + Y[k]) > 0.0f);
+  if (q.iters && tid == 0) *q.iters = q.iterations;
 }
+
+template <int ALG>
+__global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p) {
+  extern __shared__ float smem[];
+  const int64_t f = blockIdx.x;
+  const int nblk = (p.K + 3 + kBlk - 1) / kBlk;
+  LteJob q;
+  q.K = p.K;
+  q.Kp = p.Kp;
+  q.Tp = p.Tp;
+  q.seg_len = p.seg_len;
+  q.train = p.train;
+  q.iterations = p.iterations;
+  q.sf = p.sf;
+  q.perm = p.perm[1];
+  q.scratch = p.scratch + f * p.frame_stride;
+  q.ck = p.ck + f * int64_t(2 * (nblk + 1) * 8);
+  q.hard = p.hard + f * p.K;
+  q.iters = p.iters ? p.iters + f : nullptr;
+  q.stats = p.stats;
+  decode_lte_frame<ALG>(q, smem);
+}
+
 
 // Input [f][3K+12] in FeCl's turbo layout -> padded FP32 scratch.
 __global__ void turbo_lte_stage(TurboLteParams p) {
@@ -502,7 +536,90 @@ __global__ void turbo_lte_stage(TurboLteParams p) {
   }
 }
 
+// Geometry of a frame of K message bits: T trellis steps, nblk 8-step blocks, the
+// padded systematic / parity lengths Kp = Tp, the staged-input stride and the
+// segment length of the 64 forward and 64 backward segments.
+struct LteGeometry {
+  int T, nblk, Tp, Kp, stride, seg_len;
+  __host__ __device__ explicit LteGeometry(int K) {
+    T = K + 3;
+    nblk = (T + kBlk - 1) / kBlk;
+    Tp = nblk * kBlk;
+    Kp = Tp;
+    stride = Kp + 2 * Tp + 8;
+    const int L = (T + kSegs - 1) / kSegs;
+    seg_len = (L + kBlk - 1) / kBlk * kBlk;
+  }
+  // Staged inputs then checkpoints, rounded to 128 bytes so frames share no cache line.
+  __host__ __device__ int frame_floats() const { return (stride + 2 * (nblk + 1) * 8 + 31) & ~31; }
+};
+
+// Stages element i of a frame's staged inputs from FeCl's turbo layout
+// | msg [K] | systTail1 [3] | systTail2 [3] | parity1 [K+3] | parity2 [K+3] |.
+__device__ __forceinline__ float staged_value(const void* llr, int dtype, int64_t in0, int K, int Kp, int Tp, int i) {
+  if (i < Kp) return i < K ? load_llr(llr, dtype, in0 + i) : 0.0f;
+  if (i < Kp + 2 * Tp) {
+    const int c = (i - Kp) / Tp, t = (i - Kp) % Tp;
+    return t < K + 3 ? load_llr(llr, dtype, in0 + K + 6 + c * (K + 3) + t) : 0.0f;
+  }
+  const int t = i - Kp - 2 * Tp;
+  return t < 6 ? load_llr(llr, dtype, in0 + K + t) : 0.0f;
+}
+
+// Mixed-K batch, staging: one block per frame (grid-strided).
+__global__ void turbo_lte_batch_stage(TurboLteBatchParams p) {
+  for (int64_t f = blockIdx.x; f < p.nframes; f += gridDim.x) {
+    const TurboLteBatchFrame d = p.frames[f];
+    const LteGeometry g(d.K);
+    for (int i = threadIdx.x; i < g.stride; i += blockDim.x)
+      d.scratch[i] = staged_value(d.llr, d.llr_dtype, 0, d.K, g.Kp, g.Tp, i);
+  }
+}
+
+// Mixed-K batch, decoding: persistent CTAs take frames from a counter in the order
+// of the descriptor table (longest first), so frames of every size share one launch
+// and the long ones do not trail behind.  Shared memory is sized for the largest K.
+template <int ALG>
+__global__ void __launch_bounds__(kThreads, 3) turbo_lte_batch_kernel(TurboLteBatchParams p) {
+  extern __shared__ float smem[];
+  __shared__ int next;
+  for (;;) {
+    __syncthreads();  // every thread has read `next` (and finished the last frame)
+    if (threadIdx.x == 0) next = atomicAdd(p.counter, 1);
+    __syncthreads();
+    const int64_t f = next;
+    if (f >= p.nframes) break;
+    const TurboLteBatchFrame d = p.frames[f];
+    const LteGeometry g(d.K);
+    LteJob q;
+    q.K = d.K;
+    q.Kp = g.Kp;
+    q.Tp = g.Tp;
+    q.seg_len = g.seg_len;
+    q.train = p.train;
+    q.iterations = d.iterations;
+    q.sf = d.sf;
+    q.perm = d.perm;
+    q.scratch = d.scratch;
+    q.ck = d.scratch + g.stride;
+    q.hard = d.hard;
+    q.iters = d.iters;
+    q.stats = p.stats;
+    decode_lte_frame<ALG>(q, smem);
+  }
+}
+
+size_t batch_smem_bytes(int max_K) { return size_t(2 * LteGeometry(max_K).Kp) * sizeof(float) + sizeof(Shared); }
+
 }  // namespace
+
+cudaError_t turbo_lte_init() {
+  static std::atomic<unsigned long long> done{0};
+  return once_per_device(done, [] {
+    const LinearLut l = make_linear_lut();
+    return cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
+  });
+}
 
 size_t turbo_lte_scratch_bytes(int K, int64_t nframes) {
   const int T = K + 3;
@@ -514,14 +631,8 @@ size_t turbo_lte_scratch_bytes(int K, int64_t nframes) {
 }
 
 cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
-  static bool init = false;
-  if (!init) {
-    LinearLut l;
-    for (int i = 0; i < 8; ++i) l.y[i] = float(log(1.0 + exp(-(double(i) / 2.0))));
-    cudaError_t e = cudaMemcpyToSymbol(c_lut, &l, sizeof(l));
-    if (e != cudaSuccess) return e;
-    init = true;
-  }
+  cudaError_t e0 = turbo_lte_init();
+  if (e0 != cudaSuccess) return e0;
   if (p.nframes <= 0) return cudaSuccess;
   const int T = p.K + 3;
   const int nblk = (T + kBlk - 1) / kBlk;
@@ -545,6 +656,58 @@ cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
     case kExact: return launch(turbo_lte_kernel<kExact>);
     case kLinear: return launch(turbo_lte_kernel<kLinear>);
     default: return launch(turbo_lte_kernel<kApproximate>);
+  }
+}
+
+size_t turbo_lte_frame_floats(int K) { return size_t(LteGeometry(K).frame_floats()); }
+
+int turbo_lte_batch_max_ctas(int max_K, int algorithm) {
+  const size_t smem = batch_smem_bytes(max_K);
+  int per_sm = 0, sms = 0, dev = 0;
+  auto q = [&](auto kern) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 0;
+    }
+  };
+  switch (algorithm) {
+    case kExact: q(turbo_lte_batch_kernel<kExact>); break;
+    case kLinear: q(turbo_lte_batch_kernel<kLinear>); break;
+    default: q(turbo_lte_batch_kernel<kApproximate>); break;
+  }
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return per_sm * sms;
+}
+
+cudaError_t launch_turbo_lte_batch(const TurboLteBatchParams& p, cudaStream_t s) {
+  cudaError_t e = turbo_lte_init();
+  if (e != cudaSuccess) return e;
+  if (p.nframes <= 0) return cudaSuccess;
+  if (p.max_K <= 0 || p.max_K > 12288) return cudaErrorInvalidValue;
+  TurboLteBatchParams q = p;
+  if (q.train < 0) q.train = 96;
+  e = cudaMemsetAsync(q.counter, 0, sizeof(int32_t), s);
+  if (e != cudaSuccess) return e;
+  const unsigned stage_blocks = unsigned(q.nframes < 148 * 8 ? q.nframes : 148 * 8);
+  turbo_lte_batch_stage<<<stage_blocks, 256, 0, s>>>(q);
+  const size_t smem = batch_smem_bytes(q.max_K);
+  int ctas = q.ctas > 0 ? q.ctas : turbo_lte_batch_max_ctas(q.max_K, q.algorithm);
+  if (ctas <= 0) return cudaErrorInvalidConfiguration;
+  if (int64_t(ctas) > q.nframes) ctas = int(q.nframes);
+  auto launch = [&](auto kern) -> cudaError_t {
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (err != cudaSuccess) return err;
+    kern<<<unsigned(ctas), kThreads, smem, s>>>(q);
+    return cudaGetLastError();
+  };
+  switch (q.algorithm) {
+    case kExact: return launch(turbo_lte_batch_kernel<kExact>);
+    case kLinear: return launch(turbo_lte_batch_kernel<kLinear>);
+    default: return launch(turbo_lte_batch_kernel<kApproximate>);
   }
 }
 

@@ -263,6 +263,38 @@ int fecl_turbo_window_stats(fecl_codec_t codec, uint64_t* passes, uint64_t* fixu
 int fecl_lte_turbo_decode_noalloc(uint32_t K, int32_t algorithm, uint32_t iterations, const void* llr,
                                   int32_t llr_dtype, uint64_t nframes, uint8_t* msg, void* stream);
 
+/* ---- mixed batches (an extension) ------------------------------------------
+ *
+ * A batch decodes the frames of several codecs -- LDPC codes of any size and rate,
+ * LTE turbo codes of any K, any other turbo code -- with one CUDA graph launch.
+ * Every LTE turbo frame goes into one persistent launch over all K (longest
+ * frames first); every other job gets the decoder fecl_decode would pick for it,
+ * or, with FECL_BATCH_AUTOTUNE, the fastest of the LDPC kernel shapes that compute
+ * the same bits, timed on the job's own data at creation and remembered for the
+ * process.  Results equal those of fecl_decode on each job alone, bit for bit.
+ *
+ * Buffers are device memory of the codecs' device and stay bound to the batch:
+ * write new L-values into the same buffers and run the batch again.  Runs of one
+ * batch share its workspace and must not overlap (run it on one stream).  A codec
+ * must outlive every batch that uses it; changing a codec's decoder options makes
+ * fecl_batch_run fail with FECL_EINVAL until the batch is built again. */
+typedef struct fecl_batch_s* fecl_batch_t;
+typedef struct {
+  fecl_codec_t codec;
+  uint64_t nframes;
+  const void* llr;     /* [nframes][paritySize] of llr_dtype, device memory */
+  int32_t llr_dtype;
+  uint8_t* msg;        /* [nframes][msgSize] hard decisions, device memory */
+  int32_t* iterations; /* [nframes] or NULL */
+} fecl_batch_job;
+#define FECL_BATCH_AUTOTUNE 1
+int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags, fecl_batch_t* out);
+/* Launches the batch's graph on `stream` (asynchronous). */
+int fecl_batch_run(fecl_batch_t batch, void* stream);
+/* The kernel each job got, one line per job, NUL-terminated into text[size]. */
+int fecl_batch_describe(fecl_batch_t batch, char* text, uint64_t size);
+void fecl_batch_destroy(fecl_batch_t batch);
+
 const char* fecl_strerror(int status);
 /* Message of the last failing call on this thread. */
 const char* fecl_last_error(void);
