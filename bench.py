@@ -654,13 +654,101 @@ def run_mixed(args):
     return 0
 
 
+# ---- serving (--workload serving) -----------------------------------------------------
+
+SERVING_RATES = [1000, 5000, 20000, 50000, 100000, 200000]
+
+
+def run_serving(args):
+    """Poisson request streams at SERVING_RATES frames/s against the decode server
+    (one frame per request, the mix of the mixed batch: 50 % LTE turbo, 40 % DVB-S2
+    short, 10 % DVB-S2 normal, Eb/N0 U(0.5, 3.0), FP16 L-values, 40 GiB admission
+    budget).  Requests cycle over a pool of distinct frames; each rate replays
+    `--serve-seconds` of arrivals and waits for the last completion."""
+    import numpy as np
+    import torch
+    import fecl_b200 as F
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1 and rank != 0:
+        return 0
+    pool_n = args.frames or 2048
+    reqs = mixed_requests(pool_n, SEED + 7)
+    codes = MixedCodes(1)
+    pool = mixed_inputs(reqs, codes, SEED + 7)
+    srv = F.Server(device_budget=40 << 30, max_batch_frames=args.serve_batch, slots=args.serve_slots)
+    # warm-up: every code once
+    seen = {}
+    for key, _, llr in pool:
+        if key not in seen:
+            seen[key] = srv.submit(codes.get(key), llr)
+    for t in seen.values():
+        srv.wait(t)
+    rows = []
+    rng = np.random.default_rng(SEED + 11)
+    peak = None
+    for rate in SERVING_RATES:
+        n = max(200, int(rate * args.serve_seconds))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+        order = rng.integers(0, len(pool), size=n)
+        batch = [(codes.get(pool[i][0]), pool[i][2]) for i in order]
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        outs, lat = srv.replay(arrivals, batch)
+        wall = time.perf_counter() - t0
+        rep = srv.report()
+        errs = sum(int(np.any(o != pool[i][1])) for o, i in zip(outs, order))
+        bits = sum(pool[i][1].size for i in order)
+        row = {"offered_frames_per_s": rate, "requests": n, "sustained_info_mbps": round(bits / rep["wall_s"] / 1e6, 2),
+               "completed_frames_per_s": round(n / rep["wall_s"], 1), "p50_ms": round(1e3 * float(np.median(lat)), 3),
+               "p99_ms": round(1e3 * float(np.quantile(lat, 0.99)), 3), "batches": rep["batches"],
+               "fer": round(errs / n, 4), "replay_wall_s": round(wall, 3)}
+        rows.append(row)
+        if peak is None or row["sustained_info_mbps"] > peak["sustained_info_mbps"]:
+            peak = row
+    srv.close()
+
+    # the plain per-request FP32 GPU decoder: one decode call per frame, host L-values
+    sample = pool[: min(len(pool), args.plain_sample)]
+    pcodes = MixedCodes(0)
+    for key, _, llr in sample[:8]:
+        pcodes.get(key).decode(llr)
+    t1 = time.perf_counter()
+    pouts = [pcodes.get(key).decode(llr) for key, _, llr in sample]
+    pt = time.perf_counter() - t1
+    perr = sum(int(np.any(o != m)) for o, (_, m, _) in zip(pouts, sample))
+    plain = {"value": round(sum(m.size for _, m, _ in sample) / pt / 1e6, 2), "unit": "Mbit/s", "frames": len(sample),
+             "fer": round(perr / len(sample), 4), "what": "one decode call per frame, FP32 messages, host L-values"}
+    line = {
+        "metric": METRIC, "value": peak["sustained_info_mbps"], "unit": "Mbit/s", "n_gpus": 1, "steps": len(SERVING_RATES),
+        "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f16", "data": "synthetic",
+        "config": {"workload": "decode server, Poisson arrivals of single-frame requests at %s frames/s: 50%% LTE turbo "
+                               "(K uniform over the 188 QPP sizes), 40%% DVB-S2 short, 10%% DVB-S2 normal LDPC (rates "
+                               "1/2..5/6), Eb/N0 U(0.5, 3.0) dB, FP16 L-values and LDPC messages, 40 GiB budget"
+                               % SERVING_RATES,
+                   "pool_frames": len(pool), "slots": args.serve_slots, "max_batch_frames": args.serve_batch,
+                   "seconds_per_rate": args.serve_seconds},
+        "serving": rows,
+        "latency_ms": {"p50": peak["p50_ms"], "p99": peak["p99_ms"], "at_offered_frames_per_s": peak["offered_frames_per_s"]},
+        "e2e": {"value": peak["sustained_info_mbps"], "unit": "Mbit/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "note": "every request goes host -> device -> host through the server"},
+        "plain_per_request_fp32": plain,
+        "speedup_vs_plain_per_request": round(peak["sustained_info_mbps"] / plain["value"], 1),
+        "gpu_launches": None,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lte-turbo", choices=["lte-turbo", "mixed"] + sorted(LDPC_WORKLOADS),
+    ap.add_argument("--workload", default="lte-turbo", choices=["lte-turbo", "mixed", "serving"] + sorted(LDPC_WORKLOADS),
                     help="lte-turbo is the headline workload; the LDPC workloads print the same line for BP")
     ap.add_argument("--frames", type=int, default=0,
                     help="LDPC workloads: frames per code instead of the workload's (small cases for ncu)")
@@ -675,6 +763,9 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="mixed: build the batch without autotuning")
     ap.add_argument("--no-plain", action="store_true", help="mixed: skip the per-request FP32 comparison")
     ap.add_argument("--plain-sample", type=int, default=256, help="mixed: requests decoded one by one for the comparison")
+    ap.add_argument("--serve-seconds", type=float, default=0.25, help="serving: seconds of arrivals per rate")
+    ap.add_argument("--serve-slots", type=int, default=3, help="serving: batches in flight")
+    ap.add_argument("--serve-batch", type=int, default=2048, help="serving: frames per batch at most")
     ap.add_argument("--profile-decodes", type=int, default=0,
                     help="only run this many decodes of the workload (for ncu captures) and exit")
     args = ap.parse_args()
@@ -684,6 +775,8 @@ def main():
         return run_ldpc(args)
     if args.workload == "mixed":
         return run_mixed(args)
+    if args.workload == "serving":
+        return run_serving(args)
 
     import numpy as np
     import torch

@@ -26,7 +26,7 @@ from ._lib import lib as _L
 
 __all__ = [
     "Exact", "Linear", "Approximate", "Serial", "Parallel", "Custom",
-    "SparseBitMatrix", "Trellis", "Codec", "Ldpc", "Turbo", "Batch", "FeclError", "lib_path",
+    "SparseBitMatrix", "Trellis", "Codec", "Ldpc", "Turbo", "Batch", "Server", "FeclError", "lib_path",
 ]
 
 # DecoderAlgorithm (src/DecoderAlgorithm.h:30-34) and SchedulingType (src/SchedulingType.h:32-39)
@@ -713,4 +713,87 @@ class Batch:
         if h and h.value:
             _L.fecl_batch_destroy(h)
             self._h = None
+
+
+class Server:
+    """Extension: a decode server with continuous batching (fecl_server_* in
+    include/fecl_b200.h).  Requests are numpy arrays of host L-values; the server
+    batches whatever is waiting whenever one of its `slots` in-flight batches
+    finishes, within device_budget bytes of device memory."""
+
+    def __init__(self, device_budget=40 << 30, max_batch_frames=2048, slots=3):
+        o = _lib.fecl_server_options(int(device_budget), int(max_batch_frames), int(slots))
+        h = C.c_void_p()
+        _check(_L.fecl_server_create(C.byref(o), C.byref(h)))
+        self._h = h
+        self._pending = {}
+
+    def submit(self, codec, llr, iterations=False):
+        """Queues the frames in `llr` (numpy, float16/32/64); returns a ticket."""
+        x = np.asarray(llr)
+        if x.dtype not in (np.float64, np.float32, np.float16):
+            x = x.astype(np.float64)
+        x = np.ascontiguousarray(x.ravel())
+        n = codec._frames(x.size, codec.paritySize(), "parity")
+        msg = np.zeros(n * codec.msgSize(), np.uint8)
+        it = np.zeros(n, np.int32) if iterations else None
+        t = C.c_uint64()
+        _check(_L.fecl_server_submit(self._h, codec._h, _ptr(x), _dtype_code(x), n, _ptr(msg),
+                                     _ptr(it) if it is not None else None, C.byref(t)))
+        self._pending[t.value] = (codec, x, msg, it)
+        return t.value
+
+    def wait(self, ticket, timeout=600.0):
+        """The request's decisions (and iteration counts when asked), and its latency in seconds."""
+        lat = C.c_double()
+        try:
+            _check(_L.fecl_server_wait(self._h, int(ticket), float(timeout), C.byref(lat)))
+        finally:
+            entry = self._pending.pop(int(ticket), None)
+        _, _, msg, it = entry
+        return (msg, it, lat.value) if it is not None else (msg, lat.value)
+
+    def report(self):
+        st = _lib.fecl_server_stats()
+        _check(_L.fecl_server_report(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def reset_stats(self):
+        _check(_L.fecl_server_reset_stats(self._h))
+
+    def replay(self, arrivals, requests):
+        """Native load generator: request i = (codec, llr numpy) is submitted at
+        arrivals[i] seconds after the call starts; returns (decisions, latencies)."""
+        n = len(requests)
+        arr = np.ascontiguousarray(np.asarray(arrivals, np.float64))
+        codecs = (C.c_void_p * n)()
+        llrs = (C.c_void_p * n)()
+        msgs = (C.c_void_p * n)()
+        dts = np.zeros(n, np.int32)
+        nfr = np.zeros(n, np.uint64)
+        keep, outs = [], []
+        for i, (codec, llr) in enumerate(requests):
+            x = np.ascontiguousarray(np.asarray(llr).ravel())
+            nf = codec._frames(x.size, codec.paritySize(), "parity")
+            m = np.zeros(nf * codec.msgSize(), np.uint8)
+            codecs[i] = codec._h.value
+            llrs[i] = x.ctypes.data
+            msgs[i] = m.ctypes.data
+            dts[i] = _dtype_code(x)
+            nfr[i] = nf
+            keep.append(x)
+            outs.append(m)
+        lat = np.zeros(n, np.float64)
+        _check(_L.fecl_server_replay(self._h, n, _ptr(arr), C.cast(codecs, C.c_void_p), C.cast(llrs, C.c_void_p),
+                                     _ptr(dts), _ptr(nfr), C.cast(msgs, C.c_void_p), None, _ptr(lat)))
+        return outs, lat
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h and h.value:
+            _L.fecl_server_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 

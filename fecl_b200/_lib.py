@@ -82,6 +82,17 @@ class fecl_batch_job(C.Structure):
 BATCH_AUTOTUNE = 1
 
 
+class fecl_server_options(C.Structure):
+    _fields_ = [("device_budget_bytes", C.c_uint64), ("max_batch_frames", C.c_uint32), ("slots", C.c_uint32)]
+
+
+class fecl_server_stats(C.Structure):
+    _fields_ = [
+        ("requests", C.c_uint64), ("frames", C.c_uint64), ("info_bits", C.c_uint64), ("batches", C.c_uint64),
+        ("p50_s", C.c_double), ("p99_s", C.c_double), ("max_s", C.c_double), ("wall_s", C.c_double),
+    ]
+
+
 # (name, restype, argtypes) for every symbol include/fecl_b200.h declares.
 SIGNATURES = [
     ("fecl_ldpc_create", C.c_int, [C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.POINTER(fecl_ldpc_options), C.POINTER(C.c_void_p)]),
@@ -110,6 +121,15 @@ SIGNATURES = [
     ("fecl_batch_run", C.c_int, [C.c_void_p, C.c_void_p]),
     ("fecl_batch_describe", C.c_int, [C.c_void_p, C.c_char_p, C.c_uint64]),
     ("fecl_batch_destroy", None, [C.c_void_p]),
+    ("fecl_server_create", C.c_int, [C.POINTER(fecl_server_options), C.POINTER(C.c_void_p)]),
+    ("fecl_server_submit", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_uint64, C.c_void_p, C.c_void_p,
+                                     C.POINTER(C.c_uint64)]),
+    ("fecl_server_wait", C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(C.c_double)]),
+    ("fecl_server_report", C.c_int, [C.c_void_p, C.POINTER(fecl_server_stats)]),
+    ("fecl_server_reset_stats", C.c_int, [C.c_void_p]),
+    ("fecl_server_replay", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fecl_server_destroy", None, [C.c_void_p]),
     ("fecl_strerror", C.c_char_p, [C.c_int]),
     ("fecl_last_error", C.c_char_p, []),
     ("fecl_version", C.c_char_p, []),

@@ -11,8 +11,8 @@
 //      wave sizes, cluster-resident LDPC with several cluster shapes), timed on
 //      the job's own inputs and remembered per (code, batch size) for the process;
 //   3. carves every job's scratch out of one workspace and captures the launches
-//      into a graph: the turbo launch on one stream, the other jobs on a second one
-//      forked from it, so both run at once on different SMs.
+//      into a graph: the turbo launch on one branch, the other jobs spread over four
+//      more branches forked from it, so they all run at once on different SMs.
 // fecl_batch_run replays the graph.  The codecs' options and tables are read when
 // the graph is built: changing a codec's options or destroying it invalidates the
 // batch.
@@ -129,10 +129,12 @@ struct ChoiceScope {
 
 }  // namespace
 
+constexpr int kBranches = 4;  // graph branches the non-turbo-batch jobs are spread over
+
 struct fecl_batch_s {
   int device = 0;
-  cudaStream_t cap = nullptr, cap2 = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaStream_t cap = nullptr, cap2[kBranches] = {};
+  cudaEvent_t fork = nullptr, join[kBranches] = {};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   DeviceBuffer ws;
@@ -142,11 +144,13 @@ struct fecl_batch_s {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (cap) cudaStreamSynchronize(cap);
-    if (cap2) cudaStreamSynchronize(cap2);
+    for (int q = 0; q < kBranches; ++q) {
+      if (cap2[q]) cudaStreamSynchronize(cap2[q]);
+      if (join[q]) cudaEventDestroy(join[q]);
+      if (cap2[q]) cudaStreamDestroy(cap2[q]);
+    }
     if (fork) cudaEventDestroy(fork);
-    if (join) cudaEventDestroy(join);
     if (cap) cudaStreamDestroy(cap);
-    if (cap2) cudaStreamDestroy(cap2);
   }
 };
 
@@ -239,9 +243,11 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
     std::unique_ptr<fecl_batch_s> b(new fecl_batch_s);
     b->device = dev;
     cuda_check(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking), "cudaStreamCreate");
-    cuda_check(cudaStreamCreateWithFlags(&b->cap2, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (int q = 0; q < kBranches; ++q) {
+      cuda_check(cudaStreamCreateWithFlags(&b->cap2[q], cudaStreamNonBlocking), "cudaStreamCreate");
+      cuda_check(cudaEventCreateWithFlags(&b->join[q], cudaEventDisableTiming), "cudaEventCreate");
+    }
     cuda_check(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "cudaEventCreate");
-    cuda_check(cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming), "cudaEventCreate");
 
     // ---- 1. turbo frames for the mixed-K launch, per algorithm
     std::map<int, std::vector<fecl::TurboLteBatchFrame>> tframes;
@@ -334,7 +340,7 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
     cuda_check(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     try {
       cuda_check(cudaEventRecord(b->fork, b->cap), "cudaEventRecord");
-      cuda_check(cudaStreamWaitEvent(b->cap2, b->fork, 0), "cudaStreamWaitEvent");
+      for (int q = 0; q < kBranches; ++q) cuda_check(cudaStreamWaitEvent(b->cap2[q], b->fork, 0), "cudaStreamWaitEvent");
       for (auto& kv : tframes) {
         fecl::TurboLteBatchParams p;
         p.frames = reinterpret_cast<const fecl::TurboLteBatchFrame*>(base + desc_off[kv.first]);
@@ -345,22 +351,26 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
         cuda_check(fecl::launch_turbo_lte_batch(p, b->cap), "turbo batch launch");
         plan << "turbo LTE mixed-K x" << kv.second.size() << " (alg " << kv.first << ", max K " << p.max_K << ")\n";
       }
+      int branch = 0;
       for (auto& s : js) {
         if (s.lte) continue;
+        cudaStream_t st = b->cap2[branch++ % kBranches];
         ChoiceScope scope(s.c, s.choice);
         Launch d;
         d.llr = s.job->llr;
         d.hard = s.job->msg;
         d.iters = s.job->iterations;
         d.scratch = base + s.off;
-        launch_decode(s.c, d, s.sp, s.job->nframes, s.job->llr_dtype, FECL_F32, false, false, b->cap2);
+        launch_decode(s.c, d, s.sp, s.job->nframes, s.job->llr_dtype, FECL_F32, false, false, st);
         plan << (s.c->kind == 0 ? "ldpc " : "turbo ") << s.c->msg() << "/" << s.c->parity() << " x" << s.job->nframes
              << ": " << (s.sp.cluster ? "cluster C=" + std::to_string(s.sp.cluster) + " threads=" + std::to_string(s.sp.threads)
                                       : s.choice.text())
              << "\n";
       }
-      cuda_check(cudaEventRecord(b->join, b->cap2), "cudaEventRecord");
-      cuda_check(cudaStreamWaitEvent(b->cap, b->join, 0), "cudaStreamWaitEvent");
+      for (int q = 0; q < kBranches; ++q) {
+        cuda_check(cudaEventRecord(b->join[q], b->cap2[q]), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(b->cap, b->join[q], 0), "cudaStreamWaitEvent");
+      }
     } catch (...) {
       cudaGraph_t g = nullptr;
       cudaStreamEndCapture(b->cap, &g);

@@ -295,6 +295,47 @@ int fecl_batch_run(fecl_batch_t batch, void* stream);
 int fecl_batch_describe(fecl_batch_t batch, char* text, uint64_t size);
 void fecl_batch_destroy(fecl_batch_t batch);
 
+/* ---- decode server (an extension) ---------------------------------------------
+ *
+ * Continuous batching of decode requests.  A request is n frames of one codec with
+ * host L-values in and host decisions out; any thread may submit.  The server keeps
+ * up to `slots` batches in flight, each on its own stream with device_budget / slots
+ * bytes of device memory; whenever a slot is free it admits the oldest waiting
+ * requests that fit that memory and max_batch_frames, so requests that arrive while
+ * other batches are on the GPU are decoded in the next one, overlapping the batches
+ * still running.  Every LTE turbo frame of a batch goes into one mixed-K launch,
+ * the frames of each other codec into one launch sequence.  A request's decisions do
+ * not depend on the requests it was batched with: they equal fecl_decode's.
+ * The request's buffers must stay valid until fecl_server_wait returns for it; the
+ * codecs must outlive the server and keep their options while it runs. */
+typedef struct fecl_server_s* fecl_server_t;
+typedef struct {
+  uint64_t device_budget_bytes; /* device memory for batches in flight (0: 40 GiB) */
+  uint32_t max_batch_frames;    /* frames admitted into one batch (0: 2048) */
+  uint32_t slots;               /* batches in flight at once (0: 3; at most 16) */
+} fecl_server_options;
+typedef struct {
+  uint64_t requests, frames, info_bits, batches; /* finished since creation or the last reset */
+  double p50_s, p99_s, max_s; /* request latency, submission to decisions in host memory */
+  double wall_s;              /* first submission to last completion */
+} fecl_server_stats;
+int fecl_server_create(const fecl_server_options* options, fecl_server_t* out);
+/* Queues nframes frames of `codec`: llr [nframes][paritySize] of llr_dtype, msg
+ * [nframes][msgSize] bytes, iterations [nframes] or NULL, all host memory. */
+int fecl_server_submit(fecl_server_t server, fecl_codec_t codec, const void* llr, int32_t llr_dtype, uint64_t nframes,
+                       uint8_t* msg, int32_t* iterations, uint64_t* ticket);
+/* Blocks until the request is done (FECL_ETIMEDOUT after timeout_s); its latency in seconds. */
+int fecl_server_wait(fecl_server_t server, uint64_t ticket, double timeout_s, double* latency_s);
+int fecl_server_report(fecl_server_t server, fecl_server_stats* stats);
+int fecl_server_reset_stats(fecl_server_t server);
+/* Load generator: submits request i at arrival_s[i] seconds after the call starts, from
+ * the calling thread, then waits for all of them; latency_s[i] (nullable) receives
+ * each latency.  Arrays are indexed by request. */
+int fecl_server_replay(fecl_server_t server, uint64_t nreq, const double* arrival_s, const fecl_codec_t* codecs,
+                       const void* const* llr, const int32_t* llr_dtype, const uint64_t* nframes, uint8_t* const* msg,
+                       int32_t* const* iterations, double* latency_s);
+void fecl_server_destroy(fecl_server_t server);
+
 const char* fecl_strerror(int status);
 /* Message of the last failing call on this thread. */
 const char* fecl_last_error(void);

@@ -1,0 +1,103 @@
+"""The decode server (fecl_server_*): continuous batching of requests of mixed codes.
+Each request's decisions must equal the codec's own decode of the same L-values --
+the same alone and in the mix -- whatever the batches it landed in, under a memory
+budget that forces many small batches, from several submitting threads, and under
+a Poisson replay."""
+import threading
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _codes():
+    import fecl_b200 as F
+    codes = []
+    tdec = F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(6).scheduling(F.Serial)
+    for K in (40, 512, 1504, 6144):
+        codes.append(F.Turbo.lte(K, tdec))
+    ms = F.Ldpc.DecoderOptions().algorithm(F.Approximate).iterations(50).scalingFactor(0.75).precision(1)
+    for n, r in ((16200, (1, 2)), (16200, (5, 6)), (64800, (3, 4))):
+        codes.append(F.Ldpc(F.Ldpc.EncoderOptions(F.Ldpc.DvbS2.matrix(n, Fraction(*r))), ms))
+    return codes
+
+
+def _requests(codes, count, seed):
+    from fecl_b200 import channel as ch
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(count):
+        c = codes[int(rng.integers(len(codes)))]
+        nf = int(rng.integers(1, 4))
+        K, N = c.msgSize(), c.paritySize()
+        msg = ch.random_bits(nf * K, seed * 1000 + i)
+        llr = ch.awgn_llr(c.encode(msg), float(rng.uniform(0.5, 3.0)), K / N, seed * 1000 + i, np.float16)
+        reqs.append((c, llr))
+    return reqs
+
+
+def test_results_same_alone_and_in_the_mix():
+    import fecl_b200 as F
+    codes = _codes()
+    reqs = _requests(codes, 60, 1)
+    alone = [c.decode(llr) for c, llr in reqs]
+    srv = F.Server(device_budget=4 << 30, max_batch_frames=512, slots=3)
+    got = [None] * len(reqs)
+
+    def submitter(idx):
+        tickets = [(i, srv.submit(reqs[i][0], reqs[i][1])) for i in idx]
+        for i, t in tickets:
+            got[i] = srv.wait(t)
+
+    threads = [threading.Thread(target=submitter, args=(list(range(k, len(reqs), 3)),)) for k in range(3)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for i, (a, g) in enumerate(zip(alone, got)):
+        msg, lat = g
+        assert lat > 0
+        assert np.array_equal(a, msg), i
+    rep = srv.report()
+    assert rep["requests"] == len(reqs) and rep["batches"] >= 1
+    assert rep["p99_s"] >= rep["p50_s"] > 0
+    srv.close()
+
+
+def test_small_budget_forces_many_batches_and_rejects_oversize():
+    import fecl_b200 as F
+    codes = _codes()
+    reqs = [r for r in _requests(codes, 40, 2) if r[0].paritySize() <= 16200 * 1 or r[0].msgSize() <= 6144]
+    alone = [c.decode(llr) for c, llr in reqs]
+    # about 96 MiB per slot: a few short LDPC frames or turbo frames per batch
+    srv = F.Server(device_budget=3 * (96 << 20), max_batch_frames=64, slots=3)
+    tickets = [srv.submit(c, llr) for c, llr in reqs]
+    for a, t in zip(alone, tickets):
+        msg, _ = srv.wait(t)
+        assert np.array_equal(a, msg)
+    assert srv.report()["batches"] > 3
+    # a request larger than a slot's memory cannot be admitted
+    big = codes[-1]
+    from fecl_b200 import channel as ch
+    llr = ch.awgn_llr(big.encode(ch.random_bits(200 * big.msgSize(), 3)), 3.0, 0.75, 3, np.float32)
+    t = srv.submit(big, llr)
+    with pytest.raises(F.FeclError):
+        srv.wait(t)
+    srv.close()
+
+
+def test_poisson_replay():
+    import fecl_b200 as F
+    codes = _codes()
+    reqs = _requests(codes, 200, 4)
+    alone = [c.decode(llr) for c, llr in reqs]
+    rng = np.random.default_rng(5)
+    arrivals = np.cumsum(rng.exponential(1.0 / 5000.0, size=len(reqs)))
+    srv = F.Server(slots=3)
+    outs, lat = srv.replay(arrivals, reqs)
+    for a, m in zip(alone, outs):
+        assert np.array_equal(a, m)
+    assert np.all(lat > 0)
+    srv.close()
