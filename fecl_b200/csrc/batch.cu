@@ -63,7 +63,7 @@ struct Choice {
       case FECL_KERNEL_LANES: o << "lanes wave=" << (wave ? std::to_string(wave) : std::string("auto")); break;
       case FECL_KERNEL_CLUSTER: o << "cluster C=" << cluster << " threads=" << threads; break;
       case FECL_KERNEL_GENERIC: o << "generic"; break;
-      default: o << "auto";
+      default: o << "auto" << (wave ? " wave=" + std::to_string(wave) : std::string());
     }
     return o.str();
   }
@@ -92,6 +92,12 @@ std::string signature(fecl_codec_s* c, uint64_t n, int32_t dtype) {
 std::vector<Choice> ldpc_candidates(fecl_codec_s* c, uint64_t n) {
   std::vector<Choice> v;
   v.push_back(Choice{});
+  if (c->ldpc_h2_ok()) {  // the packed FP16 kernel: only its wave size is free
+    const int groups = int((n + 63) / 64);
+    for (int w : {1, 2, 4, 8, groups})
+      if (w <= groups) v.push_back(Choice{FECL_KERNEL_AUTO, 0, 0, w});
+    return v;
+  }
   if (c->ldpc_lanes_ok()) {
     const int groups = int((n + 31) / 32);
     for (int w : {1, 2, 4, 8, groups})

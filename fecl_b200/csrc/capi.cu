@@ -155,7 +155,9 @@ ScratchPlan plan_scratch(fecl_codec_s* c, uint64_t n, bool lte_fast) {
   if (c->kind == 0 && c->kernel_sel == FECL_KERNEL_CLUSTER)
     fail(FECL_EUNSUPPORTED, "the code's messages do not fit a thread-block cluster");
   if (c->kind == 0 && c->ldpc_lanes_ok()) {
-    sp.o1 = cv.take(fecl::ldpc_lanes_scratch_bytes(int64_t(P), int64_t(X), int64_t(n), c->ldpc->decoder().precision));
+    size_t b = fecl::ldpc_lanes_scratch_bytes(int64_t(P), int64_t(X), int64_t(n), c->ldpc->decoder().precision);
+    if (c->ldpc_h2_ok()) b = std::max(b, fecl::ldpc_lanes_h2_scratch_bytes(int64_t(P), int64_t(X), int64_t(n)));
+    sp.o1 = cv.take(b);
   } else if (lte_fast) {
     sp.o1 = cv.take(fecl::turbo_lte_scratch_bytes(int(c->msg()), int64_t(n)));
   } else if (c->kind == 0) {
@@ -254,7 +256,8 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
     r.parity_out = d.parity_out;
     r.state_out = d.state_out;
     r.out_dtype = out_dtype;
-    e = fecl::launch_ldpc_lanes(r, at(sp.o1), s);
+    if (c->ldpc_h2_ok() && !d.state) e = fecl::launch_ldpc_lanes_h2(r, at(sp.o1), s);
+    else e = fecl::launch_ldpc_lanes(r, at(sp.o1), s);
   } else if (c->kind == 0) {
     if (c->ldpc->decoder().precision != 0)
       fail(FECL_EUNSUPPORTED, "FP16 / int8 messages need check degrees <= 32 and a scaling constant across iterations");

@@ -331,6 +331,13 @@ struct fecl_codec_s {
       if (row != d.scaling[0]) return false;
     return true;
   }
+  // FP16 normalised min-sum goes to the packed two-frames-per-lane kernel unless a
+  // kernel is forced (FECL_KERNEL_LANES keeps FP32 check-node arithmetic).
+  bool ldpc_h2_ok() const {
+    if (kind != 0 || kernel_sel != FECL_KERNEL_AUTO || !ldpc_lanes_ok()) return false;
+    const auto& d = ldpc->decoder();
+    return d.precision == 1 && d.algorithm == 2;
+  }
   // The windowed kernel covers the LTE RSC pair with serial scheduling and FP32 messages
   // for any K whose two exchange arrays fit in shared memory.
   bool lte_fast_ok() const {

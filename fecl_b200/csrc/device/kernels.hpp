@@ -86,6 +86,11 @@ struct LdpcLanesParams {
 size_t ldpc_lanes_scratch_bytes(int64_t N, int64_t E, int64_t nframes, int msg_type);
 cudaError_t launch_ldpc_lanes(LdpcLanesParams p, void* scratch, cudaStream_t stream);
 
+// Normalised min-sum with FP16 messages and packed half2 check-node arithmetic, two
+// frames per lane (ldpc_lanes_h2.cu).  Takes no soft state input.
+size_t ldpc_lanes_h2_scratch_bytes(int64_t N, int64_t E, int64_t nframes);
+cudaError_t launch_ldpc_lanes_h2(LdpcLanesParams p, void* scratch, cudaStream_t stream);
+
 // Flooding BP with each frame's messages resident in the shared memory of a
 // thread-block cluster of `cluster` CTAs (ldpc_cluster.cu).  The address tables are
 // built per (code, cluster) by build_ldpc_cluster_plan (host/ldpc_plan.hpp).

@@ -1,0 +1,352 @@
+// LDPC normalised min-sum with FP16 messages, packed: two frames per lane, 64 frames
+// per warp.
+//
+// The decoder of ldpc_lanes.cu (BpDecoderImpl, src/detail/BpDecoder/BpDecoderImpl.cpp:37-179,
+// min-sum boxplus src/detail/LlrMetrics.h:184-191) in FP16 message passing with FP32
+// bit-node sums.  Lane l of group g holds frames 64 g + l (the .x halves) and
+// 64 g + 32 + l (the .y halves):
+//     chan[g][n][32], app[g][n][32]  float2 (FP32 bit-node values of the two frames)
+//     c2v[g][e][32]                  half2  (the two frames' check-to-bit messages)
+// so every warp access is 256 (float2) or 128 (half2) contiguous bytes, and one
+// packed instruction serves two frames:
+//   check  v = app - c2v in FP32 (packed f32x2), rounded to FP16; |v|, the two
+//          smallest magnitudes (m2 = min(m2, max(m1, |v|)), m1 = min(m1, |v|)) and
+//          the sign parity in half2; edge j gets m2 where |v_j| == m1, else m1, its
+//          sign, times the scaling, as one half2 store;
+//   bit    app = chan + sum of c2v in edge order, FP32 (packed f32x2 adds).
+// Ties are exact: two equal minima give m2 == m1.  The syndrome stop, the retirement
+// of frames and the waves are those of ldpc_lanes.cu, with a pair of lane masks per
+// group (.x frames, .y frames).
+#include <cuda_fp16.h>
+#include <math.h>
+
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace fecl {
+namespace {
+
+constexpr int kLanes = 32;
+constexpr int kWarps = 8;
+constexpr uint32_t kSigns = 0x80008000u;
+
+__device__ __forceinline__ uint32_t bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
+__device__ __forceinline__ __half2 from_bits(uint32_t u) { return *reinterpret_cast<__half2*>(&u); }
+
+// active[it & 1][g][2] and fail[it & 1][g][2]: .x and .y frame masks.
+__device__ __forceinline__ uint32_t* active_of(const LdpcLanesParams& p, int it) { return p.active + (it & 1) * 2 * p.groups; }
+__device__ __forceinline__ uint32_t* fail_of(const LdpcLanesParams& p, int it) { return p.fail + (it & 1) * 2 * p.groups; }
+
+template <int DMAX>
+struct Row {
+  uint32_t e0;
+  int d;
+  __half2 v[DMAX];
+  unsigned px, py;  // parity of the hard decisions of the previous APP
+};
+
+template <int DMAX>
+__device__ __forceinline__ void load_row(const LdpcLanesParams& p, int g, int r, int lane, Row<DMAX>& w) {
+  const __half2* c2v = static_cast<const __half2*>(p.c2v);
+  const float2* app = reinterpret_cast<const float2*>(p.app);
+  w.e0 = __ldg(p.row_ptr + r);
+  w.d = int(__ldg(p.row_ptr + r + 1) - w.e0);
+  const __half2* cg = c2v + (int64_t(g) * p.E + w.e0) * kLanes + lane;
+  const float2* ag = app + int64_t(g) * p.N * kLanes + lane;
+  w.px = w.py = 0;
+#pragma unroll
+  for (int j = 0; j < DMAX; ++j) {
+    if (j < w.d) {
+      const uint32_t col = __ldg(p.col_idx + w.e0 + j);
+      const float2 a = ag[int64_t(col) * kLanes];
+      const float2 c = __half22float2(cg[j * kLanes]);
+      w.px ^= unsigned(a.x >= 0.0f);
+      w.py ^= unsigned(a.y >= 0.0f);
+      // a - c in FP32, rounded to FP16 and kept finite (saturated at +-65504)
+      const __half2 vh = __float22half2_rn(__ffma2_rn(c, make_float2(-1.0f, -1.0f), a));
+      w.v[j] = __hmax2(__hmin2(vh, __float2half2_rn(65504.0f)), __float2half2_rn(-65504.0f));
+    }
+  }
+}
+
+template <int DMAX>
+__device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, int lane, const Row<DMAX>& w, __half2 sf2,
+                                          bool mine_x, bool mine_y) {
+  __half2* c2v = static_cast<__half2*>(p.c2v);
+  const __half2 inf2 = __floats2half2_rn(INFINITY, INFINITY);
+  __half2 m1 = inf2, m2 = inf2;
+  uint32_t sg = 0;
+#pragma unroll
+  for (int j = 0; j < DMAX; ++j) {
+    if (j < w.d) {
+      const __half2 a = __habs2(w.v[j]);
+      m2 = __hmin2(m2, __hmax2(m1, a));
+      m1 = __hmin2(m1, a);
+      sg ^= bits(w.v[j]);
+    }
+  }
+  // d - 1 inputs per output: the sign is (d - 2) xor the parity of the others' signs.
+  sg = (sg & kSigns) ^ (((w.d - 2) & 1) ? kSigns : 0u);
+  const uint32_t b1 = bits(m1), b2 = bits(m2);
+  // lanes whose frames are not decoding keep their messages
+  const uint32_t keep = (mine_x ? 0u : 0x0000ffffu) | (mine_y ? 0u : 0xffff0000u);
+  __half2* cg = c2v + (int64_t(g) * p.E + w.e0) * kLanes + lane;
+#pragma unroll
+  for (int j = 0; j < DMAX; ++j) {
+    if (j < w.d) {
+      const uint32_t eq = __heq2_mask(__habs2(w.v[j]), m1);
+      const uint32_t mag = (b2 & eq) | (b1 & ~eq);
+      const uint32_t sign = (sg ^ bits(w.v[j])) & kSigns;
+      const __half2 out = __hmul2(from_bits(mag | sign), sf2);
+      if (keep == 0u) {
+        cg[j * kLanes] = out;
+      } else if (keep != 0xffffffffu) {
+        const uint32_t old = bits(cg[j * kLanes]);
+        cg[j * kLanes] = from_bits((bits(out) & ~keep) | (old & keep));
+      }
+    }
+  }
+}
+
+template <int DMAX>
+__global__ void __launch_bounds__(kWarps * 32) h2_check(LdpcLanesParams p, int it, int g0) {
+  constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  const int lane = threadIdx.x & 31;
+  const int warps = int(gridDim.x) * kWarps;
+  const bool check_syndrome = it > 0 && !p.fixed_iterations;
+  const int g = g0 + int(blockIdx.y);
+  const uint32_t ax = active_of(p, it)[2 * g], ay = active_of(p, it)[2 * g + 1];
+  if ((ax | ay) == 0) return;
+  const bool mx = (ax >> lane) & 1, my = (ay >> lane) & 1;
+  uint32_t bx = 0, by = 0;
+  const int w0 = int(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  for (int r = w0 * kRows; r < p.M; r += warps * kRows) {
+    Row<DMAX> w[kRows];
+#pragma unroll
+    for (int q = 0; q < kRows; ++q) {
+      w[q].d = 0;
+      if (r + q < p.M) load_row<DMAX>(p, g, r + q, lane, w[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < kRows; ++q) {
+      if (w[q].d > 0) {
+        if (check_syndrome) {
+          bx |= __ballot_sync(0xffffffffu, w[q].px != 0);
+          by |= __ballot_sync(0xffffffffu, w[q].py != 0);
+        }
+        // the scaling of rows of this degree (constant across iterations on this path)
+        const float s = p.sf[size_t(it % p.n_sf) * p.sf_stride + (w[q].d >= 2 ? w[q].d - 2 : 0)];
+        store_row<DMAX>(p, g, lane, w[q], __float2half2_rn(s), mx, my);
+      }
+    }
+  }
+  bx &= ax;
+  by &= ay;
+  if (lane == 0) {
+    if (bx) atomicOr(fail_of(p, it) + 2 * g, bx);
+    if (by) atomicOr(fail_of(p, it) + 2 * g + 1, by);
+  }
+}
+
+// Bit pass; with it < 0 the initial APP for every lane.  Block (0, y) retires frames
+// and writes the group's masks for iteration it + 1.
+__global__ void __launch_bounds__(kWarps * 32) h2_bit(LdpcLanesParams p, int it, int g0) {
+  const __half2* c2v = static_cast<const __half2*>(p.c2v);
+  const float2* chan = reinterpret_cast<const float2*>(p.chan);
+  float2* app = reinterpret_cast<float2*>(p.app);
+  const int lane = threadIdx.x & 31;
+  const int warps = int(gridDim.x) * kWarps;
+  const int g = g0 + int(blockIdx.y);
+  const uint32_t ax = it < 0 ? 0xffffffffu : active_of(p, it)[2 * g];
+  const uint32_t ay = it < 0 ? 0xffffffffu : active_of(p, it)[2 * g + 1];
+  if (it >= 0 && blockIdx.x == 0 && threadIdx.x < 2) {
+    const int h = threadIdx.x;  // 0: .x frames, 1: .y frames
+    const uint32_t a = h ? ay : ax;
+    uint32_t done = 0;
+    if (it == p.iterations - 1) done = a;
+    else if (it > 0 && !p.fixed_iterations) done = a & ~fail_of(p, it)[2 * g + h];
+    for (uint32_t m = done; m; m &= m - 1) p.iters_ws[int64_t(g) * 64 + h * 32 + (__ffs(m) - 1)] = it + 1;
+    active_of(p, it + 1)[2 * g + h] = a & ~done;
+    fail_of(p, it + 1)[2 * g + h] = 0;
+  }
+  const bool mx = (ax >> lane) & 1, my = (ay >> lane) & 1;
+  if (!mx && !my) return;
+  const __half2* cg = c2v + int64_t(g) * p.E * kLanes + lane;
+  for (int b = int(blockIdx.x) * kWarps + (threadIdx.x >> 5); b < p.N; b += warps) {
+    const int64_t base = (int64_t(g) * p.N + b) * kLanes + lane;
+    const uint32_t k0 = __ldg(p.col_ptr + b), k1 = __ldg(p.col_ptr + b + 1);
+    float2 acc = chan[base];
+    uint32_t k = k0;
+    for (; k + 4 <= k1; k += 4) {
+      const uint32_t e_0 = __ldg(p.col_edges + k), e_1 = __ldg(p.col_edges + k + 1);
+      const uint32_t e_2 = __ldg(p.col_edges + k + 2), e_3 = __ldg(p.col_edges + k + 3);
+      const float2 x0 = __half22float2(cg[int64_t(e_0) * kLanes]), x1 = __half22float2(cg[int64_t(e_1) * kLanes]);
+      const float2 x2 = __half22float2(cg[int64_t(e_2) * kLanes]), x3 = __half22float2(cg[int64_t(e_3) * kLanes]);
+      acc = __fadd2_rn(acc, x0);
+      acc = __fadd2_rn(acc, x1);
+      acc = __fadd2_rn(acc, x2);
+      acc = __fadd2_rn(acc, x3);
+    }
+    for (; k < k1; ++k) acc = __fadd2_rn(acc, __half22float2(cg[int64_t(__ldg(p.col_edges + k)) * kLanes]));
+    if (mx && my) {
+      app[base] = acc;
+    } else {  // one of the lane's frames has retired: its APP stays
+      float2 out = app[base];
+      if (mx) out.x = acc.x;
+      if (my) out.y = acc.y;
+      app[base] = out;
+    }
+  }
+}
+
+// Frame f of group g sits in lane f % 32, half (f / 32) % 2.
+__device__ __forceinline__ int64_t frame_of(int g, int lane, int h) { return int64_t(g) * 64 + h * 32 + lane; }
+
+__global__ void h2_stage(LdpcLanesParams p) {
+  float2* chan = reinterpret_cast<float2*>(p.chan);
+  __half2* c2v = static_cast<__half2*>(p.c2v);
+  const int g = int(blockIdx.y);
+  const int stride = int(gridDim.x) * blockDim.x;
+  const int t0 = int(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (int i = t0; i < p.N * kLanes; i += stride) {
+    const int lane = i % kLanes, b = i / kLanes;
+    float v[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int64_t f = frame_of(g, lane, h);
+      v[h] = 0.0f;
+      if (f < p.nframes) {
+        v[h] = load_llr(p.llr, p.llr_dtype, f * p.N + b);
+        if (p.syst_in && b < p.msg) v[h] += load_llr(p.syst_in, p.llr_dtype, f * p.msg + b);
+      }
+    }
+    chan[int64_t(g) * p.N * kLanes + i] = make_float2(v[0], v[1]);
+  }
+  for (int64_t i = t0; i < p.E * kLanes; i += stride) c2v[int64_t(g) * p.E * kLanes + i] = __floats2half2_rn(0.0f, 0.0f);
+  if (t0 == 0) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int64_t left = p.nframes - int64_t(g) * 64 - h * 32;
+      p.active[2 * g + h] = left >= 32 ? 0xffffffffu : (left > 0 ? ((1u << left) - 1u) : 0u);
+      p.active[2 * p.groups + 2 * g + h] = 0;
+      p.fail[2 * g + h] = 0;
+      p.fail[2 * p.groups + 2 * g + h] = 0;
+    }
+  }
+}
+
+__global__ void h2_finish(LdpcLanesParams p) {
+  const float2* chan = reinterpret_cast<const float2*>(p.chan);
+  const float2* app = reinterpret_cast<const float2*>(p.app);
+  const __half2* c2v = static_cast<const __half2*>(p.c2v);
+  const int g = int(blockIdx.y);
+  const int stride = int(gridDim.x) * blockDim.x;
+  const int t0 = int(blockIdx.x) * blockDim.x + threadIdx.x;
+  const bool soft = p.msg_out || p.syst_out || p.parity_out;
+  const __half2* cg = c2v + int64_t(g) * p.E * kLanes;
+  for (int i = t0; i < p.N * kLanes; i += stride) {
+    const int lane = i % kLanes, b = i / kLanes;
+    const int64_t at = int64_t(g) * p.N * kLanes + i;
+    const float2 a = app[at];
+    float2 ext = make_float2(0.0f, 0.0f);
+    if (soft)
+      for (uint32_t k = __ldg(p.col_ptr + b); k < __ldg(p.col_ptr + b + 1); ++k)
+        ext = __fadd2_rn(ext, __half22float2(cg[int64_t(__ldg(p.col_edges + k)) * kLanes + lane]));
+    const float2 ch = chan[at];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int64_t f = frame_of(g, lane, h);
+      if (f >= p.nframes) continue;
+      const float av = h ? a.y : a.x, ev = h ? ext.y : ext.x, cv = h ? ch.y : ch.x;
+      if (p.hard && b < p.msg) p.hard[f * p.msg + b] = uint8_t(av >= 0.0f);
+      if (soft) {
+        if (p.parity_out) store_llr(p.parity_out, p.out_dtype, f * p.N + b, ev);
+        if (b < p.msg) {
+          if (p.syst_out) store_llr(p.syst_out, p.out_dtype, f * p.msg + b, ev);
+          if (p.msg_out) store_llr(p.msg_out, p.out_dtype, f * p.msg + b, cv + ev);
+        }
+      }
+    }
+  }
+  if (p.state_out) {
+    for (int64_t i = t0; i < p.E * kLanes; i += stride) {
+      const int lane = int(i % kLanes);
+      const int64_t e = i / kLanes;
+      const float2 c = __half22float2(cg[i]);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int64_t f = frame_of(g, lane, h);
+        if (f < p.nframes) store_llr(p.state_out, p.out_dtype, f * p.E + e, h ? c.y : c.x);
+      }
+    }
+  }
+  if (p.iters && t0 < 64) {
+    const int64_t f = int64_t(g) * 64 + t0;
+    if (f < p.nframes) p.iters[f] = p.iters_ws[f];
+  }
+}
+
+dim3 grid_for(int64_t per_group, int groups) {
+  const int64_t need = (per_group + kWarps - 1) / kWarps;
+  const int64_t share = (148 * 16 + groups - 1) / groups;
+  const int64_t x = need < share ? need : share;
+  return dim3(unsigned(x > 0 ? x : 1), unsigned(groups));
+}
+
+constexpr int64_t kWaveBytes = 64ll << 20;
+
+template <int DMAX>
+cudaError_t run(const LdpcLanesParams& p, cudaStream_t s) {
+  if (p.groups > 65535) return cudaErrorInvalidValue;
+  const int64_t gb = int64_t(kLanes) * (2 * 8 * int64_t(p.N) + 4 * p.E);
+  int wave = int(p.wave_groups > 0 ? p.wave_groups : (kWaveBytes + gb - 1) / gb);
+  if (wave < 1) wave = 1;
+  if (wave > p.groups) wave = p.groups;
+  const dim3 gs((148 * 8 + p.groups - 1) / p.groups, p.groups);
+  h2_stage<<<gs, 256, 0, s>>>(p);
+  for (int w0 = 0; w0 < p.groups; w0 += wave) {
+    const int nw = p.groups - w0 < wave ? p.groups - w0 : wave;
+    const dim3 gbit = grid_for(p.N, nw);
+    const dim3 gchk = grid_for((p.M + (DMAX <= 8 ? 1 : 0)) / (DMAX <= 8 ? 2 : 1), nw);
+    h2_bit<<<gbit, kWarps * 32, 0, s>>>(p, -1, w0);
+    for (int it = 0; it < p.iterations; ++it) {
+      h2_check<DMAX><<<gchk, kWarps * 32, 0, s>>>(p, it, w0);
+      h2_bit<<<gbit, kWarps * 32, 0, s>>>(p, it, w0);
+    }
+  }
+  h2_finish<<<gs, 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t ldpc_lanes_h2_scratch_bytes(int64_t N, int64_t E, int64_t nframes) {
+  const int64_t groups = (nframes + 63) / 64;
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  return al(size_t(groups) * N * kLanes * 8) * 2 + al(size_t(groups) * E * kLanes * 4) + al(size_t(groups) * 32) +
+         al(size_t(groups) * 64 * 4);
+}
+
+cudaError_t launch_ldpc_lanes_h2(LdpcLanesParams p, void* scratch, cudaStream_t s) {
+  if (p.nframes <= 0) return cudaSuccess;
+  if (p.state_in || p.algorithm != 2) return cudaErrorInvalidValue;
+  p.groups = int32_t((p.nframes + 63) / 64);
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  char* q = static_cast<char*>(scratch);
+  p.chan = reinterpret_cast<float*>(q);
+  q += al(size_t(p.groups) * p.N * kLanes * 8);
+  p.app = reinterpret_cast<float*>(q);
+  q += al(size_t(p.groups) * p.N * kLanes * 8);
+  p.c2v = q;
+  q += al(size_t(p.groups) * p.E * kLanes * 4);
+  p.active = reinterpret_cast<uint32_t*>(q);  // [2][groups][2]
+  p.fail = p.active + 4 * p.groups;          // [2][groups][2]
+  q += al(size_t(p.groups) * 32);
+  p.iters_ws = reinterpret_cast<int32_t*>(q);
+  if (p.d_max <= 8) return run<8>(p, s);
+  if (p.d_max <= 16) return run<16>(p, s);
+  if (p.d_max <= 32) return run<32>(p, s);
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace fecl

@@ -35,8 +35,8 @@ __device__ __forceinline__ float box_linear(const LinearLut& lut, float a, float
 // tanh rounds to +-1.  Inputs are clamped to 80 so phi stays normal.
 __device__ __forceinline__ float phi(float x) { return log1pf(2.0f / expm1f(x)); }
 
-// Storage of check-to-bit messages: FP32 (reference parity), FP16, or saturated int8
-// in Q5.2 (step 1/4, range +-31.75).  Arithmetic is FP32 in every case.
+// Storage of check-to-bit messages: FP32 (reference parity), saturated FP16 (+-65504),
+// or saturated int8 in Q5.2 (step 1/4, range +-31.75).  Arithmetic is FP32 in every case.
 template <int MSG>
 struct Msg;
 template <>
@@ -50,7 +50,8 @@ template <>
 struct Msg<1> {
   using T = __half;
   __device__ static float load(const T* p) { return __half2float(*p); }
-  __device__ static void store(T* p, float v) { *p = __float2half_rn(v); }
+  // saturated at the largest finite FP16 value, so that no message becomes infinite
+  __device__ static void store(T* p, float v) { *p = __float2half_rn(fminf(fmaxf(v, -65504.0f), 65504.0f)); }
   __device__ static float from_bits(uint32_t b) { return __half2float(__ushort_as_half((unsigned short)b)); }
 };
 template <>
