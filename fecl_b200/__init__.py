@@ -256,7 +256,19 @@ class Codec:
         return blocks
 
     def encode(self, msg):
-        """Codec::encode -- src/Codec.h:171-198."""
+        """Codec::encode -- src/Codec.h:171-198.  A torch CUDA tensor of message bits is
+        encoded on the GPU (asynchronous on the current stream) and returns a CUDA tensor."""
+        if _is_device(msg):
+            import torch
+            m = msg.contiguous().view(-1)
+            if m.dtype != torch.uint8:
+                raise ValueError("message bits must be uint8")
+            n = self._frames(m.numel(), self.msgSize(), "message")
+            parity = torch.empty(n * self.paritySize(), dtype=torch.uint8, device=m.device)
+            stream = torch.cuda.current_stream(m.device).cuda_stream
+            _check(_L.fecl_encode(self._h, C.c_void_p(m.data_ptr()), n, C.c_void_p(parity.data_ptr()),
+                                  _lib.DEVICE_MEMORY, C.c_void_p(stream)))
+            return parity
         m = np.ascontiguousarray(np.asarray(msg, dtype=np.uint8).ravel())
         n = self._frames(m.size, self.msgSize(), "message")
         parity = np.zeros(n * self.paritySize(), dtype=np.uint8)

@@ -108,6 +108,8 @@ SIGNATURES = [
     ("fecl_codec_sizes", C.c_int, [C.c_void_p, C.POINTER(fecl_sizes)]),
     ("fecl_encode", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int32, C.c_void_p]),
     ("fecl_check", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_int32)]),
+    ("fecl_awgn_llr", C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.c_double, C.c_uint64, C.c_int32, C.c_void_p,
+                                C.c_void_p]),
     ("fecl_decode", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     ("fecl_so_decode", C.c_int, [C.c_void_p, C.POINTER(fecl_so_io), C.c_uint64, C.c_int32, C.c_void_p]),
     ("fecl_destroy", None, [C.c_void_p]),

@@ -36,3 +36,21 @@ def awgn_llr_per_frame(bits, frame_size, ebn0_db, rate, seed, dtype=np.float64):
     sigma2 = 1.0 / (2.0 * esn0)
     y = (2.0 * bits.astype(np.float64) - 1.0) + _rng(seed, 2).normal(0.0, 1.0, size=bits.shape) * np.sqrt(sigma2)
     return (2.0 * y / sigma2).astype(dtype).ravel()
+
+
+def awgn_llr_device(bits, ebn0_db, rate, seed, dtype=None):
+    """BPSK/AWGN L-values computed on the GPU (fecl_awgn_llr): bits is a torch CUDA
+    uint8 tensor; returns a CUDA tensor of `dtype` (float32 by default).  Same model
+    as awgn_llr, different generator (Philox-4x32-10 on the device)."""
+    import ctypes as C
+    import torch
+    from . import _lib
+    dtype = dtype or torch.float32
+    code = {torch.float64: _lib.F64, torch.float32: _lib.F32, torch.float16: _lib.F16}[dtype]
+    b = bits.contiguous().view(-1)
+    out = torch.empty(b.numel(), dtype=dtype, device=b.device)
+    stream = torch.cuda.current_stream(b.device).cuda_stream
+    _lib.check(_lib.lib.fecl_awgn_llr(C.c_void_p(b.data_ptr()), b.numel(), float(ebn0_db), float(rate), int(seed) & (2**64 - 1),
+                                      code, C.c_void_p(out.data_ptr()), C.c_void_p(stream)))
+    return out
+

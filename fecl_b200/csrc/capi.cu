@@ -7,6 +7,7 @@
 // for before it reuses the workspace.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -619,29 +620,37 @@ int fecl_encode(fecl_codec_t codec, const uint8_t* msg, uint64_t nframes, uint8_
     auto c = checked(codec);
     if (!msg || !parity) fail(FECL_EINVAL, "null buffer");
     const uint64_t M = c->msg(), P = c->parity();
-    std::vector<uint8_t> hm, hp;
-    const uint8_t* m = msg;
-    uint8_t* p = parity;
     if (flags == FECL_DEVICE_MEMORY) {
+      // the device encoders (device/encode.cu), asynchronous on the caller's stream
+      std::lock_guard<std::mutex> lk(c->mu);
+      c->ensure_device();
       DeviceGuard dg(c->device);
-      hm.resize(nframes * M);
-      hp.resize(nframes * P);
-      cuda_check(cudaMemcpyAsync(hm.data(), msg, hm.size(), cudaMemcpyDeviceToHost, (cudaStream_t)stream), "copy");
-      cuda_check(cudaStreamSynchronize((cudaStream_t)stream), "copy");
-      m = hm.data();
-      p = hp.data();
-    } else if (flags != FECL_HOST_MEMORY) {
-      fail(FECL_EINVAL, "Invalid memory flag");
+      cudaStream_t s = static_cast<cudaStream_t>(stream);
+      if (c->kind == 0) cuda_check(fecl::launch_ldpc_encode(c->ltab, msg, parity, int64_t(nframes), s), "encode");
+      else cuda_check(fecl::launch_turbo_encode(c->tdev, msg, parity, int64_t(nframes), s), "encode");
+      return;
     }
+    if (flags != FECL_HOST_MEMORY) fail(FECL_EINVAL, "Invalid memory flag");
     for (uint64_t f = 0; f < nframes; ++f) {
-      if (c->kind == 0) c->ldpc->encode(m + f * M, p + f * P);
-      else c->turbo->encode(m + f * M, p + f * P);
+      if (c->kind == 0) c->ldpc->encode(msg + f * M, parity + f * P);
+      else c->turbo->encode(msg + f * M, parity + f * P);
     }
-    if (flags == FECL_DEVICE_MEMORY) {
-      DeviceGuard dg(c->device);
-      cuda_check(cudaMemcpyAsync(parity, hp.data(), hp.size(), cudaMemcpyHostToDevice, (cudaStream_t)stream), "copy");
-      cuda_check(cudaStreamSynchronize((cudaStream_t)stream), "copy");
+  });
+}
+
+int fecl_awgn_llr(const uint8_t* bits, uint64_t n, double ebn0_db, double rate, uint64_t seed, int32_t out_dtype, void* out,
+                  void* stream) {
+  return guarded([&] {
+    if (!bits || !out) fail(FECL_EINVAL, "null buffer");
+    if (!(rate > 0.0)) fail(FECL_EINVAL, "rate must be positive");
+    dsize(out_dtype);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      fail(FECL_ENODEV, "no CUDA device is visible");
     }
+    const double esn0 = std::pow(10.0, ebn0_db / 10.0) * rate;
+    cuda_check(fecl::launch_awgn(bits, int64_t(n), esn0, seed, out_dtype, out, static_cast<cudaStream_t>(stream)), "awgn");
   });
 }
 

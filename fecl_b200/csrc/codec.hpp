@@ -119,6 +119,8 @@ struct fecl_codec_s {
   DeviceBuffer row_ptr, col_idx, col_ptr, col_edges, sf;
   std::vector<std::unique_ptr<DeviceBuffer>> tables;
   fecl::LdpcDeviceCode ldev;
+  DeviceBuffer enc[8];  // LDPC generator pieces (DC, A, B, T as CSR) for the device encoder
+  fecl::LdpcEncodeTables ltab;
   fecl::TurboDeviceCode tdev;
   // workspace
   DeviceBuffer ws;
@@ -175,6 +177,26 @@ struct fecl_codec_s {
     ldev.col_idx = col_idx.as<uint32_t>();
     ldev.col_ptr = col_ptr.as<uint32_t>();
     ldev.col_edges = col_edges.as<uint32_t>();
+    const fecl::Csr* parts[4] = {&ldpc->gen_dc(), &ldpc->gen_a(), &ldpc->gen_b(), &ldpc->gen_t()};
+    for (int i = 0; i < 4; ++i) {
+      enc[2 * i].upload(parts[i]->row_ptr);
+      enc[2 * i + 1].upload(parts[i]->col_idx);
+    }
+    ltab.K = int32_t(ldpc->msg_size());
+    ltab.N = int32_t(H.cols);
+    ltab.gap = int32_t(ldpc->gen_dc().rows);
+    ltab.dc_rows = int32_t(ldpc->gen_dc().rows);
+    ltab.a_rows = int32_t(ldpc->gen_a().rows);
+    ltab.b_rows = int32_t(ldpc->gen_b().rows);
+    ltab.t_rows = int32_t(ldpc->gen_t().rows);
+    ltab.dc_ptr = enc[0].as<uint32_t>();
+    ltab.dc_idx = enc[1].as<uint32_t>();
+    ltab.a_ptr = enc[2].as<uint32_t>();
+    ltab.a_idx = enc[3].as<uint32_t>();
+    ltab.b_ptr = enc[4].as<uint32_t>();
+    ltab.b_idx = enc[5].as<uint32_t>();
+    ltab.t_ptr = enc[6].as<uint32_t>();
+    ltab.t_idx = enc[7].as<uint32_t>();
     upload_ldpc_options();
   }
 

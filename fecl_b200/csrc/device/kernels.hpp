@@ -229,6 +229,24 @@ size_t turbo_lte_frame_floats(int K);
 int turbo_lte_batch_max_ctas(int max_K, int algorithm);
 cudaError_t launch_turbo_lte_batch(const TurboLteBatchParams& p, cudaStream_t s);
 
+// ---- encoders and channel (encode.cu) ---------------------------------------
+
+// The generator pieces of LdpcCode::encode on the device (CSR each).
+struct LdpcEncodeTables {
+  int32_t K = 0, N = 0, gap = 0;
+  int32_t dc_rows = 0, a_rows = 0, b_rows = 0, t_rows = 0;
+  const uint32_t *dc_ptr = nullptr, *dc_idx = nullptr;
+  const uint32_t *a_ptr = nullptr, *a_idx = nullptr;
+  const uint32_t *b_ptr = nullptr, *b_idx = nullptr;
+  const uint32_t *t_ptr = nullptr, *t_idx = nullptr;
+};
+cudaError_t launch_ldpc_encode(const LdpcEncodeTables& t, const uint8_t* msg, uint8_t* parity, int64_t nframes,
+                               cudaStream_t s);
+cudaError_t launch_turbo_encode(const TurboDeviceCode& code, const uint8_t* msg, uint8_t* parity, int64_t nframes,
+                                cudaStream_t s);
+// L = 2 y / sigma^2 with y = (2 b - 1) + N(0, sigma^2), sigma^2 = 1 / (2 esn0), for n bits.
+cudaError_t launch_awgn(const uint8_t* bits, int64_t n, double esn0, uint64_t seed, int dtype, void* out, cudaStream_t s);
+
 // Uploads of every translation unit's __constant__ tables to the current device
 // (each launcher calls its own; a stream capture must run them before it starts).
 cudaError_t ldpc_flood_init();

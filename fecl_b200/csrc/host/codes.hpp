@@ -60,6 +60,12 @@ class LdpcCode {
   void encode(const uint8_t* msg, uint8_t* parity) const;
   bool check(const uint8_t* parity) const;
 
+  // The generator pieces encode() walks, for the device encoder.
+  const Csr& gen_dc() const { return DC_; }
+  const Csr& gen_a() const { return A_; }
+  const Csr& gen_b() const { return B_; }
+  const Csr& gen_t() const { return T_; }
+
  private:
   void compute_generator(Csr H);
 

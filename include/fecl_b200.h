@@ -175,9 +175,18 @@ int fecl_turbo_set_options(fecl_codec_t codec, const fecl_turbo_options* options
 
 int fecl_codec_sizes(fecl_codec_t codec, fecl_sizes* sizes);
 
-/* Codec::encode -- src/Codec.h:171-198.  Bits are one byte each (0/1). */
+/* Codec::encode -- src/Codec.h:171-198.  Bits are one byte each (0/1).  With
+ * FECL_DEVICE_MEMORY the frames are encoded on the GPU (one thread per frame, the
+ * reference's encoding steps, bit-exact), asynchronously on `stream`. */
 int fecl_encode(fecl_codec_t codec, const uint8_t* msg, uint64_t nframes, uint8_t* parity, int32_t flags,
                 void* stream);
+
+/* BPSK over AWGN on the GPU (an extension): bit b -> x = 2b - 1, y = x + N(0, s2) with
+ * s2 = 1 / (2 Es/N0), Es/N0 = 10^(ebn0_db / 10) * rate, out = 2 y / s2 in out_dtype.
+ * bits and out are device memory; counter-based Philox-4x32-10 noise keyed by `seed`
+ * (the same seed gives the same L-values).  Asynchronous on `stream`. */
+int fecl_awgn_llr(const uint8_t* bits, uint64_t n, double ebn0_db, double rate, uint64_t seed, int32_t out_dtype,
+                  void* out, void* stream);
 
 /* Codec::check -- src/Codec.h:137-145; *ok = 1 when every frame is a codeword. */
 int fecl_check(fecl_codec_t codec, const uint8_t* parity, uint64_t nframes, int32_t* ok);
