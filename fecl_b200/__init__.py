@@ -26,7 +26,7 @@ from ._lib import lib as _L
 
 __all__ = [
     "Exact", "Linear", "Approximate", "Serial", "Parallel", "Custom",
-    "SparseBitMatrix", "Trellis", "Codec", "Ldpc", "Turbo", "Batch", "Server", "FeclError", "lib_path",
+    "SparseBitMatrix", "Trellis", "Codec", "Ldpc", "Turbo", "Batch", "Server", "Permutation", "FeclError", "lib_path",
 ]
 
 # DecoderAlgorithm (src/DecoderAlgorithm.h:30-34) and SchedulingType (src/SchedulingType.h:32-39)
@@ -434,7 +434,32 @@ class Ldpc(Codec):
             return self
 
     class PunctureOptions:
-        pass
+        """Ldpc::PunctureOptions -- src/detail/Ldpc.h (mask, systMask: repeating bit masks)."""
+
+        def __init__(self):
+            self._mask, self._syst = [], []
+
+        def mask(self, m=None):
+            if m is None:
+                return list(self._mask)
+            self._mask = [bool(x) for x in m]
+            return self
+
+        def systMask(self, m=None):
+            if m is None:
+                return list(self._syst)
+            self._syst = [bool(x) for x in m]
+            return self
+
+    def puncturing(self, options):
+        """Ldpc::puncturing -- src/Ldpc.h:94: the fec::Permutation of the kept code bits."""
+        m = np.asarray(options._mask, np.uint8)
+        sm = np.asarray(options._syst, np.uint8)
+        n = C.c_uint64()
+        _check(_L.fecl_ldpc_puncturing(self._h, _ptr(m), m.size, _ptr(sm), sm.size, None, C.byref(n)))
+        seq = np.zeros(n.value, np.uint32)
+        _check(_L.fecl_ldpc_puncturing(self._h, _ptr(m), m.size, _ptr(sm), sm.size, _ptr(seq), C.byref(n)))
+        return Permutation(seq, self.paritySize())
 
     class Gallager:
         @staticmethod
@@ -579,6 +604,34 @@ class Turbo(Codec):
             self._term = list(t) if isinstance(t, (list, tuple)) else [t]
             return self
 
+    Alternate, Group = 0, 1  # Turbo::BitOrdering, src/detail/Turbo.h:54-57
+
+    class PunctureOptions:
+        """Turbo::PunctureOptions -- src/detail/Turbo.h: mask (one repeating mask per
+        stream: systematic, then each constituent's parity), tailMask (two per
+        constituent), bitOrdering (Alternate or Group)."""
+
+        def __init__(self):
+            self._mask, self._tail, self._ordering = [], [], 0
+
+        def mask(self, m=None):
+            if m is None:
+                return [list(x) for x in self._mask]
+            self._mask = [[bool(b) for b in x] for x in m]
+            return self
+
+        def tailMask(self, m=None):
+            if m is None:
+                return [list(x) for x in self._tail]
+            self._tail = [[bool(b) for b in x] for x in m]
+            return self
+
+        def bitOrdering(self, o=None):
+            if o is None:
+                return self._ordering
+            self._ordering = int(o)
+            return self
+
     class DecoderOptions:
         """Turbo::DecoderOptions -- src/detail/Turbo.h:77-101."""
 
@@ -658,6 +711,21 @@ class Turbo(Codec):
         _check(_L.fecl_turbo_set_options(self._h, C.byref(opts)))
         self._decoder = decoder
 
+    def puncturing(self, options):
+        """Turbo::puncturing -- src/Turbo.h:102: the fec::Permutation of the kept code bits."""
+        def flat(ms):
+            data = np.asarray([b for x in ms for b in x], np.uint8)
+            lens = np.asarray([len(x) for x in ms], np.uint32)
+            return data, lens
+        md, ml = flat(options._mask)
+        td, tl = flat(options._tail)
+        n = C.c_uint64()
+        args = (_ptr(md), _ptr(ml), ml.size, _ptr(td), _ptr(tl), tl.size, options._ordering)
+        _check(_L.fecl_turbo_puncturing(self._h, *args, None, C.byref(n)))
+        seq = np.zeros(n.value, np.uint32)
+        _check(_L.fecl_turbo_puncturing(self._h, *args, _ptr(seq), C.byref(n)))
+        return Permutation(seq, self.paritySize())
+
     def setWindowTraining(self, steps):
         """Extension: training steps of the windowed LTE decoder (multiple of 8, -1 default)."""
         _check(_L.fecl_turbo_set_window_training(self._h, int(steps)))
@@ -670,6 +738,67 @@ class Turbo(Codec):
 
     def getDecoderOptions(self):
         return self._decoder
+
+
+class Permutation:
+    """fec::Permutation -- src/Permutation.h: a sequence of input indices.  permute()
+    gathers out[i] = in[seq[i]] block by block; dePermute() scatters back and leaves
+    zeros (erasures) where nothing maps.  Both run on the GPU: torch CUDA tensors stay
+    there (asynchronous on the current stream); numpy arrays are copied through."""
+
+    def __init__(self, sequence, inputSize=None):
+        self._seq = np.ascontiguousarray(np.asarray(sequence, np.uint32).ravel())
+        self._in = int(inputSize) if inputSize is not None else (int(self._seq.max()) + 1 if self._seq.size else 0)
+        self._h = None
+
+    def inputSize(self):
+        return self._in
+
+    def outputSize(self):
+        return int(self._seq.size)
+
+    def __getitem__(self, i):
+        return int(self._seq[i])
+
+    def sequence(self):
+        return self._seq.copy()
+
+    def _handle(self):
+        if self._h is None:
+            h = C.c_void_p()
+            _check(_L.fecl_permutation_create(_ptr(self._seq), self._seq.size, self._in, C.byref(h)))
+            self._h = h
+        return self._h
+
+    def _apply(self, x, inverse):
+        import torch
+        host = not _is_device(x)
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(x))).cuda() if host else x.contiguous()
+        t = t.view(-1)
+        codes = {torch.float64: _lib.F64, torch.float32: _lib.F32, torch.float16: _lib.F16, torch.uint8: _lib.U8}
+        if t.dtype not in codes:
+            raise ValueError("unsupported element type")
+        size_in, size_out = (self.outputSize(), self._in) if inverse else (self._in, self.outputSize())
+        if size_in == 0 or t.numel() % size_in:
+            raise ValueError("Invalid input size")
+        nb = t.numel() // size_in
+        out = torch.empty(nb * size_out, dtype=t.dtype, device=t.device)
+        stream = torch.cuda.current_stream(t.device).cuda_stream
+        _check(_L.fecl_permute(self._handle(), C.c_void_p(t.data_ptr()), codes[t.dtype], nb, C.c_void_p(out.data_ptr()),
+                               1 if inverse else 0, C.c_void_p(stream)))
+        return out.cpu().numpy() if host else out
+
+    def permute(self, x):
+        return self._apply(x, False)
+
+    def dePermute(self, x):
+        return self._apply(x, True)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _L.fecl_permutation_destroy(h)
+            self._h = None
 
 
 class Batch:

@@ -10,7 +10,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfecl_b200.so")
 
 OK, EINVAL, ECUDA, ENOMEM, ETIMEDOUT, EUNSUPPORTED, ENODEV = 0, -1, -2, -3, -4, -5, -6
-F64, F32, F16 = 0, 1, 2
+F64, F32, F16, U8 = 0, 1, 2, 3
 MSG_F32, MSG_F16, MSG_I8 = 0, 1, 2
 HOST_MEMORY, DEVICE_MEMORY = 0, 1
 KERNEL_AUTO, KERNEL_GENERIC = 0, 1
@@ -113,6 +113,13 @@ SIGNATURES = [
     ("fecl_decode", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     ("fecl_so_decode", C.c_int, [C.c_void_p, C.POINTER(fecl_so_io), C.c_uint64, C.c_int32, C.c_void_p]),
     ("fecl_destroy", None, [C.c_void_p]),
+    ("fecl_ldpc_puncturing", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                       C.POINTER(C.c_uint64)]),
+    ("fecl_turbo_puncturing", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                        C.c_uint32, C.c_int32, C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("fecl_permutation_create", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("fecl_permute", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_uint64, C.c_void_p, C.c_int32, C.c_void_p]),
+    ("fecl_permutation_destroy", None, [C.c_void_p]),
     ("fecl_set_kernel", C.c_int, [C.c_void_p, C.c_int32]),
     ("fecl_ldpc_set_cluster_shape", C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     ("fecl_ldpc_set_wave", C.c_int, [C.c_void_p, C.c_int32]),

@@ -692,6 +692,95 @@ int fecl_so_decode(fecl_codec_t codec, const fecl_so_io* io, uint64_t nframes, i
   });
 }
 
+int fecl_ldpc_puncturing(fecl_codec_t codec, const uint8_t* mask, uint32_t mask_len, const uint8_t* syst_mask,
+                         uint32_t syst_mask_len, uint32_t* seq, uint64_t* seq_len) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 0) fail(FECL_EINVAL, "not an LDPC codec");
+    if (!seq_len) fail(FECL_EINVAL, "null output");
+    std::vector<uint8_t> m(mask, mask + (mask ? mask_len : 0)), sm(syst_mask, syst_mask + (syst_mask ? syst_mask_len : 0));
+    const auto v = fecl::ldpc_puncturing(*c->ldpc, m, sm);
+    *seq_len = v.size();
+    if (seq) std::memcpy(seq, v.data(), v.size() * sizeof(uint32_t));
+  });
+}
+
+int fecl_turbo_puncturing(fecl_codec_t codec, const uint8_t* mask_data, const uint32_t* mask_len, uint32_t n_masks,
+                          const uint8_t* tail_data, const uint32_t* tail_len, uint32_t n_tail, int32_t bit_ordering,
+                          uint32_t* seq, uint64_t* seq_len) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 1) fail(FECL_EINVAL, "not a turbo codec");
+    if (!seq_len) fail(FECL_EINVAL, "null output");
+    auto split = [](const uint8_t* data, const uint32_t* len, uint32_t n) {
+      std::vector<std::vector<uint8_t>> v(n);
+      size_t off = 0;
+      for (uint32_t i = 0; i < n; ++i) {
+        if (len[i] && !data) fail(FECL_EINVAL, "null mask data");
+        v[i].assign(data + off, data + off + len[i]);
+        off += len[i];
+      }
+      return v;
+    };
+    if ((n_masks && !mask_len) || (n_tail && !tail_len)) fail(FECL_EINVAL, "null mask lengths");
+    const auto v = fecl::turbo_puncturing(*c->turbo, split(mask_data, mask_len, n_masks), split(tail_data, tail_len, n_tail),
+                                          bit_ordering);
+    *seq_len = v.size();
+    if (seq) std::memcpy(seq, v.data(), v.size() * sizeof(uint32_t));
+  });
+}
+
+int fecl_permutation_create(const uint32_t* seq, uint64_t output_size, uint64_t input_size, fecl_permutation_t* out) {
+  return guarded([&] {
+    if (!out || (output_size && !seq)) fail(FECL_EINVAL, "null argument");
+    if (input_size >= 0xffffffffull) fail(FECL_EINVAL, "permutation input too large");
+    std::vector<uint32_t> fwd(seq, seq + output_size), inv(input_size, 0xffffffffu);
+    for (uint64_t i = 0; i < output_size; ++i) {
+      if (fwd[i] >= input_size) fail(FECL_EINVAL, "permutation index out of range");
+      inv[fwd[i]] = uint32_t(i);
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      fail(FECL_ENODEV, "no CUDA device is visible");
+    }
+    std::unique_ptr<fecl_permutation_s> p(new fecl_permutation_s);
+    cuda_check(cudaGetDevice(&p->device), "cudaGetDevice");
+    p->out_size = output_size;
+    p->in_size = input_size;
+    p->fwd.upload(fwd);
+    p->inv.upload(inv);
+    *out = p.release();
+  });
+}
+
+int fecl_permute(fecl_permutation_t perm, const void* in, int32_t elem_type, uint64_t nblocks, void* out, int32_t inverse,
+                 void* stream) {
+  return guarded([&] {
+    if (!perm || !in || !out) fail(FECL_EINVAL, "null argument");
+    const int bytes = elem_type == FECL_U8 ? 1 : int(dsize(elem_type));
+    DeviceGuard dg(perm->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!inverse)
+      cuda_check(fecl::launch_gather(in, out, perm->fwd.as<uint32_t>(), int64_t(perm->in_size), int64_t(perm->out_size),
+                                     int64_t(nblocks), bytes, 0, s),
+                 "permute");
+    else
+      cuda_check(fecl::launch_gather(in, out, perm->inv.as<uint32_t>(), int64_t(perm->out_size), int64_t(perm->in_size),
+                                     int64_t(nblocks), bytes, 1, s),
+                 "dePermute");
+  });
+}
+
+void fecl_permutation_destroy(fecl_permutation_t perm) {
+  if (!perm) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(perm->device);
+  delete perm;
+  if (prev >= 0) cudaSetDevice(prev);
+}
+
 int fecl_set_kernel(fecl_codec_t codec, int32_t kernel) {
   return guarded([&] {
     auto c = checked(codec);

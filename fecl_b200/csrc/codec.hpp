@@ -18,6 +18,7 @@
 #include "device/kernels.hpp"
 #include "host/codes.hpp"
 #include "host/ldpc_plan.hpp"
+#include "host/puncture.hpp"
 
 namespace fecl {
 // Sets the message fecl_last_error() returns on this thread.
@@ -389,6 +390,13 @@ struct fecl_codec_s {
     cuda_check(cudaEventRecord(done, s), "cudaEventRecord");
     pending = true;
   }
+};
+
+// A permutation on the device: the gather map and its last-writer inverse.
+struct fecl_permutation_s {
+  int device = 0;
+  uint64_t out_size = 0, in_size = 0;
+  DeviceBuffer fwd, inv;
 };
 
 namespace fecl {

@@ -247,6 +247,11 @@ cudaError_t launch_turbo_encode(const TurboDeviceCode& code, const uint8_t* msg,
 // L = 2 y / sigma^2 with y = (2 b - 1) + N(0, sigma^2), sigma^2 = 1 / (2 esn0), for n bits.
 cudaError_t launch_awgn(const uint8_t* bits, int64_t n, double esn0, uint64_t seed, int dtype, void* out, cudaStream_t s);
 
+// out[b][i] = in[b][map[i]] for b < nblocks, i < out_size (permute.cu); with zero_fill,
+// map[i] == 0xffffffff gives zero (dePermute of a punctured position).
+cudaError_t launch_gather(const void* in, void* out, const uint32_t* map, int64_t in_size, int64_t out_size,
+                          int64_t nblocks, int elem_bytes, int zero_fill, cudaStream_t s);
+
 // Uploads of every translation unit's __constant__ tables to the current device
 // (each launcher calls its own; a stream capture must run them before it starts).
 cudaError_t ldpc_flood_init();

@@ -56,10 +56,11 @@ extern "C" {
 /* Trellis::Termination, src/Trellis.h */
 #define FECL_TAIL 0
 #define FECL_TRUNCATE 1
-/* element types of L-value buffers */
+/* element types of L-value buffers (FECL_U8: bits, for fecl_permute) */
 #define FECL_F64 0
 #define FECL_F32 1
 #define FECL_F16 2
+#define FECL_U8 3
 /* precision of the decoder's internal messages (an extension; FP32 is the reference-parity mode) */
 #define FECL_MSG_F32 0
 #define FECL_MSG_F16 1
@@ -213,6 +214,33 @@ typedef struct {
 int fecl_so_decode(fecl_codec_t codec, const fecl_so_io* io, uint64_t nframes, int32_t flags, void* stream);
 
 void fecl_destroy(fecl_codec_t codec);
+
+/* ---- puncturing ------------------------------------------------------------ */
+
+/* Ldpc::puncturing (src/Ldpc.h:94, src/detail/Ldpc.cpp:333-353): the kept code-bit
+ * indices of Ldpc::PunctureOptions().mask(mask).systMask(syst_mask), the sequence of
+ * the fec::Permutation the reference returns (input size paritySize).  Call with
+ * seq == NULL for the length. */
+int fecl_ldpc_puncturing(fecl_codec_t codec, const uint8_t* mask, uint32_t mask_len, const uint8_t* syst_mask,
+                         uint32_t syst_mask_len, uint32_t* seq, uint64_t* seq_len);
+
+/* Turbo::puncturing (src/Turbo.h:102, src/detail/Turbo.cpp:200-320): masks as
+ * concatenated bytes with one length each -- n_masks 0 or constituents + 1 (systematic,
+ * then each constituent's parity), n_tail 0 or 2 per constituent; bit_ordering 0 =
+ * Alternate, 1 = Group (Turbo::BitOrdering). */
+int fecl_turbo_puncturing(fecl_codec_t codec, const uint8_t* mask_data, const uint32_t* mask_len, uint32_t n_masks,
+                          const uint8_t* tail_data, const uint32_t* tail_len, uint32_t n_tail, int32_t bit_ordering,
+                          uint32_t* seq, uint64_t* seq_len);
+
+/* fec::Permutation (src/Permutation.h) on the device: permute gathers
+ * out[b][i] = in[b][seq[i]] (blocks of input_size -> output_size); the inverse,
+ * dePermute, scatters back and leaves zeros (erasures) where nothing maps.  Buffers
+ * are device memory of elem_type (FECL_F64 / F32 / F16 / U8); asynchronous on stream. */
+typedef struct fecl_permutation_s* fecl_permutation_t;
+int fecl_permutation_create(const uint32_t* seq, uint64_t output_size, uint64_t input_size, fecl_permutation_t* out);
+int fecl_permute(fecl_permutation_t perm, const void* in, int32_t elem_type, uint64_t nblocks, void* out, int32_t inverse,
+                 void* stream);
+void fecl_permutation_destroy(fecl_permutation_t perm);
 
 /* ---- extensions (no counterpart in the reference) ------------------------ */
 

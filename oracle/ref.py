@@ -183,3 +183,32 @@ class RefCodec:
         _chk(lib().fref_codec_so_decode(self.h, C.c_size_t(n), _p(x), _p(s), _p(st), _p(out.get("msg")),
                                         _p(out.get("syst")), _p(out.get("parity")), _p(out.get("state"))))
         return out
+
+    def ldpc_puncturing(self, mask=(), syst_mask=()):
+        """Ldpc::Structure::puncturing (src/detail/Ldpc.cpp:333-353): (sequence, input size)."""
+        m = np.ascontiguousarray(np.asarray(mask, np.uint8).reshape(-1)) if len(mask) else np.zeros(1, np.uint8)
+        sm = np.ascontiguousarray(np.asarray(syst_mask, np.uint8).reshape(-1)) if len(syst_mask) else np.zeros(1, np.uint8)
+        n, ins = C.c_size_t(), C.c_size_t()
+        L = lib()
+        _chk(L.fref_ldpc_puncturing(self.h, _p(m), C.c_size_t(len(mask)), _p(sm), C.c_size_t(len(syst_mask)), None,
+                                    C.byref(n), C.byref(ins)))
+        seq = np.zeros(max(n.value, 1), np.uint32)
+        _chk(L.fref_ldpc_puncturing(self.h, _p(m), C.c_size_t(len(mask)), _p(sm), C.c_size_t(len(syst_mask)), _p(seq),
+                                    C.byref(n), C.byref(ins)))
+        return seq[: n.value], ins.value
+
+    def turbo_puncturing(self, masks=(), tails=(), ordering=0):
+        """Turbo::Structure::puncturing (src/detail/Turbo.cpp:200-320): (sequence, input size)."""
+        def flat(ms):
+            data = np.asarray([b for x in ms for b in x] or [0], np.uint8)
+            lens = np.asarray([len(x) for x in ms] or [0], np.uintp)
+            return data, lens
+        md, ml = flat(masks)
+        td, tl = flat(tails)
+        n, ins = C.c_size_t(), C.c_size_t()
+        L = lib()
+        args = (self.h, _p(md), _p(ml), C.c_size_t(len(masks)), _p(td), _p(tl), C.c_size_t(len(tails)), C.c_int(ordering))
+        _chk(L.fref_turbo_puncturing(*args, None, C.byref(n), C.byref(ins)))
+        seq = np.zeros(max(n.value, 1), np.uint32)
+        _chk(L.fref_turbo_puncturing(*args, _p(seq), C.byref(n), C.byref(ins)))
+        return seq[: n.value], ins.value

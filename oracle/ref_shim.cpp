@@ -224,6 +224,51 @@ int fref_turbo_create(size_t nconst, const fref_trellis* trellis, size_t ntrelli
   });
 }
 
+// Ldpc::Structure::puncturing (src/detail/Ldpc.cpp:333-353): the kept code-bit
+// indices and the permutation's input size.  Call with seq == NULL for the length.
+int fref_ldpc_puncturing(void* h, const uint8_t* mask, size_t mask_len, const uint8_t* syst_mask, size_t syst_len,
+                         uint32_t* seq, size_t* seq_len, size_t* input_size) {
+  return guarded([&] {
+    auto rc = static_cast<RefCodec*>(h);
+    fec::Ldpc::PunctureOptions o;
+    o.mask(std::vector<bool>(mask, mask + mask_len));
+    o.systMask(std::vector<bool>(syst_mask, syst_mask + syst_len));
+    const fec::Permutation p = rc->ldpc->puncturing(o);
+    *seq_len = p.outputSize();
+    *input_size = p.inputSize();
+    if (seq)
+      for (size_t i = 0; i < p.outputSize(); ++i) seq[i] = uint32_t(p[i]);
+  });
+}
+
+// Turbo::Structure::puncturing (src/detail/Turbo.cpp:200-320); masks are given as
+// concatenated bytes with one length per mask, ordering 0 = Alternate, 1 = Group.
+int fref_turbo_puncturing(void* h, const uint8_t* mask_data, const size_t* mask_len, size_t n_masks,
+                          const uint8_t* tail_data, const size_t* tail_len, size_t n_tail, int ordering, uint32_t* seq,
+                          size_t* seq_len, size_t* input_size) {
+  return guarded([&] {
+    auto rc = static_cast<RefCodec*>(h);
+    std::vector<std::vector<bool>> m(n_masks), t(n_tail);
+    size_t off = 0;
+    for (size_t i = 0; i < n_masks; ++i) {
+      m[i].assign(mask_data + off, mask_data + off + mask_len[i]);
+      off += mask_len[i];
+    }
+    off = 0;
+    for (size_t i = 0; i < n_tail; ++i) {
+      t[i].assign(tail_data + off, tail_data + off + tail_len[i]);
+      off += tail_len[i];
+    }
+    fec::Turbo::PunctureOptions o;
+    o.mask(m).tailMask(t).bitOrdering(ordering == 0 ? fec::Turbo::BitOrdering::Alternate : fec::Turbo::BitOrdering::Group);
+    const fec::Permutation p = rc->turbo->puncturing(o);
+    *seq_len = p.outputSize();
+    *input_size = p.inputSize();
+    if (seq)
+      for (size_t i = 0; i < p.outputSize(); ++i) seq[i] = uint32_t(p[i]);
+  });
+}
+
 void fref_codec_destroy(void* h) { delete static_cast<RefCodec*>(h); }
 
 int fref_codec_sizes(void* h, size_t* out4) {
