@@ -26,7 +26,7 @@ from ._lib import lib as _L
 
 __all__ = [
     "Exact", "Linear", "Approximate", "Serial", "Parallel", "Custom",
-    "SparseBitMatrix", "Trellis", "Codec", "Ldpc", "Turbo", "Batch", "Server", "Permutation", "FeclError", "lib_path",
+    "SparseBitMatrix", "Trellis", "Codec", "Ldpc", "Turbo", "Convolutional", "Batch", "Server", "Permutation", "FeclError", "lib_path",
 ]
 
 # DecoderAlgorithm (src/DecoderAlgorithm.h:30-34) and SchedulingType (src/SchedulingType.h:32-39)
@@ -738,6 +738,91 @@ class Turbo(Codec):
 
     def getDecoderOptions(self):
         return self._decoder
+
+
+class Convolutional(Codec):
+    """fec::Convolutional -- src/Convolutional.h:40-81: decode by Viterbi, soDecode by
+    the MAP decoder, on the GPU."""
+
+    class EncoderOptions:
+        """Convolutional::EncoderOptions -- src/detail/Convolutional.h:36-46 (termination
+        defaults to Truncate)."""
+
+        def __init__(self, trellis, length):
+            self._trellis = trellis
+            self._length = int(length)
+            self._term = Trellis.Truncate
+
+        def termination(self, t=None):
+            if t is None:
+                return self._term
+            self._term = int(t)
+            return self
+
+    class DecoderOptions:
+        """Convolutional::DecoderOptions -- src/detail/Convolutional.h:48-62."""
+
+        def __init__(self):
+            self._alg = Approximate
+            self._sf = 1.0
+
+        def algorithm(self, a=None):
+            if a is None:
+                return self._alg
+            self._alg = int(a)
+            return self
+
+        def scalingFactor(self, f=None):
+            if f is None:
+                return self._sf
+            self._sf = float(f)
+            return self
+
+    class PunctureOptions:
+        """Convolutional::PunctureOptions -- src/detail/Convolutional.h:64-75."""
+
+        def __init__(self):
+            self._mask, self._tail = [], []
+
+        def mask(self, m=None):
+            if m is None:
+                return list(self._mask)
+            self._mask = [bool(x) for x in m]
+            return self
+
+        def tailMask(self, m=None):
+            if m is None:
+                return list(self._tail)
+            self._tail = [bool(x) for x in m]
+            return self
+
+    def __init__(self, encoder, decoder=None, workGroupSize=8):
+        decoder = decoder or Convolutional.DecoderOptions()
+        o = _lib.fecl_conv_options(decoder._alg, decoder._sf)
+        tr = encoder._trellis._c()
+        h = C.c_void_p()
+        _check(_L.fecl_conv_create(C.byref(tr), encoder._length, encoder._term, C.byref(o), C.byref(h)))
+        super().__init__(h.value)
+        self._decoder = decoder
+        self._work_group = workGroupSize
+
+    def setDecoderOptions(self, decoder):
+        o = _lib.fecl_conv_options(decoder._alg, decoder._sf)
+        _check(_L.fecl_conv_set_options(self._h, C.byref(o)))
+        self._decoder = decoder
+
+    def getDecoderOptions(self):
+        return self._decoder
+
+    def puncturing(self, options):
+        """Convolutional::puncturing -- src/Convolutional.h:73."""
+        m = np.asarray(options._mask, np.uint8)
+        t = np.asarray(options._tail, np.uint8)
+        n = C.c_uint64()
+        _check(_L.fecl_conv_puncturing(self._h, _ptr(m), m.size, _ptr(t), t.size, None, C.byref(n)))
+        seq = np.zeros(n.value, np.uint32)
+        _check(_L.fecl_conv_puncturing(self._h, _ptr(m), m.size, _ptr(t), t.size, _ptr(seq), C.byref(n)))
+        return Permutation(seq, self.paritySize())
 
 
 class Permutation:

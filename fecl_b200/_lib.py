@@ -54,6 +54,10 @@ class fecl_turbo_options(C.Structure):
     ]
 
 
+class fecl_conv_options(C.Structure):
+    _fields_ = [("algorithm", C.c_int32), ("scaling", C.c_double)]
+
+
 class fecl_so_io(C.Structure):
     _fields_ = [
         ("parity", C.c_void_p),
@@ -105,6 +109,11 @@ SIGNATURES = [
     ("fecl_turbo_create_lte", C.c_int, [C.c_uint32, C.POINTER(fecl_turbo_options), C.POINTER(C.c_void_p)]),
     ("fecl_lte_interleaver", C.c_int, [C.c_uint32, C.c_void_p]),
     ("fecl_turbo_set_options", C.c_int, [C.c_void_p, C.POINTER(fecl_turbo_options)]),
+    ("fecl_conv_create", C.c_int, [C.POINTER(fecl_trellis), C.c_uint32, C.c_int32, C.POINTER(fecl_conv_options),
+                                   C.POINTER(C.c_void_p)]),
+    ("fecl_conv_set_options", C.c_int, [C.c_void_p, C.POINTER(fecl_conv_options)]),
+    ("fecl_conv_puncturing", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                       C.POINTER(C.c_uint64)]),
     ("fecl_codec_sizes", C.c_int, [C.c_void_p, C.POINTER(fecl_sizes)]),
     ("fecl_encode", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int32, C.c_void_p]),
     ("fecl_check", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_int32)]),

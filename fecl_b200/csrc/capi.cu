@@ -126,6 +126,11 @@ ScratchPlan plan_scratch(fecl_codec_s* c, uint64_t n, bool lte_fast) {
   Carver cv;
   ScratchPlan sp;
   const uint64_t P = c->parity(), X = c->state();
+  if (c->kind == 2) {
+    sp.o1 = cv.take(std::max(fecl::viterbi_scratch_bytes(c->cdev, int64_t(n)), fecl::conv_map_scratch_bytes(c->cdev, int64_t(n))));
+    sp.bytes = cv.off;
+    return sp;
+  }
   uint32_t C = 0;
   int threads = 0;
   // LDPC kernel choice under FECL_KERNEL_AUTO: the lane-batched decoder where it
@@ -180,7 +185,31 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
                    int32_t out_dtype, bool soft, bool lte_fast, cudaStream_t s) {
   cudaError_t e;
   auto at = [&](size_t off) { return d.scratch + off; };
-  if (c->kind == 0 && sp.cluster) {
+  if (c->kind == 2) {
+    if (soft) {
+      fecl::ConvMapRun r;
+      r.nframes = int64_t(n);
+      r.algorithm = c->conv->decoder().algorithm;
+      r.sf = float(c->conv->decoder().scaling);
+      r.llr = d.llr;
+      r.syst_in = d.syst;
+      r.llr_dtype = in_dtype;
+      r.msg_out = d.msg;
+      r.syst_out = d.syst_out;
+      r.parity_out = d.parity_out;
+      r.out_dtype = out_dtype;
+      e = fecl::launch_conv_map(c->cdev, r, at(sp.o1), s);
+    } else {
+      fecl::ViterbiRun r;
+      r.nframes = int64_t(n);
+      r.llr = d.llr;
+      r.llr_dtype = in_dtype;
+      r.hard = d.hard;
+      r.trace = reinterpret_cast<uint8_t*>(at(sp.o1));
+      e = fecl::launch_viterbi(c->cdev, r, s);
+      if (e == cudaSuccess && d.iters) e = cudaMemsetAsync(d.iters, 0, n * sizeof(int32_t), s);
+    }
+  } else if (c->kind == 0 && sp.cluster) {
     auto& cd = c->cluster_plan(sp.cluster);
     c->upload_cluster(cd);
     fecl::LdpcClusterParams r;
@@ -569,6 +598,44 @@ int fecl_turbo_create(uint32_t n_constituents, const fecl_trellis* trellis, uint
   });
 }
 
+int fecl_conv_create(const fecl_trellis* trellis, uint32_t length, int32_t termination, const fecl_conv_options* options,
+                     fecl_codec_t* out) {
+  return guarded([&] {
+    if (!out || !trellis) fail(FECL_EINVAL, "null argument");
+    std::unique_ptr<fecl_codec_s> c(new fecl_codec_s);
+    c->kind = 2;
+    c->conv.reset(new fecl::ConvCode(fecl::Trellis::from_tables(trellis->state_count, trellis->input_count,
+                                                                trellis->output_size, trellis->next_state, trellis->output),
+                                     length, termination));
+    if (options) c->conv->set_decoder(fecl::ConvDecoderConfig{options->algorithm, options->scaling});
+    *out = c.release();
+  });
+}
+
+int fecl_conv_set_options(fecl_codec_t codec, const fecl_conv_options* options) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 2) fail(FECL_EINVAL, "not a convolutional codec");
+    if (!options) fail(FECL_EINVAL, "null options");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->conv->set_decoder(fecl::ConvDecoderConfig{options->algorithm, options->scaling});
+    c->generation.fetch_add(1);
+  });
+}
+
+int fecl_conv_puncturing(fecl_codec_t codec, const uint8_t* mask, uint32_t mask_len, const uint8_t* tail_mask,
+                         uint32_t tail_mask_len, uint32_t* seq, uint64_t* seq_len) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 2) fail(FECL_EINVAL, "not a convolutional codec");
+    if (!seq_len) fail(FECL_EINVAL, "null output");
+    std::vector<uint8_t> m(mask, mask + (mask ? mask_len : 0)), t(tail_mask, tail_mask + (tail_mask ? tail_mask_len : 0));
+    const auto v = fecl::conv_puncturing(*c->conv, m, t);
+    *seq_len = v.size();
+    if (seq) std::memcpy(seq, v.data(), v.size() * sizeof(uint32_t));
+  });
+}
+
 int fecl_lte_interleaver(uint32_t K, uint32_t* perm) {
   return guarded([&] {
     auto p = fecl::lte_interleaver(K);
@@ -627,13 +694,15 @@ int fecl_encode(fecl_codec_t codec, const uint8_t* msg, uint64_t nframes, uint8_
       DeviceGuard dg(c->device);
       cudaStream_t s = static_cast<cudaStream_t>(stream);
       if (c->kind == 0) cuda_check(fecl::launch_ldpc_encode(c->ltab, msg, parity, int64_t(nframes), s), "encode");
-      else cuda_check(fecl::launch_turbo_encode(c->tdev, msg, parity, int64_t(nframes), s), "encode");
+      else if (c->kind == 1) cuda_check(fecl::launch_turbo_encode(c->tdev, msg, parity, int64_t(nframes), s), "encode");
+      else cuda_check(fecl::launch_conv_encode(c->cdev, msg, parity, int64_t(nframes), s), "encode");
       return;
     }
     if (flags != FECL_HOST_MEMORY) fail(FECL_EINVAL, "Invalid memory flag");
     for (uint64_t f = 0; f < nframes; ++f) {
       if (c->kind == 0) c->ldpc->encode(msg + f * M, parity + f * P);
-      else c->turbo->encode(msg + f * M, parity + f * P);
+      else if (c->kind == 1) c->turbo->encode(msg + f * M, parity + f * P);
+      else c->conv->encode(msg + f * M, parity + f * P);
     }
   });
 }
@@ -660,7 +729,10 @@ int fecl_check(fecl_codec_t codec, const uint8_t* parity, uint64_t nframes, int3
     if (!parity || !ok) fail(FECL_EINVAL, "null buffer");
     const uint64_t P = c->parity();
     int32_t r = 1;
-    for (uint64_t f = 0; f < nframes && r; ++f) r = (c->kind == 0 ? c->ldpc->check(parity + f * P) : c->turbo->check(parity + f * P)) ? 1 : 0;
+    for (uint64_t f = 0; f < nframes && r; ++f) {
+      const uint8_t* q = parity + f * P;
+      r = (c->kind == 0 ? c->ldpc->check(q) : c->kind == 1 ? c->turbo->check(q) : c->conv->check(q)) ? 1 : 0;
+    }
     *ok = r;
   });
 }

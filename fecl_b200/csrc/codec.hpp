@@ -111,6 +111,8 @@ struct fecl_codec_s {
   int device = 0;
   std::unique_ptr<fecl::LdpcCode> ldpc;
   std::unique_ptr<fecl::TurboCode> turbo;
+  std::unique_ptr<fecl::ConvCode> conv;  // kind 2
+  fecl::TurboDeviceConstituent cdev{};   // the convolutional trellis on the device
   std::mutex mu;
   cudaStream_t stream = nullptr;   // host-memory calls: first pipeline stream
   cudaStream_t stream2 = nullptr;  // host-memory calls: second pipeline stream
@@ -138,10 +140,10 @@ struct fecl_codec_s {
     if (done) cudaEventDestroy(done);
   }
 
-  uint64_t msg() const { return kind == 0 ? ldpc->msg_size() : turbo->msg_size(); }
-  uint64_t syst() const { return kind == 0 ? ldpc->syst_size() : turbo->syst_size(); }
-  uint64_t parity() const { return kind == 0 ? ldpc->parity_size() : turbo->parity_size(); }
-  uint64_t state() const { return kind == 0 ? ldpc->state_size() : turbo->state_size(); }
+  uint64_t msg() const { return kind == 0 ? ldpc->msg_size() : kind == 1 ? turbo->msg_size() : conv->msg_size(); }
+  uint64_t syst() const { return kind == 0 ? ldpc->syst_size() : kind == 1 ? turbo->syst_size() : conv->syst_size(); }
+  uint64_t parity() const { return kind == 0 ? ldpc->parity_size() : kind == 1 ? turbo->parity_size() : conv->parity_size(); }
+  uint64_t state() const { return kind == 0 ? ldpc->state_size() : kind == 1 ? turbo->state_size() : 0; }
 
   void init_runtime() {
     int n = 0;
@@ -257,6 +259,34 @@ struct fecl_codec_s {
       tdev.max_states = std::max(tdev.max_states, int32_t(c.trellis.state_count));
     }
     upload_turbo_options();
+  }
+
+  void upload_conv() {
+    const fecl::Constituent& c = conv->constituent();
+    if (c.trellis.state_count > 64 || c.trellis.input_count > 4 || c.trellis.output_size > 6)
+      fail(FECL_EUNSUPPORTED, "trellis too large for the device decoder");
+    tables.clear();
+    std::vector<uint32_t> padded_perm(c.perm);
+    padded_perm.resize(c.perm.size() + 16, 0);
+    for (const std::vector<uint32_t>* v : {&c.trellis.next_state, &c.trellis.output,
+                                           static_cast<const std::vector<uint32_t>*>(&padded_perm)}) {
+      tables.emplace_back(new DeviceBuffer);
+      tables.back()->upload(*v);
+    }
+    cdev.state_count = int32_t(c.trellis.state_count);
+    cdev.input_count = int32_t(c.trellis.input_count);
+    cdev.input_size = int32_t(c.trellis.input_size);
+    cdev.output_size = int32_t(c.trellis.output_size);
+    cdev.length = int32_t(c.length);
+    cdev.tail = int32_t(c.tail);
+    cdev.termination = c.termination;
+    cdev.msg_size = int32_t(c.msg_size());
+    cdev.syst_size = int32_t(c.syst_size());
+    cdev.syst_tail_size = int32_t(c.syst_tail_size());
+    cdev.parity_size = int32_t(c.parity_size());
+    cdev.next_state = tables[0]->as<uint32_t>();
+    cdev.output = tables[1]->as<uint32_t>();
+    cdev.perm = tables[2]->as<uint32_t>();
   }
 
   void upload_turbo_options() {
@@ -378,7 +408,8 @@ struct fecl_codec_s {
     if (on_device) return;
     init_runtime();
     if (kind == 0) upload_ldpc();
-    else upload_turbo();
+    else if (kind == 1) upload_turbo();
+    else upload_conv();
     on_device = true;
   }
 

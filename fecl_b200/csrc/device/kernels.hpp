@@ -229,6 +229,37 @@ size_t turbo_lte_frame_floats(int K);
 int turbo_lte_batch_max_ctas(int max_K, int algorithm);
 cudaError_t launch_turbo_lte_batch(const TurboLteBatchParams& p, cudaStream_t s);
 
+// ---- convolutional codec (conv.cu, turbo_generic.cu) -----------------------
+
+struct ViterbiRun {
+  int64_t nframes = 0;
+  const void* llr = nullptr;  // [nframes][parity]
+  int32_t llr_dtype = 1;
+  uint8_t* hard = nullptr;    // [nframes][msg]
+  uint8_t* trace = nullptr;   // viterbi_scratch_bytes
+};
+size_t viterbi_scratch_bytes(const TurboDeviceConstituent& k, int64_t nframes);
+cudaError_t launch_viterbi(const TurboDeviceConstituent& k, const ViterbiRun& r, cudaStream_t s);
+cudaError_t launch_conv_encode(const TurboDeviceConstituent& c, const uint8_t* msg, uint8_t* parity, int64_t nframes,
+                               cudaStream_t s);
+
+struct ConvMapRun {
+  int64_t nframes = 0;
+  int32_t algorithm = 2;
+  float sf = 1.0f;
+  const void* llr = nullptr;      // [nframes][parity]
+  const void* syst_in = nullptr;  // [nframes][syst] or null
+  int32_t llr_dtype = 1;
+  void* msg_out = nullptr;        // [nframes][msg]
+  void* syst_out = nullptr;       // [nframes][syst]
+  void* parity_out = nullptr;     // [nframes][parity]
+  int32_t out_dtype = 1;
+  // scratch (filled by the launcher)
+  float *par = nullptr, *pout = nullptr, *sys = nullptr, *app = nullptr, *alpha = nullptr;
+};
+size_t conv_map_scratch_bytes(const TurboDeviceConstituent& k, int64_t nframes);
+cudaError_t launch_conv_map(const TurboDeviceConstituent& k, ConvMapRun r, void* scratch, cudaStream_t s);
+
 // ---- encoders and channel (encode.cu) ---------------------------------------
 
 // The generator pieces of LdpcCode::encode on the device (CSR each).

@@ -62,9 +62,11 @@ __device__ __forceinline__ float gamma_of(const TurboDeviceConstituent& k, const
 
 // One MAP pass of constituent k.  sys: a-priori in, extrinsic out (in place).
 // par: the constituent's parity L-values.  parity_out: optional parity extrinsic.
+// app_out (optional): sf * L of the message steps' input bits (the convolutional
+// codec's msg output, MapDecoderImpl.cpp:197-212).
 template <int ALG>
 __device__ void map_pass(const TurboDeviceConstituent& k, const float* par, float* sys, float* parity_out, float sf,
-                         float* alpha) {
+                         float* alpha, float* app_out = nullptr) {
   const int S = k.state_count, U = k.input_count;
   const int T = k.length + k.tail;
   // forward, MapDecoderImpl.cpp:117-139 (recursive) and :237-274 (LogSum)
@@ -204,6 +206,7 @@ __device__ void map_pass(const TurboDeviceConstituent& k, const float* par, floa
     // extrinsic on the input bits, written over the a-priori of this step
     for (int j = 0; j < k.input_size; ++j) {
       const int idx = t * k.input_size + j;
+      if (app_out && t < k.length) app_out[idx] = sf * lin[j];
       sys[idx] = sf * (lin[j] - sys[idx]);
     }
   }
@@ -334,6 +337,31 @@ __global__ void __launch_bounds__(64) turbo_generic_f32(TurboDeviceCode c, Turbo
   if (p.iters) p.iters[f] = c.iterations;
 }
 
+// The convolutional codec's soDecode (Convolutional::soDecodeBlocks ->
+// MapDecoderImpl::soDecodeBlock, src/detail/MapDecoder/MapDecoderImpl.cpp:56-78,
+// :174-235): one MAP pass over the trellis per frame, one thread per frame.
+template <int ALG>
+__global__ void __launch_bounds__(64) conv_map_f32(TurboDeviceConstituent k, ConvMapRun r) {
+  const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (f >= r.nframes) return;
+  const int P = k.parity_size, Sy = k.syst_size, M = k.msg_size;
+  const int T = k.length + k.tail;
+  float* par = r.par + f * P;
+  float* sys = r.sys + f * Sy;
+  float* pout = r.parity_out ? r.pout + f * P : nullptr;
+  float* app = r.app + f * M;
+  float* alpha = r.alpha + f * int64_t(T) * k.state_count;
+  for (int i = 0; i < P; ++i) par[i] = load_llr(r.llr, r.llr_dtype, f * P + i);
+  for (int i = 0; i < Sy; ++i) sys[i] = r.syst_in ? load_llr(r.syst_in, r.llr_dtype, f * Sy + i) : 0.0f;
+  map_pass<ALG>(k, par, sys, pout, r.sf, alpha, app);
+  if (r.msg_out)
+    for (int i = 0; i < M; ++i) store_llr(r.msg_out, r.out_dtype, f * M + i, app[i]);
+  if (r.syst_out)
+    for (int i = 0; i < Sy; ++i) store_llr(r.syst_out, r.out_dtype, f * Sy + i, sys[i]);
+  if (r.parity_out)
+    for (int i = 0; i < P; ++i) store_llr(r.parity_out, r.out_dtype, f * P + i, pout[i]);
+}
+
 }  // namespace
 
 cudaError_t turbo_generic_init() {
@@ -356,6 +384,35 @@ cudaError_t launch_turbo_generic(const TurboDeviceCode& c, const TurboRun& p, cu
     case kExact: turbo_generic_f32<kExact><<<grid, block, 0, s>>>(c, p); break;
     case kLinear: turbo_generic_f32<kLinear><<<grid, block, 0, s>>>(c, p); break;
     default: turbo_generic_f32<kApproximate><<<grid, block, 0, s>>>(c, p); break;
+  }
+  return cudaGetLastError();
+}
+
+size_t conv_map_scratch_bytes(const TurboDeviceConstituent& k, int64_t nframes) {
+  const int64_t T = k.length + k.tail;
+  return size_t(nframes) * size_t(2 * k.parity_size + k.syst_size + k.msg_size + T * k.state_count) * sizeof(float) + 1024;
+}
+
+cudaError_t launch_conv_map(const TurboDeviceConstituent& k, ConvMapRun r, void* scratch, cudaStream_t s) {
+  cudaError_t e = turbo_generic_init();
+  if (e != cudaSuccess) return e;
+  if (r.nframes <= 0) return cudaSuccess;
+  if (k.state_count > kMaxS || k.input_count > kMaxU) return cudaErrorInvalidValue;
+  float* q = static_cast<float*>(scratch);
+  r.par = q;
+  q += r.nframes * k.parity_size;
+  r.pout = q;
+  q += r.nframes * k.parity_size;
+  r.sys = q;
+  q += r.nframes * k.syst_size;
+  r.app = q;
+  q += r.nframes * k.msg_size;
+  r.alpha = q;
+  const unsigned blocks = unsigned((r.nframes + 63) / 64);
+  switch (r.algorithm) {
+    case kExact: conv_map_f32<kExact><<<blocks, 64, 0, s>>>(k, r); break;
+    case kLinear: conv_map_f32<kLinear><<<blocks, 64, 0, s>>>(k, r); break;
+    default: conv_map_f32<kApproximate><<<blocks, 64, 0, s>>>(k, r); break;
   }
   return cudaGetLastError();
 }

@@ -600,4 +600,44 @@ std::vector<uint32_t> lte_interleaver(uint32_t K) {
   return p;
 }
 
+ConvCode::ConvCode(const Trellis& trellis, uint32_t length, int termination) {
+  if (length == 0) throw std::invalid_argument("Invalid length");
+  if (termination != 0 && termination != 1) throw std::invalid_argument("Invalid termination");
+  c_.trellis = trellis;
+  c_.length = length;
+  c_.termination = termination;
+  c_.tail = termination == 0 ? trellis.state_size : 0;
+  c_.perm.resize(size_t(length) * trellis.input_size);
+  for (size_t i = 0; i < c_.perm.size(); ++i) c_.perm[i] = uint32_t(i);
+}
+
+void ConvCode::set_decoder(const ConvDecoderConfig& cfg) {
+  if (cfg.algorithm < 0 || cfg.algorithm > 2) throw std::invalid_argument("Invalid decoder algorithm");
+  dec_ = cfg;
+}
+
+void ConvCode::encode(const uint8_t* msg, uint8_t* parity) const {
+  std::vector<uint8_t> tail_bits(size_t(c_.tail) * c_.trellis.input_size + 1);
+  c_.encode(msg, parity, tail_bits.data());
+}
+
+bool ConvCode::check(const uint8_t* parity) const {
+  const Trellis& t = c_.trellis;
+  uint32_t state = 0;
+  for (uint32_t j = 0; j < c_.length + c_.tail; ++j, parity += t.output_size) {
+    bool found = false;
+    for (uint32_t u = 0; u < t.input_count && !found; ++u) {
+      const uint32_t out = t.output[state * t.input_count + u];
+      bool equal = true;
+      for (uint32_t k = 0; k < t.output_size && equal; ++k) equal = ((out >> k) & 1) == (parity[k] & 1);
+      if (equal) {
+        found = true;
+        state = t.next_state[state * t.input_count + u];
+      }
+    }
+    if (!found) return false;
+  }
+  return c_.termination == 0 ? state == 0 : true;
+}
+
 }  // namespace fecl

@@ -162,6 +162,40 @@ class TurboCode {
   TurboDecoderConfig dec_;
 };
 
+// ---------------------------------------------------------------- convolutional
+
+struct ConvDecoderConfig {
+  int algorithm = 2;   // Approximate (src/detail/Convolutional.h:60)
+  double scaling = 1.0;
+};
+
+// detail::Convolutional::Structure (src/detail/Convolutional.h:81-125,
+// src/detail/Convolutional.cpp:45-221): one trellis over `length` steps, Truncate
+// (the default) or Tail termination.  The codeword is the trellis output bits only;
+// the tail inputs belong to the systematic part (systSize) but are not transmitted.
+class ConvCode {
+ public:
+  ConvCode(const Trellis& trellis, uint32_t length, int termination);
+
+  uint32_t msg_size() const { return c_.msg_size(); }
+  uint32_t syst_size() const { return c_.syst_size(); }
+  uint32_t parity_size() const { return c_.parity_size(); }
+  uint32_t state_size() const { return 0; }
+  const Constituent& constituent() const { return c_; }
+
+  void set_decoder(const ConvDecoderConfig& cfg);
+  const ConvDecoderConfig& decoder() const { return dec_; }
+
+  // Convolutional::Structure::encode / check (src/detail/Convolutional.cpp:167-221,
+  // and the greedy path search of check).
+  void encode(const uint8_t* msg, uint8_t* parity) const;
+  bool check(const uint8_t* parity) const;
+
+ private:
+  Constituent c_;
+  ConvDecoderConfig dec_;
+};
+
 // Turbo::Lte3Gpp::interleaver -- src/Lte3Gpp.cpp:219-237.
 std::vector<uint32_t> lte_interleaver(uint32_t K);
 bool lte_qpp_params(uint32_t K, uint32_t* f1, uint32_t* f2);

@@ -93,4 +93,17 @@ std::vector<uint32_t> turbo_puncturing(const TurboCode& code, std::vector<std::v
   return seq;
 }
 
+std::vector<uint32_t> conv_puncturing(const ConvCode& code, const std::vector<uint8_t>& mask,
+                                      const std::vector<uint8_t>& tail_mask) {
+  const Constituent& c = code.constituent();
+  const size_t out = c.trellis.output_size;
+  std::vector<uint32_t> seq;
+  size_t at = 0;
+  for (size_t i = 0; i < size_t(c.length) * out; ++i, ++at)
+    if (keep(mask, i)) seq.push_back(uint32_t(at));
+  for (size_t i = 0; i < size_t(c.tail) * out; ++i, ++at)
+    if (tail_mask.empty() ? keep(mask, i) : keep(tail_mask, at)) seq.push_back(uint32_t(at));
+  return seq;
+}
+
 }  // namespace fecl

@@ -23,4 +23,9 @@ std::vector<uint32_t> ldpc_puncturing(const LdpcCode& code, const std::vector<ui
 std::vector<uint32_t> turbo_puncturing(const TurboCode& code, std::vector<std::vector<uint8_t>> mask,
                                        std::vector<std::vector<uint8_t>> tail_mask, int ordering);
 
+// Convolutional::Structure::puncturing, src/detail/Convolutional.cpp:223-242 (the tail
+// bits follow the mask from its start, or the tail mask at their absolute index).
+std::vector<uint32_t> conv_puncturing(const ConvCode& code, const std::vector<uint8_t>& mask,
+                                      const std::vector<uint8_t>& tail_mask);
+
 }  // namespace fecl

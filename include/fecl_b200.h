@@ -172,6 +172,25 @@ int fecl_lte_interleaver(uint32_t K, uint32_t* perm);
 /* Turbo::setDecoderOptions -- src/Turbo.h:105. */
 int fecl_turbo_set_options(fecl_codec_t codec, const fecl_turbo_options* options);
 
+/* ---- Convolutional ----------------------------------------------------------- */
+
+/* Convolutional::DecoderOptions -- src/detail/Convolutional.h:48-62. */
+typedef struct {
+  int32_t algorithm; /* soDecode's MAP algorithm (default FECL_APPROXIMATE); decode is Viterbi */
+  double scaling;    /* scaling factor of the soft outputs (default 1.0) */
+} fecl_conv_options;
+
+/* fec::Convolutional(EncoderOptions(trellis, length).termination(t), DecoderOptions)
+ * -- src/Convolutional.h:51, src/detail/Convolutional.cpp:45-66.  The reference's
+ * default termination is FECL_TRUNCATE.  decode runs Viterbi
+ * (src/detail/ViterbiDecoder/ViterbiDecoderImpl.cpp), soDecode the MAP decoder. */
+int fecl_conv_create(const fecl_trellis* trellis, uint32_t length, int32_t termination, const fecl_conv_options* options,
+                     fecl_codec_t* out);
+int fecl_conv_set_options(fecl_codec_t codec, const fecl_conv_options* options);
+/* Convolutional::puncturing (src/Convolutional.h:73, src/detail/Convolutional.cpp:223-242). */
+int fecl_conv_puncturing(fecl_codec_t codec, const uint8_t* mask, uint32_t mask_len, const uint8_t* tail_mask,
+                         uint32_t tail_mask_len, uint32_t* seq, uint64_t* seq_len);
+
 /* ---- every codec ----------------------------------------------------------- */
 
 int fecl_codec_sizes(fecl_codec_t codec, fecl_sizes* sizes);

@@ -140,6 +140,27 @@ class RefCodec:
                                      _p(sf), C.c_size_t(rows_), C.c_size_t(cols_), C.c_int(workgroup), C.byref(h)))
         return cls(h.value)
 
+    @classmethod
+    def conv(cls, trellis_spec, length, termination, algorithm=2, scaling=1.0, workgroup=1):
+        keep = []
+        t = _trellis_struct(trellis_spec, keep)
+        h = C.c_void_p()
+        _chk(lib().fref_conv_create(C.byref(t), C.c_size_t(length), C.c_int(termination), C.c_int(algorithm),
+                                    C.c_double(scaling), C.c_int(workgroup), C.byref(h)))
+        return cls(h.value)
+
+    def conv_puncturing(self, mask=(), tail_mask=()):
+        """Convolutional::Structure::puncturing: (sequence, input size)."""
+        m = np.asarray(list(mask) or [0], np.uint8)
+        t = np.asarray(list(tail_mask) or [0], np.uint8)
+        n, ins = C.c_size_t(), C.c_size_t()
+        L = lib()
+        args = (self.h, _p(m), C.c_size_t(len(mask)), _p(t), C.c_size_t(len(tail_mask)))
+        _chk(L.fref_conv_puncturing(*args, None, C.byref(n), C.byref(ins)))
+        seq = np.zeros(max(n.value, 1), np.uint32)
+        _chk(L.fref_conv_puncturing(*args, _p(seq), C.byref(n), C.byref(ins)))
+        return seq[: n.value], ins.value
+
     def set_workgroup(self, n):
         _chk(lib().fref_codec_set_workgroup(self.h, C.c_int(n)))
 

@@ -20,6 +20,7 @@
 #include <string>
 #include <vector>
 
+#include "Convolutional.h"
 #include "Ldpc.h"
 #include "Turbo.h"
 #include "Trellis.h"
@@ -32,6 +33,7 @@ struct RefCodec {
   std::unique_ptr<fec::Codec> codec;
   std::unique_ptr<fec::detail::Ldpc::Structure> ldpc;    // set for LDPC codecs
   std::unique_ptr<fec::detail::Turbo::Structure> turbo;  // set for turbo codecs
+  std::unique_ptr<fec::detail::Convolutional::Structure> conv;  // set for convolutional codecs
 };
 
 template <class F>
@@ -262,6 +264,36 @@ int fref_turbo_puncturing(void* h, const uint8_t* mask_data, const size_t* mask_
     fec::Turbo::PunctureOptions o;
     o.mask(m).tailMask(t).bitOrdering(ordering == 0 ? fec::Turbo::BitOrdering::Alternate : fec::Turbo::BitOrdering::Group);
     const fec::Permutation p = rc->turbo->puncturing(o);
+    *seq_len = p.outputSize();
+    *input_size = p.inputSize();
+    if (seq)
+      for (size_t i = 0; i < p.outputSize(); ++i) seq[i] = uint32_t(p[i]);
+  });
+}
+
+// fec::Convolutional(EncoderOptions(trellis, length).termination(t),
+// DecoderOptions().algorithm(a).scalingFactor(sf)) -- src/Convolutional.h:51.
+int fref_conv_create(const fref_trellis* trellis, size_t length, int termination, int algorithm, double scaling,
+                     int workgroup, void** out) {
+  return guarded([&] {
+    auto enc = fec::Convolutional::EncoderOptions(make_trellis(*trellis), length)
+                   .termination(termination == 0 ? fec::Trellis::Tail : fec::Trellis::Truncate);
+    auto dec = fec::Convolutional::DecoderOptions().algorithm(to_alg(algorithm)).scalingFactor(scaling);
+    auto rc = new RefCodec;
+    rc->conv.reset(new fec::detail::Convolutional::Structure(enc, dec));
+    rc->codec.reset(new fec::Convolutional(*rc->conv, workgroup));
+    *out = rc;
+  });
+}
+
+// Convolutional::Structure::puncturing (src/detail/Convolutional.cpp:223-242).
+int fref_conv_puncturing(void* h, const uint8_t* mask, size_t mask_len, const uint8_t* tail_mask, size_t tail_len,
+                         uint32_t* seq, size_t* seq_len, size_t* input_size) {
+  return guarded([&] {
+    auto rc = static_cast<RefCodec*>(h);
+    fec::Convolutional::PunctureOptions o;
+    o.mask(std::vector<bool>(mask, mask + mask_len)).tailMask(std::vector<bool>(tail_mask, tail_mask + tail_len));
+    const fec::Permutation p = rc->conv->puncturing(o);
     *seq_len = p.outputSize();
     *input_size = p.inputSize();
     if (seq)
