@@ -606,6 +606,14 @@ class Turbo(Codec):
 
     Alternate, Group = 0, 1  # Turbo::BitOrdering, src/detail/Turbo.h:54-57
 
+    class Stage:
+        """Turbo::Stage -- src/detail/Turbo.h:38-48: constituents decoded in the stage and,
+        for each, the constituents whose extrinsic values form its a-priori input."""
+
+        def __init__(self, activation, transfer):
+            self.activation = [int(a) for a in activation]
+            self.transfer = [[int(t) for t in lst] for lst in transfer]
+
     class PunctureOptions:
         """Turbo::PunctureOptions -- src/detail/Turbo.h: mask (one repeating mask per
         stream: systematic, then each constituent's parity), tailMask (two per
@@ -646,10 +654,19 @@ class Turbo(Codec):
             return self
 
         def scheduling(self, s=None):
+            """Serial, Parallel, or a custom schedule: a list of Turbo.Stage (then the
+            scheduling type is Custom, as DecoderOptions::scheduling(Scheduling) sets it)."""
             if s is None:
                 return self._sched
-            self._sched = int(s)
+            if isinstance(s, (list, tuple)):
+                self._stages = [st if isinstance(st, Turbo.Stage) else Turbo.Stage(*st) for st in s]
+                self._sched = Custom
+            else:
+                self._sched = int(s)
             return self
+
+        def schedule(self):
+            return list(getattr(self, "_stages", []))
 
         def algorithm(self, a=None):
             if a is None:
@@ -693,8 +710,14 @@ class Turbo(Codec):
         return cls(None, decoder, lte_length=K)
 
     def _options(self, d):
-        sf = np.ascontiguousarray(np.asarray(d.scalingFactor(), dtype=np.float64))
-        if sf.ndim != 2:
+        rows = [list(np.atleast_1d(np.asarray(r, dtype=np.float64))) for r in d.scalingFactor()]
+        width = max((len(r) for r in rows), default=0)
+        # rows of 1 entry cycle like rows of `iterations` entries (src/detail/Turbo.cpp:148-153):
+        # widen them so that the table is rectangular
+        if any(len(r) not in (1, width) for r in rows):
+            raise ValueError("Wrong size for scaling factor")
+        sf = np.ascontiguousarray(np.asarray([r * width if len(r) == 1 else r for r in rows], dtype=np.float64))
+        if sf.ndim != 2 or sf.size == 0:
             raise ValueError("Wrong size for scaling factor")
         o = _lib.fecl_turbo_options()
         o.algorithm = d.algorithm()
@@ -704,6 +727,19 @@ class Turbo(Codec):
         o.scaling_rows, o.scaling_cols = sf.shape
         o.precision = d.precision()
         self._sf_table = sf
+        stages = d.schedule() if d.scheduling() == Custom else []
+        for st in stages:  # src/detail/Turbo.cpp:109-111 (the C-ABI pairs one transfer list with each activation)
+            if len(st.activation) != len(st.transfer):
+                raise ValueError("Invalid scheduling : activation and transfer not the same size")
+        if stages:
+            counts = _u32([len(st.activation) for st in stages])
+            act = _u32([a for st in stages for a in st.activation] or [0])
+            tcounts = _u32([len(t) for st in stages for t in st.transfer] or [0])
+            tr = _u32([v for st in stages for t in st.transfer for v in t] or [0])
+            self._sched_arrays = (counts, act, tcounts, tr)
+            o.n_stages = len(stages)
+            o.stage_counts, o.activation = counts.ctypes.data, act.ctypes.data
+            o.transfer_counts, o.transfer = tcounts.ctypes.data, tr.ctypes.data
         return o, sf
 
     def setDecoderOptions(self, decoder):

@@ -51,6 +51,11 @@ class fecl_turbo_options(C.Structure):
         ("scaling_rows", C.c_uint32),
         ("scaling_cols", C.c_uint32),
         ("precision", C.c_int32),
+        ("n_stages", C.c_uint32),
+        ("stage_counts", C.c_void_p),
+        ("activation", C.c_void_p),
+        ("transfer_counts", C.c_void_p),
+        ("transfer", C.c_void_p),
     ]
 
 

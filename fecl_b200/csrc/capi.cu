@@ -77,6 +77,21 @@ fecl::TurboDecoderConfig turbo_config(const fecl_turbo_options* o) {
   cfg.algorithm = o->algorithm;
   cfg.iterations = o->iterations;
   cfg.scheduling = o->scheduling;
+  if (o->scheduling == FECL_CUSTOM) {
+    if (o->n_stages && (!o->stage_counts || !o->activation || !o->transfer_counts)) fail(FECL_EINVAL, "null schedule");
+    size_t a = 0, t = 0;
+    for (uint32_t st = 0; st < o->n_stages; ++st) {
+      fecl::TurboStage stage;
+      for (uint32_t k = 0; k < o->stage_counts[st]; ++k, ++a) {
+        stage.activation.push_back(o->activation[a]);
+        const uint32_t n = o->transfer_counts[a];
+        if (n && !o->transfer) fail(FECL_EINVAL, "null schedule");
+        stage.transfer.emplace_back(o->transfer + t, o->transfer + t + n);
+        t += n;
+      }
+      cfg.schedule.push_back(std::move(stage));
+    }
+  }
   cfg.precision = o->precision;
   if (o->scaling) {
     if (o->scaling_rows == 0 || o->scaling_cols == 0) fail(FECL_EINVAL, "Wrong size for scaling factor");

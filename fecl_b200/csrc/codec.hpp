@@ -122,6 +122,7 @@ struct fecl_codec_s {
   DeviceBuffer row_ptr, col_idx, col_ptr, col_edges, sf;
   std::vector<std::unique_ptr<DeviceBuffer>> tables;
   fecl::LdpcDeviceCode ldev;
+  DeviceBuffer sched[4];  // custom turbo schedule (stage_ptr, act_con, act_tptr, transfer)
   DeviceBuffer enc[8];  // LDPC generator pieces (DC, A, B, T as CSR) for the device encoder
   fecl::LdpcEncodeTables ltab;
   fecl::TurboDeviceCode tdev;
@@ -299,6 +300,24 @@ struct fecl_codec_s {
     tdev.algorithm = d.algorithm;
     tdev.iterations = int32_t(d.iterations);
     tdev.scheduling = d.scheduling;
+    std::vector<int32_t> sp{0}, ac, ap{0}, tr;
+    for (const auto& st : d.schedule) {
+      for (size_t k = 0; k < st.activation.size(); ++k) {
+        ac.push_back(int32_t(st.activation[k]));
+        for (auto v : st.transfer[k]) tr.push_back(int32_t(v));
+        ap.push_back(int32_t(tr.size()));
+      }
+      sp.push_back(int32_t(ac.size()));
+    }
+    sched[0].upload(sp);
+    sched[1].upload(ac);
+    sched[2].upload(ap);
+    sched[3].upload(tr);
+    tdev.n_stages = int32_t(d.schedule.size());
+    tdev.stage_ptr = sched[0].as<int32_t>();
+    tdev.act_con = sched[1].as<int32_t>();
+    tdev.act_tptr = sched[2].as<int32_t>();
+    tdev.transfer = sched[3].as<int32_t>();
   }
 
   bool on_device = false;

@@ -154,6 +154,14 @@ struct TurboDeviceCode {
   TurboDeviceConstituent c[kMaxConstituents];
   const float* sf = nullptr;  // [n][iterations] resolved scaling
   int32_t algorithm = 1, iterations = 6, scheduling = 0;
+  // Custom scheduling: stage s holds activations [stage_ptr[s], stage_ptr[s+1]);
+  // activation a decodes constituent act_con[a] with a-priori input from the
+  // constituents transfer[act_tptr[a] .. act_tptr[a+1]) (each list sorted).
+  int32_t n_stages = 0;
+  const int32_t* stage_ptr = nullptr;
+  const int32_t* act_con = nullptr;
+  const int32_t* act_tptr = nullptr;
+  const int32_t* transfer = nullptr;
 };
 
 struct TurboRun {

@@ -266,6 +266,66 @@ __device__ void parallel_transfer(const TurboDeviceCode& c, Frame& fr) {
   }
 }
 
+// Membership in a sorted constituent list [lo, hi), advanced monotonically like the
+// reference's iterator walks.
+__device__ __forceinline__ bool take(const int32_t* list, int& at, int hi, int j) {
+  while (at < hi && list[at] < j) ++at;
+  return at < hi && list[at] == j;
+}
+
+// TurboDecoderImpl::customTransferUpdate, TurboDecoderImpl.cpp:252-289: the a-priori
+// input of activation a (constituent i) is the channel systematic plus the
+// de-interleaved extrinsic values of the listed constituents, interleaved into the
+// buffer's slot of constituent i; the systematic tail is copied into the live
+// extrinsic array (as the reference does), not into the buffer.
+__device__ void custom_transfer(const TurboDeviceCode& c, Frame& fr, int a) {
+  const int i = c.act_con[a];
+  const int t_hi = c.act_tptr[a + 1];
+  int at = c.act_tptr[a];
+  float* syst = fr.pout;
+  for (int k = 0; k < c.msg; ++k) syst[k] = fr.pin[k];
+  const float* ext = fr.ext;
+  float* tmp = fr.extb;
+  const float* systTail = fr.pin + c.msg;
+  for (int j = 0; j < i; ++j) {
+    if (take(c.transfer, at, t_hi, j))
+      for (int k = 0; k < c.c[j].msg_size; ++k) syst[c.c[j].perm[k]] += ext[k];
+    ext += c.c[j].syst_size;
+    tmp += c.c[j].syst_size;
+    systTail += c.c[j].syst_tail_size;
+  }
+  float* slot = tmp;
+  float* tail_dst = fr.ext + (ext - fr.ext) + c.c[i].msg_size;
+  for (int k = 0; k < c.c[i].syst_tail_size; ++k) tail_dst[k] = systTail[k];
+  ext += c.c[i].syst_size;
+  for (int j = i + 1; j < c.n; ++j) {
+    if (take(c.transfer, at, t_hi, j)) {
+      for (int k = 0; k < c.c[j].msg_size; ++k) syst[c.c[j].perm[k]] += ext[k];
+    } else if (at >= t_hi) {
+      break;
+    }
+    ext += c.c[j].syst_size;
+  }
+  for (int k = 0; k < c.c[i].msg_size; ++k) slot[k] = syst[c.c[i].perm[k]];
+}
+
+// TurboDecoderImpl::customActivationUpdate, TurboDecoderImpl.cpp:170-189: the stage's
+// constituents, in increasing order, each with the scaling of (iteration, constituent)
+// -- in decode and soDecode alike.
+template <int ALG>
+__device__ void custom_activation(const TurboDeviceCode& c, Frame& fr, int it, int stage) {
+  const int hi = c.stage_ptr[stage + 1];
+  int at = c.stage_ptr[stage];
+  const float* par = fr.pin + c.syst;
+  float* ext = fr.ext;
+  for (int j = 0; j < c.n; ++j) {
+    if (take(c.act_con, at, hi, j)) map_pass<ALG>(c.c[j], par, ext, nullptr, c.sf[j * c.iterations + it], fr.alpha);
+    else if (at >= hi) break;
+    ext += c.c[j].syst_size;
+    par += c.c[j].parity_size;
+  }
+}
+
 __device__ void aposteriori(const TurboDeviceCode& c, Frame& fr) {
   // TurboDecoderImpl::aPosterioriUpdate, TurboDecoderImpl.cpp:152-168
   const float* ext = fr.ext;
@@ -303,6 +363,17 @@ __global__ void __launch_bounds__(64) turbo_generic_f32(TurboDeviceCode c, Turbo
     for (int k = c.syst; k < c.parity; ++k) fr.pout[k] = 0.0f;
 
   for (int i = 0; i < c.iterations; ++i) {
+    if (c.scheduling == 2) {
+      for (int st = 0; st < c.n_stages; ++st) {
+        for (int k = 0; k < c.state; ++k) fr.extb[k] = fr.ext[k];
+        for (int a = c.stage_ptr[st]; a < c.stage_ptr[st + 1]; ++a) custom_transfer(c, fr, a);
+        float* t = fr.ext;
+        fr.ext = fr.extb;
+        fr.extb = t;
+        custom_activation<ALG>(c, fr, i, st);
+      }
+      continue;
+    }
     if (c.scheduling == 1) parallel_transfer(c, fr);
     const float* par = fr.pin + c.syst;
     float* pout = fr.pout + c.syst;

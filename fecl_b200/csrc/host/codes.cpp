@@ -514,8 +514,27 @@ TurboCode::TurboCode(const std::vector<Trellis>& trellis, const std::vector<std:
 
 void TurboCode::set_decoder(const TurboDecoderConfig& cfg) {
   if (cfg.algorithm < 0 || cfg.algorithm > 2) throw std::invalid_argument("Invalid decoder algorithm");
-  if (cfg.scheduling == 2) throw std::invalid_argument("Custom scheduling is not supported by the device decoder");
   if (cfg.scheduling < 0 || cfg.scheduling > 2) throw std::invalid_argument("Invalid scheduling");
+  TurboDecoderConfig c = cfg;
+  if (c.scheduling == 2) {
+    // src/detail/Turbo.cpp:106-124: activation and transfer lists of equal size, each
+    // list sorted; a transfer list stays paired with the activation at its index after
+    // the activation list is sorted.  Constituent ids must name a constituent (the
+    // reference accepts an id equal to the count, which it then reads out of range).
+    for (auto& st : c.schedule) {
+      if (st.activation.size() != st.transfer.size())
+        throw std::invalid_argument("Invalid scheduling : activation and transfer not the same size");
+      std::sort(st.activation.begin(), st.activation.end());
+      for (size_t j = 0; j < st.activation.size(); ++j) {
+        if (st.activation[j] >= c_.size()) throw std::invalid_argument("Invalid scheduling : activation of an invalid constituent");
+        for (auto t : st.transfer[j])
+          if (t >= c_.size()) throw std::invalid_argument("Invalid scheduling : transfer from an invalid constituent");
+        std::sort(st.transfer[j].begin(), st.transfer[j].end());
+      }
+    }
+  } else {
+    c.schedule.clear();
+  }
   if (cfg.precision < 0 || cfg.precision > 1) throw std::invalid_argument("Invalid message precision");
   // src/detail/Turbo.cpp:127-135
   if (cfg.scaling.size() == c_.size()) {
@@ -526,7 +545,7 @@ void TurboCode::set_decoder(const TurboDecoderConfig& cfg) {
   }
   for (auto& r : cfg.scaling)
     if (r.empty()) throw std::invalid_argument("Wrong size for scaling factor");
-  dec_ = cfg;
+  dec_ = c;
 }
 
 double TurboCode::scaling_factor(size_t i, size_t j) const {

@@ -121,12 +121,21 @@ struct Constituent {
   void encode(const uint8_t* msg, uint8_t* parity, uint8_t* tail_bits) const;
 };
 
+// A stage of a custom schedule (detail::Turbo::Stage, src/detail/Turbo.h:38-48): the
+// constituents decoded in the stage, and for the k-th of them (after sorting) the
+// constituents whose extrinsic values form its a-priori input.
+struct TurboStage {
+  std::vector<uint32_t> activation;
+  std::vector<std::vector<uint32_t>> transfer;
+};
+
 struct TurboDecoderConfig {
   int algorithm = 1;  // Linear (src/detail/Turbo.h:99)
   uint32_t iterations = 6;
   int scheduling = 0;  // Serial
   std::vector<std::vector<double>> scaling{{1.0}};  // [constituent][iteration]
   int precision = 0;
+  std::vector<TurboStage> schedule;  // scheduling == Custom
 };
 
 class TurboCode {

@@ -146,13 +146,22 @@ int fecl_trellis_build(uint32_t ninputs, const uint32_t* constraint_lengths, uin
 typedef struct {
   int32_t algorithm;   /* default FECL_LINEAR in the reference */
   uint32_t iterations; /* default 6 */
-  int32_t scheduling;  /* FECL_SERIAL / FECL_PARALLEL */
+  int32_t scheduling;  /* FECL_SERIAL / FECL_PARALLEL / FECL_CUSTOM (with the schedule below) */
   /* scaling[row][col], rows = 1 or constituent count, cols = 1 or iterations
    * (Turbo::Structure::scalingFactor, src/detail/Turbo.cpp:148-153). NULL = 1.0. */
   const double* scaling;
   uint32_t scaling_rows;
   uint32_t scaling_cols;
   int32_t precision; /* FECL_MSG_F32 (reference parity) / FECL_MSG_F16 */
+  /* FECL_CUSTOM: a Turbo::Scheduling (src/detail/Turbo.h:38-48, DecoderOptions::scheduling):
+   * n_stages stages; stage s activates stage_counts[s] constituents (ids concatenated in
+   * `activation`); activation a takes its a-priori input from transfer_counts[a]
+   * constituents (ids concatenated in `transfer`). */
+  uint32_t n_stages;
+  const uint32_t* stage_counts;
+  const uint32_t* activation;
+  const uint32_t* transfer_counts;
+  const uint32_t* transfer;
 } fecl_turbo_options;
 
 /* fec::Turbo(EncoderOptions(trellis, interleavers).termination(t), DecoderOptions)

@@ -161,6 +161,20 @@ class RefCodec:
         _chk(L.fref_conv_puncturing(*args, _p(seq), C.byref(n), C.byref(ins)))
         return seq[: n.value], ins.value
 
+    def set_turbo_schedule(self, stages, algorithm, iterations, scaling=None):
+        """A custom schedule: stages = [(activation, [transfer, ...]), ...]."""
+        counts = np.asarray([len(a) for a, _ in stages] or [0], np.uint32)
+        act = np.asarray([x for a, _ in stages for x in a] or [0], np.uint32)
+        tc = np.asarray([len(t) for _, tr in stages for t in tr] or [0], np.uint32)
+        tr = np.asarray([x for _, trs in stages for t in trs for x in t] or [0], np.uint32)
+        if scaling is None:
+            sf, r, c = np.zeros(1, np.float64), 0, 0
+        else:
+            sf = np.ascontiguousarray(scaling, np.float64)
+            r, c = sf.shape
+        _chk(lib().fref_turbo_set_schedule(self.h, C.c_int(algorithm), C.c_size_t(iterations), _p(sf), C.c_size_t(r),
+                                           C.c_size_t(c), C.c_size_t(len(stages)), _p(counts), _p(act), _p(tc), _p(tr)))
+
     def set_workgroup(self, n):
         _chk(lib().fref_codec_set_workgroup(self.h, C.c_int(n)))
 

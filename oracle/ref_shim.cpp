@@ -301,6 +301,33 @@ int fref_conv_puncturing(void* h, const uint8_t* mask, size_t mask_len, const ui
   });
 }
 
+// Sets a custom schedule (Turbo::DecoderOptions::scheduling(Scheduling), which also
+// selects Custom scheduling) on a turbo codec made by fref_turbo_create; the layout
+// of the arrays is fecl_turbo_options'.
+int fref_turbo_set_schedule(void* h, int algorithm, size_t iterations, const double* scaling, size_t nscaling_rows,
+                            size_t nscaling_cols, size_t n_stages, const uint32_t* stage_counts, const uint32_t* activation,
+                            const uint32_t* transfer_counts, const uint32_t* transfer) {
+  return guarded([&] {
+    auto rc = static_cast<RefCodec*>(h);
+    fec::Turbo::Scheduling sched(n_stages);
+    size_t a = 0, t = 0;
+    for (size_t s = 0; s < n_stages; ++s)
+      for (uint32_t k = 0; k < stage_counts[s]; ++k, ++a) {
+        sched[s].activation.push_back(activation[a]);
+        sched[s].transfer.emplace_back(transfer + t, transfer + t + transfer_counts[a]);
+        t += transfer_counts[a];
+      }
+    auto dec = fec::Turbo::DecoderOptions().algorithm(to_alg(algorithm)).iterations(iterations).scheduling(sched);
+    if (nscaling_rows > 0) {
+      std::vector<std::vector<double>> sf(nscaling_rows);
+      for (size_t i = 0; i < nscaling_rows; ++i)
+        sf[i].assign(scaling + i * nscaling_cols, scaling + (i + 1) * nscaling_cols);
+      dec.scalingFactor(sf);
+    }
+    static_cast<fec::Turbo*>(rc->codec.get())->setDecoderOptions(dec);
+  });
+}
+
 void fref_codec_destroy(void* h) { delete static_cast<RefCodec*>(h); }
 
 int fref_codec_sizes(void* h, size_t* out4) {

@@ -82,8 +82,13 @@ def test_invalid_options_raise():
     with pytest.raises(ValueError):
         F.Turbo.lte(40, F.Turbo.DecoderOptions().iterations(4).scalingFactor([[1.0, 0.5], [0.5, 1.0]]))
     F.Turbo.lte(40, F.Turbo.DecoderOptions().iterations(4).scalingFactor([[1.0, 0.5]]))  # accepted, cycled
+    # src/detail/Turbo.cpp:106-124: custom schedules need one transfer list per
+    # activation and valid constituent ids
     with pytest.raises(ValueError):
-        F.Turbo.lte(40, F.Turbo.DecoderOptions().scheduling(F.Custom))
+        F.Turbo.lte(40, F.Turbo.DecoderOptions().scheduling([F.Turbo.Stage([0, 1], [[1]])]))
+    with pytest.raises(ValueError):
+        F.Turbo.lte(40, F.Turbo.DecoderOptions().scheduling([F.Turbo.Stage([2], [[0]])]))
+    F.Turbo.lte(40, F.Turbo.DecoderOptions().scheduling([F.Turbo.Stage([1, 0], [[0], [1]])]))
     t = F.Turbo.lte(40)
     with pytest.raises(ValueError):
         t.setWindowTraining(12)

@@ -196,3 +196,39 @@ def test_device_memory_decode_matches_host():
     b = code.decode(torch.from_numpy(llr).cuda()).cpu().numpy()
     c = code.decode(torch.from_numpy(llr).pin_memory()).numpy()
     assert np.array_equal(a, b) and np.array_equal(a, c)
+
+
+CUSTOM_SCHEDULES = [
+    [([0, 1, 2], [[1, 2], [0, 2], [0, 1]])],                       # all constituents at once (like Parallel)
+    [([0], [[1, 2]]), ([2, 1], [[0, 1], [0, 2]])],                 # two stages, activation given out of order
+    [([1], [[0]]), ([0], [[1]]), ([2], [[0, 1]])],                 # one constituent per stage, partial transfers
+]
+
+
+@pytest.mark.parametrize("stages", CUSTOM_SCHEDULES)
+@pytest.mark.parametrize("alg", [2, 0])
+def test_custom_scheduling_matches_reference(stages, alg):
+    """Turbo::DecoderOptions::scheduling(Scheduling) (TurboDecoderImpl.cpp:170-189,
+    252-289) on the reference suite's three-constituent code, against the compiled
+    reference: decode hard decisions and soDecode soft outputs."""
+    import fecl_b200 as F
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference library not built")
+    perms = [ARRAYS["perm_1024"], ARRAYS["perm_512"], ARRAYS["perm_even_512"]]
+    sf = [[0.7, 0.8, 0.9, 1.0], [0.75], [0.9]]
+    dec = F.Turbo.DecoderOptions().algorithm(alg).iterations(4).scheduling([F.Turbo.Stage(a, t) for a, t in stages])
+    dec.scalingFactor(sf)
+    code = F.Turbo(F.Turbo.EncoderOptions([F.Trellis(*s) for s in SUITE3], perms).termination(0), dec)
+    rc = ref.RefCodec.turbo(SUITE3, perms, 0, alg, 0, 4)
+    rc.set_turbo_schedule(stages, alg, 4, np.asarray([[0.7, 0.8, 0.9, 1.0], [0.75] * 4, [0.9] * 4]))
+    msg = np.random.default_rng(90).integers(0, 2, 6 * code.msgSize()).astype(np.uint8)
+    llr = distort(code.encode(msg), -1.0, 91).astype(np.float32).astype(np.float64)
+    want = rc.decode(llr)
+    out = rc.so_decode(llr, outputs=("msg", "syst", "parity", "state"))
+    assert_hard_parity(code.decode(llr), want, msg, code.msgSize(), ref_app=out["msg"])
+    got = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output().msg().syst().parity().state())
+    ok = frame_ok((out["msg"] > 0).astype(np.uint8), msg, code.msgSize())
+    for k, size in (("msg", code.msgSize()), ("syst", code.systSize()), ("parity", code.paritySize()),
+                    ("state", code.stateSize())):
+        assert_soft_parity(getattr(got, k)(), out[k], ok, size, what=k, exact=alg == 0)
