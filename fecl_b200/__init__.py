@@ -25,13 +25,43 @@ from ._lib import check as _check
 from ._lib import lib as _L
 
 __all__ = [
-    "Exact", "Linear", "Approximate", "Serial", "Parallel", "Custom",
+    "Exact", "Linear", "Approximate", "Serial", "Parallel", "Custom", "CRC24A", "CRC24B", "crc24_attach", "crc24_check",
     "SparseBitMatrix", "Trellis", "Codec", "Ldpc", "Turbo", "Convolutional", "Batch", "Server", "Permutation", "FeclError", "lib_path",
 ]
 
 # DecoderAlgorithm (src/DecoderAlgorithm.h:30-34) and SchedulingType (src/SchedulingType.h:32-39)
 Exact, Linear, Approximate = 0, 1, 2
 Serial, Parallel, Custom = 0, 1, 2
+# CRC polynomials of 3GPP TS 36.212 section 5.1.1 (an extension)
+CRC24A, CRC24B = 1, 2
+
+
+def crc24_attach(bits, kind, nframes=1):
+    """Extension: appends to each of `nframes` frames of the torch CUDA uint8 tensor
+    `bits` its 24 CRC bits (fecl_crc24_attach); returns a CUDA tensor."""
+    import torch
+    b = bits.contiguous().view(-1)
+    n = int(nframes)
+    if n <= 0 or b.numel() % n:
+        raise ValueError("Invalid size for message")
+    L = b.numel() // n
+    out = torch.empty(n * (L + 24), dtype=torch.uint8, device=b.device)
+    _check(_L.fecl_crc24_attach(C.c_void_p(b.data_ptr()), L, n, int(kind), C.c_void_p(out.data_ptr()),
+                                C.c_void_p(torch.cuda.current_stream(b.device).cuda_stream)))
+    return out
+
+
+def crc24_check(bits, kind, nframes=1):
+    """Extension: per frame, whether its bits (CRC included) pass (fecl_crc24_check)."""
+    import torch
+    b = bits.contiguous().view(-1)
+    n = int(nframes)
+    if n <= 0 or b.numel() % n:
+        raise ValueError("Invalid size")
+    ok = torch.empty(n, dtype=torch.int32, device=b.device)
+    _check(_L.fecl_crc24_check(C.c_void_p(b.data_ptr()), b.numel() // n, n, int(kind), C.c_void_p(ok.data_ptr()),
+                               C.c_void_p(torch.cuda.current_stream(b.device).cuda_stream)))
+    return ok.bool()
 FeclError = _lib.FeclError
 lib_path = _lib.LIB_PATH
 
@@ -668,6 +698,14 @@ class Turbo(Codec):
         def schedule(self):
             return list(getattr(self, "_stages", []))
 
+        def crc(self, kind=None):
+            """Extension: CRC24A / CRC24B when the message ends with that CRC of the rest;
+            decode then stops each frame at the first iteration whose decisions pass it."""
+            if kind is None:
+                return getattr(self, "_crc", 0)
+            self._crc = int(kind)
+            return self
+
         def algorithm(self, a=None):
             if a is None:
                 return self._alg
@@ -727,6 +765,7 @@ class Turbo(Codec):
         o.scaling_rows, o.scaling_cols = sf.shape
         o.precision = d.precision()
         self._sf_table = sf
+        o.crc = d.crc()
         stages = d.schedule() if d.scheduling() == Custom else []
         for st in stages:  # src/detail/Turbo.cpp:109-111 (the C-ABI pairs one transfer list with each activation)
             if len(st.activation) != len(st.transfer):

@@ -56,6 +56,7 @@ class fecl_turbo_options(C.Structure):
         ("activation", C.c_void_p),
         ("transfer_counts", C.c_void_p),
         ("transfer", C.c_void_p),
+        ("crc", C.c_int32),
     ]
 
 
@@ -127,6 +128,8 @@ SIGNATURES = [
     ("fecl_decode", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     ("fecl_so_decode", C.c_int, [C.c_void_p, C.POINTER(fecl_so_io), C.c_uint64, C.c_int32, C.c_void_p]),
     ("fecl_destroy", None, [C.c_void_p]),
+    ("fecl_crc24_attach", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_int32, C.c_void_p, C.c_void_p]),
+    ("fecl_crc24_check", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_int32, C.c_void_p, C.c_void_p]),
     ("fecl_ldpc_puncturing", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                        C.POINTER(C.c_uint64)]),
     ("fecl_turbo_puncturing", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,

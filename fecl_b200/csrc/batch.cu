@@ -270,6 +270,7 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
         d.iters = s.job->iterations ? s.job->iterations + f : nullptr;
         d.perm = s.c->tdev.c[1].perm;
         d.sf = s.c->tdev.sf;
+        d.crc = s.c->crc_table();
         d.K = K;
         d.iterations = s.c->tdev.iterations;
         d.llr_dtype = s.job->llr_dtype;

@@ -77,6 +77,7 @@ fecl::TurboDecoderConfig turbo_config(const fecl_turbo_options* o) {
   cfg.algorithm = o->algorithm;
   cfg.iterations = o->iterations;
   cfg.scheduling = o->scheduling;
+  cfg.crc = o->crc;
   if (o->scheduling == FECL_CUSTOM) {
     if (o->n_stages && (!o->stage_counts || !o->activation || !o->transfer_counts)) fail(FECL_EINVAL, "null schedule");
     size_t a = 0, t = 0;
@@ -343,8 +344,10 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
       cuda_check(cudaMemset(c->stats.ptr, 0, 3 * sizeof(unsigned long long)), "cudaMemset");
     }
     r.stats = c->stats.as<unsigned long long>();
+    r.crc = c->crc_table();
     e = fecl::launch_turbo_lte(r, s);
   } else {
+    if (!soft && c->turbo->decoder().crc) fail(FECL_EUNSUPPORTED, "CRC stop needs the LTE turbo code with serial scheduling");
     fecl::TurboRun r;
     r.nframes = int64_t(n);
     r.soft = soft ? 1 : 0;
@@ -776,6 +779,26 @@ int fecl_so_decode(fecl_codec_t codec, const fecl_so_io* io, uint64_t nframes, i
     std::lock_guard<std::mutex> lk(c->mu);
     if (nframes == 0) return;
     run_decode(c, io, nframes, nullptr, nullptr, true, flags, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fecl_crc24_attach(const uint8_t* bits, uint64_t len, uint64_t nframes, int32_t kind, uint8_t* out, void* stream) {
+  return guarded([&] {
+    if (!bits || !out) fail(FECL_EINVAL, "null buffer");
+    if (kind != FECL_CRC24A && kind != FECL_CRC24B) fail(FECL_EINVAL, "Invalid CRC");
+    cuda_check(fecl::launch_crc24_attach(bits, int64_t(len), int64_t(nframes), kind == FECL_CRC24A ? fecl::kCrc24A : fecl::kCrc24B,
+                                         out, static_cast<cudaStream_t>(stream)),
+               "crc");
+  });
+}
+
+int fecl_crc24_check(const uint8_t* bits, uint64_t len, uint64_t nframes, int32_t kind, int32_t* ok, void* stream) {
+  return guarded([&] {
+    if (!bits || !ok) fail(FECL_EINVAL, "null buffer");
+    if (kind != FECL_CRC24A && kind != FECL_CRC24B) fail(FECL_EINVAL, "Invalid CRC");
+    cuda_check(fecl::launch_crc24_check(bits, int64_t(len), int64_t(nframes), kind == FECL_CRC24A ? fecl::kCrc24A : fecl::kCrc24B,
+                                        ok, static_cast<cudaStream_t>(stream)),
+               "crc");
   });
 }
 

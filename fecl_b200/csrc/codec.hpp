@@ -123,6 +123,9 @@ struct fecl_codec_s {
   std::vector<std::unique_ptr<DeviceBuffer>> tables;
   fecl::LdpcDeviceCode ldev;
   DeviceBuffer sched[4];  // custom turbo schedule (stage_ptr, act_con, act_tptr, transfer)
+  DeviceBuffer crc_tab;   // CRC syndrome table of the turbo decoder's CRC stop
+  // The CRC stop's syndrome table on the device, or null when the decoder has none.
+  const uint32_t* crc_table() const { return (kind == 1 && turbo->decoder().crc) ? crc_tab.as<uint32_t>() : nullptr; }
   DeviceBuffer enc[8];  // LDPC generator pieces (DC, A, B, T as CSR) for the device encoder
   fecl::LdpcEncodeTables ltab;
   fecl::TurboDeviceCode tdev;
@@ -313,6 +316,7 @@ struct fecl_codec_s {
     sched[1].upload(ac);
     sched[2].upload(ap);
     sched[3].upload(tr);
+    if (d.crc) crc_tab.upload(fecl::crc24_syndrome_table(turbo->msg_size(), d.crc == 1 ? fecl::kCrc24A : fecl::kCrc24B));
     tdev.n_stages = int32_t(d.schedule.size());
     tdev.stage_ptr = sched[0].as<int32_t>();
     tdev.act_con = sched[1].as<int32_t>();

@@ -203,6 +203,7 @@ struct TurboLteParams {
   int32_t* iters = nullptr;
   float* scratch = nullptr;  // turbo_lte_scratch_bytes(K, nframes)
   unsigned long long* stats = nullptr;  // [3] passes, fix-up rounds, recomputed segments (nullable)
+  const uint32_t* crc = nullptr;        // [K] CRC syndrome table: stop a frame when its CRC checks (nullable)
   // filled by the launcher
   int32_t Kp = 0, Tp = 0, seg_len = 0;
   int64_t frame_stride = 0;
@@ -221,6 +222,7 @@ struct TurboLteBatchFrame {
   float* scratch = nullptr;        // turbo_lte_frame_floats(K) floats, 16-byte aligned
   const uint32_t* perm = nullptr;  // interleaver of constituent 1, padded by 16 entries
   const float* sf = nullptr;       // [2][iterations] scaling of the extrinsic values
+  const uint32_t* crc = nullptr;   // [K] CRC syndrome table, or null for no CRC stop
   int32_t K = 0, iterations = 0, llr_dtype = 1, pad = 0;
 };
 struct TurboLteBatchParams {
@@ -267,6 +269,17 @@ struct ConvMapRun {
 };
 size_t conv_map_scratch_bytes(const TurboDeviceConstituent& k, int64_t nframes);
 cudaError_t launch_conv_map(const TurboDeviceConstituent& k, ConvMapRun r, void* scratch, cudaStream_t s);
+
+// ---- CRC-24 (crc.cu) ----------------------------------------------------------
+
+// The generator polynomials of 3GPP TS 36.212 section 5.1.1, without the x^24 term.
+constexpr uint32_t kCrc24A = 0x864CFBu, kCrc24B = 0x800063u;
+// Appends to each frame of `len` bits its 24 CRC bits (out: [nframes][len + 24]).
+cudaError_t launch_crc24_attach(const uint8_t* bits, int64_t len, int64_t nframes, uint32_t poly, uint8_t* out,
+                                cudaStream_t s);
+// ok[f] = 1 when frame f (len bits, CRC included) has a zero syndrome.
+cudaError_t launch_crc24_check(const uint8_t* bits, int64_t len, int64_t nframes, uint32_t poly, int32_t* ok,
+                               cudaStream_t s);
 
 // ---- encoders and channel (encode.cu) ---------------------------------------
 

@@ -195,6 +195,7 @@ struct Shared {
   int bad[2][kSegs];
   int any_bad;
   float etail[2][4];
+  uint32_t crc_part[kThreads / 32];  // per-warp CRC syndromes
 };
 
 // Inputs of one 8-step chunk [8c, 8c + 8): a-priori and parity L-values.  Every
@@ -325,6 +326,7 @@ struct LteJob {
   uint8_t* hard = nullptr;              // [K]
   int32_t* iters = nullptr;             // nullable
   unsigned long long* stats = nullptr;  // nullable
+  const uint32_t* crc = nullptr;        // [K] x^(K-1-i) mod g: stop when the decisions' CRC checks (nullable)
 };
 
 // Decodes one frame with the whole CTA; smem holds 2 * Kp floats + Shared.
@@ -357,6 +359,7 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
   }
   __syncthreads();
 
+  int ran = q.iterations;
   for (int it = 0; it < q.iterations; ++it) {
     for (int j = 0; j < 2; ++j) {
       const uint32_t* perm = q.perm;
@@ -485,10 +488,30 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
       }
       __syncthreads();
     }
+    // CRC stop (an extension; LTE transport blocks end with a CRC-24): the decisions
+    // after this iteration are those the frame would end with; the CRC syndrome of the
+    // K decided bits is the xor of the table entries of the bits that are 1.
+    if (q.crc) {
+      uint32_t syn = 0;
+      for (int k = tid; k < K; k += kThreads)
+        if ((X[k] + Y[k]) > 0.0f) syn ^= __ldg(q.crc + k);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) syn ^= __shfl_xor_sync(0xffffffffu, syn, o);
+      if ((tid & 31) == 0) sh.crc_part[tid >> 5] = syn;
+      __syncthreads();
+      uint32_t all = 0;
+#pragma unroll
+      for (int w = 0; w < kThreads / 32; ++w) all ^= sh.crc_part[w];
+      __syncthreads();
+      if (all == 0) {
+        ran = it + 1;
+        break;
+      }
+    }
   }
   // a-posteriori and hard decision, TurboDecoderImpl.cpp:64-71
   for (int k = tid; k < K; k += kThreads) q.hard[k] = uint8_t((X[k] + Y[k]) > 0.0f);
-  if (q.iters && tid == 0) *q.iters = q.iterations;
+  if (q.iters && tid == 0) *q.iters = ran;
 }
 
 template <int ALG>
@@ -510,6 +533,7 @@ __global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p
   q.hard = p.hard + f * p.K;
   q.iters = p.iters ? p.iters + f : nullptr;
   q.stats = p.stats;
+  q.crc = p.crc;
   decode_lte_frame<ALG>(q, smem);
 }
 
@@ -605,6 +629,7 @@ __global__ void __launch_bounds__(kThreads, 3) turbo_lte_batch_kernel(TurboLteBa
     q.hard = d.hard;
     q.iters = d.iters;
     q.stats = p.stats;
+    q.crc = d.crc;
     decode_lte_frame<ALG>(q, smem);
   }
 }

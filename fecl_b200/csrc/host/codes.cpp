@@ -536,6 +536,7 @@ void TurboCode::set_decoder(const TurboDecoderConfig& cfg) {
     c.schedule.clear();
   }
   if (cfg.precision < 0 || cfg.precision > 1) throw std::invalid_argument("Invalid message precision");
+  if (cfg.crc < 0 || cfg.crc > 2) throw std::invalid_argument("Invalid CRC");
   // src/detail/Turbo.cpp:127-135
   if (cfg.scaling.size() == c_.size()) {
     for (auto& r : cfg.scaling)
@@ -657,6 +658,18 @@ bool ConvCode::check(const uint8_t* parity) const {
     if (!found) return false;
   }
   return c_.termination == 0 ? state == 0 : true;
+}
+
+std::vector<uint32_t> crc24_syndrome_table(uint32_t K, uint32_t poly) {
+  std::vector<uint32_t> t(K);
+  uint32_t r = poly & 0xFFFFFFu;  // a single 1 as the last bit
+  for (uint32_t i = K; i-- > 0;) {
+    t[i] = r;
+    const uint32_t fb = (r >> 23) & 1u;  // one more zero bit after it
+    r = (r << 1) & 0xFFFFFFu;
+    if (fb) r ^= poly;
+  }
+  return t;
 }
 
 }  // namespace fecl

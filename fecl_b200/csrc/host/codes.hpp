@@ -136,7 +136,12 @@ struct TurboDecoderConfig {
   std::vector<std::vector<double>> scaling{{1.0}};  // [constituent][iteration]
   int precision = 0;
   std::vector<TurboStage> schedule;  // scheduling == Custom
+  int crc = 0;  // an extension: 0 none, 1 CRC-24A, 2 CRC-24B -- decode stops a frame whose CRC checks
 };
+
+// x^(K-1-i) x^24 mod g(x) for i < K: the CRC register a K-bit block with only bit i set
+// leaves, so that a block's syndrome is the xor of the entries of its one bits.
+std::vector<uint32_t> crc24_syndrome_table(uint32_t K, uint32_t poly);
 
 class TurboCode {
  public:

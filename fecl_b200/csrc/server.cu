@@ -244,6 +244,7 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
       d.scratch = reinterpret_cast<float*>(base + cv.take(fecl::turbo_lte_frame_floats(K) * sizeof(float)));
       d.perm = g.c->tdev.c[1].perm;
       d.sf = g.c->tdev.sf;
+      d.crc = g.c->crc_table();
       d.K = K;
       d.iterations = g.c->tdev.iterations;
       d.llr_dtype = g.dtype;

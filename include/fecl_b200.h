@@ -65,6 +65,9 @@ extern "C" {
 #define FECL_MSG_F32 0
 #define FECL_MSG_F16 1
 #define FECL_MSG_I8 2
+/* CRC polynomials (3GPP TS 36.212 section 5.1.1) */
+#define FECL_CRC24A 1
+#define FECL_CRC24B 2
 /* memory flags */
 #define FECL_HOST_MEMORY 0
 #define FECL_DEVICE_MEMORY 1
@@ -162,6 +165,11 @@ typedef struct {
   const uint32_t* activation;
   const uint32_t* transfer_counts;
   const uint32_t* transfer;
+  /* An extension: FECL_CRC24A / FECL_CRC24B when the last 24 message bits are that CRC
+   * of the others (3GPP TS 36.212 section 5.1.1): decode stops a frame after the first
+   * iteration whose decisions pass the CRC (its bits are then those of a decode with
+   * that many iterations); 0 runs every iteration.  LTE turbo codes only. */
+  int32_t crc;
 } fecl_turbo_options;
 
 /* fec::Turbo(EncoderOptions(trellis, interleavers).termination(t), DecoderOptions)
@@ -242,6 +250,14 @@ typedef struct {
 int fecl_so_decode(fecl_codec_t codec, const fecl_so_io* io, uint64_t nframes, int32_t flags, void* stream);
 
 void fecl_destroy(fecl_codec_t codec);
+
+/* ---- CRC-24 (an extension) -------------------------------------------------- */
+
+/* Appends to each of nframes frames of len bits its 24 CRC bits (kind FECL_CRC24A /
+ * FECL_CRC24B): out is [nframes][len + 24].  Device memory, asynchronous on stream. */
+int fecl_crc24_attach(const uint8_t* bits, uint64_t len, uint64_t nframes, int32_t kind, uint8_t* out, void* stream);
+/* ok[f] = 1 when frame f (len bits, its CRC included) passes.  Device memory. */
+int fecl_crc24_check(const uint8_t* bits, uint64_t len, uint64_t nframes, int32_t kind, int32_t* ok, void* stream);
 
 /* ---- puncturing ------------------------------------------------------------ */
 

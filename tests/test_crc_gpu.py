@@ -1,0 +1,78 @@
+"""CRC-24A / CRC-24B (3GPP TS 36.212 section 5.1.1) on the GPU, and the LTE turbo
+decoder's CRC stop: a frame that stops after t iterations has exactly the bits of a
+decode with t iterations; frames whose CRC never passes run every iteration."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _crc_ref(bits, poly):
+    """Bitwise CRC register over a 0/1 sequence, most significant bit first."""
+    r = 0
+    for b in bits:
+        fb = ((r >> 23) & 1) ^ int(b)
+        r = (r << 1) & 0xFFFFFF
+        if fb:
+            r ^= poly
+    return r
+
+
+@pytest.mark.parametrize("kind,poly", [(1, 0x864CFB), (2, 0x800063)])
+def test_attach_and_check(kind, poly):
+    import torch
+    import fecl_b200 as F
+    rng = np.random.default_rng(95)
+    n, L = 9, 1000
+    bits = torch.from_numpy(rng.integers(0, 2, n * L).astype(np.uint8)).cuda()
+    out = F.crc24_attach(bits, kind, n)
+    o = out.cpu().numpy().reshape(n, L + 24)
+    assert np.array_equal(o[:, :L].ravel(), bits.cpu().numpy())
+    for f in range(n):
+        r = _crc_ref(o[f, :L], poly)
+        assert [int(x) for x in o[f, L:]] == [(r >> (23 - k)) & 1 for k in range(24)]
+        assert _crc_ref(o[f], poly) == 0
+    assert bool(F.crc24_check(out, kind, n).all())
+    bad = out.clone()
+    bad[3 * (L + 24) + 17] ^= 1
+    ok = F.crc24_check(bad, kind, n).cpu().numpy()
+    assert not ok[3] and ok.sum() == n - 1
+
+
+@pytest.mark.parametrize("K", [40, 1024, 6144])
+def test_lte_crc_stop_equals_shorter_decodes(K):
+    import torch
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    I = 8
+    dec = F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(I)
+    stop = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(I).crc(F.CRC24A))
+    full = F.Turbo.lte(K, dec)
+    n = 48
+    info = torch.from_numpy(ch.random_bits(n * (K - 24), 96)).cuda()
+    msg = F.crc24_attach(info, F.CRC24A, n)
+    cw = stop.encode(msg)
+    ebn0 = np.repeat(np.linspace(0.2, 2.5, 8), n // 8)
+    llr = torch.from_numpy(ch.awgn_llr_per_frame(cw.cpu().numpy(), stop.paritySize(), ebn0, K / stop.paritySize(), 97,
+                                                 np.float32)).cuda()
+    bits, its = stop.decode(llr, iterations=True)
+    its = its.cpu().numpy()
+    assert its.min() >= 1 and its.max() <= I and len(set(its.tolist())) > 1
+    ok = F.crc24_check(bits, F.CRC24A, n).cpu().numpy()
+    b = bits.cpu().numpy().reshape(n, K)
+    x = llr.cpu().numpy().reshape(n, -1)
+    for t in sorted(set(its.tolist())):
+        shorter = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(t))
+        sel = np.nonzero(its == t)[0]
+        ref = shorter.decode(x[sel].ravel()).reshape(len(sel), K)
+        assert np.array_equal(b[sel], ref), t
+        if t < I:
+            assert ok[sel].all()
+    # the mixed-K batch kernel applies the same stop
+    out = torch.zeros_like(bits)
+    it2 = torch.zeros(n, dtype=torch.int32, device="cuda")
+    F.Batch([(stop, llr, out, it2)]).run()
+    torch.cuda.synchronize()
+    assert torch.equal(out, bits) and np.array_equal(it2.cpu().numpy(), its)
+    # without the CRC stop every frame runs all iterations
+    assert (full.decode(llr, iterations=True)[1].cpu().numpy() == I).all()
