@@ -382,15 +382,16 @@ namespace {
 void reserve_workspace(fecl_codec_s* c, size_t bytes) {
   if (c->ws.bytes >= bytes) return;
   if (c->pending) cuda_check(cudaEventSynchronize(c->done), "cudaEventSynchronize");
-  cuda_check(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
-  cuda_check(cudaStreamSynchronize(c->stream2), "cudaStreamSynchronize");
+  c->sync_pipes();
   c->ws.reserve(bytes);
 }
 
 // Runs a decode.  Device-memory calls launch on the caller's stream.  Host-memory
-// calls pipeline the batch in chunks over two streams of the codec -- copy in,
-// decode, copy out -- so that the copies of one chunk overlap the decode of the
-// other, and return when every result is on the host.
+// calls pipeline the batch in chunks over the codec's streams -- copy in, decode,
+// copy out -- and return when every result is on the host.  A chunk's decode starts
+// as soon as its L-values are in, while later chunks are still being copied, and
+// the decodes of neighbouring chunks share the GPU, so the copy of the batch is
+// hidden behind decoding except for the first chunk.
 void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard, int32_t* iters, bool soft,
                 int32_t flags, cudaStream_t user_stream) {
   if (flags != FECL_HOST_MEMORY && flags != FECL_DEVICE_MEMORY) fail(FECL_EINVAL, "Invalid memory flag");
@@ -422,11 +423,12 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
     return;
   }
 
-  // Chunks of at least kMinChunk frames, at most 4 chunks per call.
-  constexpr uint64_t kMinChunk = 128;
-  const uint64_t nchunks = std::max<uint64_t>(1, std::min<uint64_t>(4, n / kMinChunk));
+  // Chunks of at least kMinChunk frames, at most kMaxChunks per call, one stream each
+  // (reused round robin once every stream has a chunk).
+  constexpr uint64_t kMinChunk = 64, kMaxChunks = 8;
+  const uint64_t nchunks = std::max<uint64_t>(1, std::min<uint64_t>(kMaxChunks, n / kMinChunk));
   const uint64_t chunk = (n + nchunks - 1) / nchunks;
-  const int nslots = nchunks > 1 ? 2 : 1;
+  const int nslots = int(std::min<uint64_t>(nchunks, fecl_codec_s::kPipe));
   Carver cv;
   const size_t o_llr = cv.take(chunk * P * isz);
   const size_t o_syst = io->syst ? cv.take(chunk * S * isz) : 0;
@@ -440,10 +442,8 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
   const ScratchPlan sp = plan_scratch(c, chunk, lte_fast);
   const size_t o_scr = cv.take(sp.bytes);
   const size_t slot_bytes = cv.off;
-  if (c->pending) {
-    cuda_check(cudaStreamWaitEvent(c->stream, c->done, 0), "cudaStreamWaitEvent");
-    cuda_check(cudaStreamWaitEvent(c->stream2, c->done, 0), "cudaStreamWaitEvent");
-  }
+  if (c->pending)
+    for (int q = 0; q < nslots; ++q) cuda_check(cudaStreamWaitEvent(c->pipe[q], c->done, 0), "cudaStreamWaitEvent");
   reserve_workspace(c, slot_bytes * nslots);
   const char* hp = static_cast<const char*>(io->parity);
   for (uint64_t k = 0; k < nchunks; ++k) {
@@ -451,7 +451,7 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
     if (f0 >= n) break;
     const uint64_t nk = std::min(chunk, n - f0);
     const int slot = int(k % nslots);
-    cudaStream_t st = slot == 0 ? c->stream : c->stream2;
+    cudaStream_t st = c->pipe[slot];
     char* base = c->ws.as<char>() + slot * slot_bytes;
     Launch d;
     cuda_check(cudaMemcpyAsync(base + o_llr, hp + f0 * P * isz, nk * P * isz, cudaMemcpyHostToDevice, st), "copy in");
@@ -489,8 +489,7 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
       cuda_check(cudaMemcpyAsync(static_cast<char*>(io->state_out) + f0 * X * osz, d.state_out, nk * X * osz,
                                  cudaMemcpyDeviceToHost, st), "copy out");
   }
-  cuda_check(cudaStreamSynchronize(c->stream), "decode");
-  cuda_check(cudaStreamSynchronize(c->stream2), "decode");
+  c->sync_pipes();
   c->pending = false;
 }
 
@@ -947,7 +946,7 @@ int fecl_turbo_window_stats(fecl_codec_t codec, uint64_t* passes, uint64_t* fixu
     if (c->stats.ptr) {
       DeviceGuard dg(c->device);
       if (c->pending) cuda_check(cudaEventSynchronize(c->done), "cudaEventSynchronize");
-      cuda_check(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+      c->sync_pipes();
       cuda_check(cudaMemcpy(v, c->stats.ptr, sizeof(v), cudaMemcpyDeviceToHost), "stats");
       cuda_check(cudaMemset(c->stats.ptr, 0, sizeof(v)), "stats");
     }

@@ -114,8 +114,8 @@ struct fecl_codec_s {
   std::unique_ptr<fecl::ConvCode> conv;  // kind 2
   fecl::TurboDeviceConstituent cdev{};   // the convolutional trellis on the device
   std::mutex mu;
-  cudaStream_t stream = nullptr;   // host-memory calls: first pipeline stream
-  cudaStream_t stream2 = nullptr;  // host-memory calls: second pipeline stream
+  static constexpr int kPipe = 4;
+  cudaStream_t pipe[kPipe] = {};  // host-memory calls: one stream per chunk in flight
   cudaEvent_t done = nullptr;
   bool pending = false;
   // device description
@@ -133,15 +133,17 @@ struct fecl_codec_s {
   DeviceBuffer ws;
 
   ~fecl_codec_s() {
-    if (stream) {
-      cudaStreamSynchronize(stream);
-      cudaStreamDestroy(stream);
-    }
-    if (stream2) {
-      cudaStreamSynchronize(stream2);
-      cudaStreamDestroy(stream2);
-    }
+    for (cudaStream_t st : pipe)
+      if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+      }
     if (done) cudaEventDestroy(done);
+  }
+
+  // Waits for every host-memory pipeline stream.
+  void sync_pipes() const {
+    for (cudaStream_t st : pipe) cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   }
 
   uint64_t msg() const { return kind == 0 ? ldpc->msg_size() : kind == 1 ? turbo->msg_size() : conv->msg_size(); }
@@ -156,8 +158,7 @@ struct fecl_codec_s {
       fail(FECL_ENODEV, "no CUDA device is visible");
     }
     cuda_check(cudaGetDevice(&device), "cudaGetDevice");
-    cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    cuda_check(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (cudaStream_t& st : pipe) cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "cudaEventCreate");
     cuda_check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attribute");
     cuda_check(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device), "attribute");
