@@ -8,10 +8,14 @@
 // runs on the GPU through fecl_decode / fecl_so_decode; everything else is host
 // code in libfecl_b200.so.  Link with -lfecl_b200.
 //
-// Not carried over: Boost serialization (save/load), the Convolutional codec and
-// Viterbi decoder, custom turbo scheduling, puncturing.
+// Also here: fec::Convolutional (Viterbi decode, MAP soDecode), Custom turbo
+// scheduling (Turbo::DecoderOptions::scheduling(Scheduling)), Codec::puncturing with
+// each family's PunctureOptions, and fec::Permutation's permute / dePermute.
+//
+// Not carried over: Boost serialization (save/load).
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <memory>
@@ -90,23 +94,65 @@ class SparseBitMatrix {
   std::vector<std::vector<size_t>> rows_;
 };
 
-// src/Permutation.h: out[i] = in[sequence[i]].
+// fec::Permutation, src/Permutation.h:32-70: out[i] = in[sequence[i]] per block of
+// inputSize() values; dePermute scatters back (out[sequence[i]] = in[i]), so with a
+// repeated index the last one wins and unmapped positions keep what the output held.
 class Permutation {
  public:
   Permutation() = default;
-  Permutation(const std::vector<size_t>& sequence) : seq_(sequence) {}
+  Permutation(const std::vector<size_t>& sequence) : seq_(sequence) {
+    for (auto v : seq_) input_ = std::max(input_, v + 1);
+  }
+  Permutation(std::vector<size_t> sequence, size_t inputSize) : seq_(std::move(sequence)), input_(inputSize) {}
+  size_t inputSize() const { return input_; }
   size_t outputSize() const { return seq_.size(); }
   size_t operator[](size_t i) const { return seq_[i]; }
   const std::vector<size_t>& sequence() const { return seq_; }
+
+  template <typename T1, typename T2 = T1>
+  void permute(const std::vector<T1>& in, std::vector<T2>& out) const {
+    const size_t n = input_ ? in.size() / input_ : 0;
+    out.resize(n * seq_.size());
+    for (size_t b = 0; b < n; ++b)
+      for (size_t i = 0; i < seq_.size(); ++i) out[b * seq_.size() + i] = in[b * input_ + seq_[i]];
+  }
+  template <typename T1, typename T2 = T1>
+  void dePermute(const std::vector<T1>& in, std::vector<T2>& out) const {
+    const size_t n = seq_.empty() ? 0 : in.size() / seq_.size();
+    out.resize(n * input_);
+    for (size_t b = 0; b < n; ++b)
+      for (size_t i = 0; i < seq_.size(); ++i) out[b * input_ + seq_[i]] = in[b * seq_.size() + i];
+  }
   template <typename T>
   std::vector<T> permute(const std::vector<T>& in) const {
-    std::vector<T> out(seq_.size());
-    for (size_t i = 0; i < seq_.size(); ++i) out[i] = in[seq_[i]];
+    std::vector<T> out;
+    permute(in, out);
     return out;
   }
+  template <typename T>
+  std::vector<T> dePermute(const std::vector<T>& in) const {
+    std::vector<T> out;
+    dePermute(in, out);
+    return out;
+  }
+
  private:
   std::vector<size_t> seq_;
+  size_t input_ = 0;
 };
+
+namespace detail {
+// The kept indices of a puncturing call, as a Permutation of paritySize() inputs.
+template <class F>
+Permutation puncture_list(size_t parity, F call) {
+  uint64_t n = 0;
+  check_status(call(nullptr, &n));
+  std::vector<uint32_t> seq(n);
+  check_status(call(seq.data(), &n));
+  return Permutation(std::vector<size_t>(seq.begin(), seq.end()), parity);
+}
+inline std::vector<uint8_t> bytes(const std::vector<bool>& m) { return std::vector<uint8_t>(m.begin(), m.end()); }
+}  // namespace detail
 
 // src/Trellis.h:131-172; built by Trellis(constraintLengths, generator, feedback), src/Trellis.cpp:76-143.
 class Trellis {
@@ -282,9 +328,22 @@ struct LdpcDecoderOptions {  // src/detail/Ldpc.h:56-74 (iterations default to 5
   std::unordered_map<size_t, std::vector<double>> scaling_{{0, {1.0}}};
 };
 
+// Turbo::Stage, src/detail/Turbo.h:38-48: the constituents a stage activates and, per
+// activation, the constituents whose extrinsic values form its a-priori input.
+struct TurboStage {
+  std::vector<size_t> activation;
+  std::vector<std::vector<size_t>> transfer;
+};
+
 struct TurboDecoderOptions {  // src/detail/Turbo.h:77-101
   TurboDecoderOptions& iterations(size_t n) { iterations_ = n; return *this; }
   TurboDecoderOptions& scheduling(SchedulingType s) { scheduling_ = s; return *this; }
+  TurboDecoderOptions& scheduling(const std::vector<TurboStage>& stages) {
+    scheduling_ = Custom;
+    stages_ = stages;
+    return *this;
+  }
+  std::vector<TurboStage> scheduling() const { return stages_; }
   TurboDecoderOptions& algorithm(DecoderAlgorithm a) { algorithm_ = a; return *this; }
   TurboDecoderOptions& scalingFactor(double f) { scaling_ = {{f}}; return *this; }
   TurboDecoderOptions& scalingFactor(const std::vector<std::vector<double>>& f) { scaling_ = f; return *this; }
@@ -296,6 +355,7 @@ struct TurboDecoderOptions {  // src/detail/Turbo.h:77-101
   SchedulingType scheduling_ = Serial;
   DecoderAlgorithm algorithm_ = Linear;
   std::vector<std::vector<double>> scaling_{{1.0}};
+  std::vector<TurboStage> stages_;
 };
 }  // namespace detail
 
@@ -308,6 +368,11 @@ class Ldpc : public Codec {
     SparseBitMatrix checkMatrix_;
   };
   using DecoderOptions = detail::LdpcDecoderOptions;
+  struct PunctureOptions {  // src/detail/Ldpc.h:76-88
+    PunctureOptions& mask(std::vector<bool> m) { mask_ = std::move(m); return *this; }
+    PunctureOptions& systMask(std::vector<bool> m) { systMask_ = std::move(m); return *this; }
+    std::vector<bool> mask_, systMask_;
+  };
   struct DvbS2 {
     // the standard matrix for n in {16200, 64800}; rate as in src/DvbS2.cpp:27-29
     static SparseBitMatrix matrix(size_t n, double rate) {
@@ -355,6 +420,13 @@ class Ldpc : public Codec {
     decoder_ = decoder;
   }
   DecoderOptions getDecoderOptions() const { return decoder_; }
+  // Ldpc::puncturing, src/Ldpc.h:94 (src/detail/Ldpc.cpp:333-353).
+  Permutation puncturing(const PunctureOptions& o) const {
+    const auto m = detail::bytes(o.mask_), sm = detail::bytes(o.systMask_);
+    return detail::puncture_list(paritySize(), [&](uint32_t* seq, uint64_t* n) {
+      return fecl_ldpc_puncturing(handle(), m.data(), uint32_t(m.size()), sm.data(), uint32_t(sm.size()), seq, n);
+    });
+  }
 
  private:
   // scalingMapToVector, src/detail/Ldpc.cpp:64-112: {degree: per-iteration} with key 0
@@ -415,6 +487,16 @@ class Turbo : public Codec {
     std::vector<Trellis::Termination> term_{Trellis::Tail};
   };
   using DecoderOptions = detail::TurboDecoderOptions;
+  using Stage = detail::TurboStage;
+  using Scheduling = std::vector<Stage>;
+  enum BitOrdering { Alternate = 0, Group = 1 };  // src/detail/Turbo.h:54-57
+  struct PunctureOptions {                         // src/detail/Turbo.h:103-116
+    PunctureOptions& mask(std::vector<std::vector<bool>> m) { mask_ = std::move(m); return *this; }
+    PunctureOptions& tailMask(std::vector<std::vector<bool>> m) { tailMask_ = std::move(m); return *this; }
+    PunctureOptions& bitOrdering(BitOrdering b) { bitOrdering_ = b; return *this; }
+    std::vector<std::vector<bool>> mask_, tailMask_;
+    BitOrdering bitOrdering_ = Alternate;
+  };
   struct Lte3Gpp {
     static Permutation interleaver(size_t K) {
       std::vector<uint32_t> p(K);
@@ -433,7 +515,8 @@ class Turbo : public Codec {
     }
     std::vector<int32_t> term(e.term_.begin(), e.term_.end());
     std::vector<double> table;
-    fecl_turbo_options o = options(d, table);
+    Schedule sched;
+    fecl_turbo_options o = options(d, table, sched);
     fecl_codec_t h = nullptr;
     detail::check_status(fecl_turbo_create(uint32_t(e.perms_.size()), tr.data(), uint32_t(tr.size()),
                                            data.empty() ? nullptr : data.data(), len.data(), term.data(),
@@ -444,14 +527,36 @@ class Turbo : public Codec {
   }
   void setDecoderOptions(const DecoderOptions& d) {
     std::vector<double> table;
-    fecl_turbo_options o = options(d, table);
+    Schedule sched;
+    fecl_turbo_options o = options(d, table, sched);
     detail::check_status(fecl_turbo_set_options(handle(), &o));
     decoder_ = d;
   }
   DecoderOptions getDecoderOptions() const { return decoder_; }
+  // Turbo::puncturing, src/Turbo.h:102 (src/detail/Turbo.cpp:200-320).
+  Permutation puncturing(const PunctureOptions& o) const {
+    std::vector<uint8_t> md, td;
+    std::vector<uint32_t> ml, tl;
+    for (auto& m : o.mask_) {
+      md.insert(md.end(), m.begin(), m.end());
+      ml.push_back(uint32_t(m.size()));
+    }
+    for (auto& m : o.tailMask_) {
+      td.insert(td.end(), m.begin(), m.end());
+      tl.push_back(uint32_t(m.size()));
+    }
+    return detail::puncture_list(paritySize(), [&](uint32_t* seq, uint64_t* n) {
+      return fecl_turbo_puncturing(handle(), md.data(), ml.data(), uint32_t(ml.size()), td.data(), tl.data(),
+                                   uint32_t(tl.size()), int32_t(o.bitOrdering_), seq, n);
+    });
+  }
 
  private:
-  static fecl_turbo_options options(const DecoderOptions& d, std::vector<double>& table) {
+  // A Custom schedule flattened into the arrays of fecl_turbo_options.
+  struct Schedule {
+    std::vector<uint32_t> stage_counts, activation, transfer_counts, transfer;
+  };
+  static fecl_turbo_options options(const DecoderOptions& d, std::vector<double>& table, Schedule& sc) {
     // rows of 1 entry repeat over the iterations (Turbo::Structure::scalingFactor cycles them)
     size_t cols = 1;
     for (auto& r : d.scaling_) cols = std::max(cols, r.size());
@@ -467,6 +572,88 @@ class Turbo : public Codec {
     o.scaling = table.data();
     o.scaling_rows = uint32_t(d.scaling_.size());
     o.scaling_cols = uint32_t(cols);
+    if (d.scheduling_ == Custom) {
+      for (auto& st : d.stages_) {
+        if (st.activation.size() != st.transfer.size())
+          throw std::invalid_argument("Invalid scheduling : activation and transfer not the same size");
+        sc.stage_counts.push_back(uint32_t(st.activation.size()));
+        for (size_t a = 0; a < st.activation.size(); ++a) {
+          sc.activation.push_back(uint32_t(st.activation[a]));
+          sc.transfer_counts.push_back(uint32_t(st.transfer[a].size()));
+          for (auto j : st.transfer[a]) sc.transfer.push_back(uint32_t(j));
+        }
+      }
+      o.n_stages = uint32_t(sc.stage_counts.size());
+      o.stage_counts = sc.stage_counts.data();
+      o.activation = sc.activation.data();
+      o.transfer_counts = sc.transfer_counts.data();
+      o.transfer = sc.transfer.data();
+    }
+    return o;
+  }
+  DecoderOptions decoder_;
+};
+
+// fec::Convolutional, src/Convolutional.h:40-80: decode is the Viterbi decoder, soDecode
+// one MAP pass.
+namespace detail {
+struct ConvEncoderOptions {  // src/detail/Convolutional.h:36-46
+  ConvEncoderOptions(const Trellis& trellis, size_t length) : trellis_(trellis), length_(length) {}
+  ConvEncoderOptions& termination(Trellis::Termination t) { termination_ = t; return *this; }
+  Trellis trellis_;
+  size_t length_;
+  Trellis::Termination termination_ = Trellis::Truncate;
+};
+struct ConvDecoderOptions {  // src/detail/Convolutional.h:48-62
+  ConvDecoderOptions& algorithm(DecoderAlgorithm a) { algorithm_ = a; return *this; }
+  ConvDecoderOptions& scalingFactor(double f) { scaling_ = f; return *this; }
+  DecoderAlgorithm algorithm() const { return algorithm_; }
+  double scalingFactor() const { return scaling_; }
+  DecoderAlgorithm algorithm_ = Approximate;
+  double scaling_ = 1.0;
+};
+struct ConvPunctureOptions {  // src/detail/Convolutional.h:64-75
+  ConvPunctureOptions& mask(std::vector<bool> m) { mask_ = std::move(m); return *this; }
+  ConvPunctureOptions& tailMask(std::vector<bool> m) { tailMask_ = std::move(m); return *this; }
+  std::vector<bool> mask_, tailMask_;
+};
+}  // namespace detail
+
+class Convolutional : public Codec {
+ public:
+  using EncoderOptions = detail::ConvEncoderOptions;
+  using DecoderOptions = detail::ConvDecoderOptions;
+  using PunctureOptions = detail::ConvPunctureOptions;
+
+  Convolutional(const EncoderOptions& e, const DecoderOptions& d = DecoderOptions(), int workGroupSize = 8) {
+    const fecl_trellis t = e.trellis_.table();
+    const fecl_conv_options o = options(d);
+    fecl_codec_t h = nullptr;
+    detail::check_status(fecl_conv_create(&t, uint32_t(e.length_), int32_t(e.termination_), &o, &h));
+    attach(h);
+    decoder_ = d;
+    setWorkGroupSize(workGroupSize);
+  }
+  Convolutional(const EncoderOptions& e, int workGroupSize) : Convolutional(e, DecoderOptions(), workGroupSize) {}
+  void setDecoderOptions(const DecoderOptions& d) {
+    const fecl_conv_options o = options(d);
+    detail::check_status(fecl_conv_set_options(handle(), &o));
+    decoder_ = d;
+  }
+  DecoderOptions getDecoderOptions() const { return decoder_; }
+  // Convolutional::puncturing, src/Convolutional.h:73 (src/detail/Convolutional.cpp:223-242).
+  Permutation puncturing(const PunctureOptions& o) const {
+    const auto m = detail::bytes(o.mask_), t = detail::bytes(o.tailMask_);
+    return detail::puncture_list(paritySize(), [&](uint32_t* seq, uint64_t* n) {
+      return fecl_conv_puncturing(handle(), m.data(), uint32_t(m.size()), t.data(), uint32_t(t.size()), seq, n);
+    });
+  }
+
+ private:
+  static fecl_conv_options options(const DecoderOptions& d) {
+    fecl_conv_options o{};
+    o.algorithm = d.algorithm_;
+    o.scaling = d.scaling_;
     return o;
   }
   DecoderOptions decoder_;

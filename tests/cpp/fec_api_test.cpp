@@ -1,6 +1,7 @@
 // Exercises the C++ API of include/fecl_b200_fec.hpp the way a FeCl program uses
-// fec::Ldpc / fec::Turbo (the operations of test/Cpp/operations.h in the reference:
-// encode then check, bad sizes throw, decode a noisy codeword, soDecode sizes).
+// fec::Ldpc / fec::Turbo / fec::Convolutional (the operations of test/Cpp/operations.h
+// in the reference: encode then check, bad sizes throw, decode a noisy codeword,
+// soDecode sizes), plus puncturing, fec::Permutation and Custom turbo scheduling.
 //
 //   fec_api_test cpu   construction, encode, check, option and size errors (no GPU)
 //   fec_api_test gpu   the above plus decode and soDecode on the current CUDA device
@@ -106,6 +107,28 @@ void decode_ops(const fec::Codec& code, const std::string& name, double snr_db, 
       name + ": soDecode with a bad state size throws");
 }
 
+// Every index of [0, size) at most once; all of them when `all`.
+bool distinct_indices(const fec::Permutation& p, size_t size, bool all) {
+  std::vector<int> seen(size, 0);
+  for (size_t i = 0; i < p.outputSize(); ++i) {
+    if (p[i] >= size || seen[p[i]]++) return false;
+  }
+  return !all || p.outputSize() == size;
+}
+
+void permutation_ops() {
+  fec::Permutation p(std::vector<size_t>{2, 0, 3}, 4);
+  const std::vector<int> in{10, 11, 12, 13, 20, 21, 22, 23};
+  const auto out = p.permute(in);
+  expect(out == std::vector<int>({12, 10, 13, 22, 20, 23}), "Permutation::permute over two blocks");
+  expect(p.dePermute(out) == std::vector<int>({10, 0, 12, 13, 20, 0, 22, 23}),
+         "Permutation::dePermute scatters back, zeros where nothing maps");
+  fec::Permutation rep(std::vector<size_t>{1, 1, 0}, 2);
+  expect(rep.dePermute(std::vector<int>{5, 6, 7}) == std::vector<int>({7, 6}),
+         "Permutation::dePermute: a repeated index keeps the last value");
+  expect(fec::Permutation(std::vector<size_t>{4, 1}).inputSize() == 5, "Permutation input size from its largest index");
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -143,6 +166,80 @@ int main(int argc, char** argv) {
     }
     expect_throw<std::invalid_argument>([&] { fec::Turbo::Lte3Gpp::interleaver(41); },
                                         "Lte3Gpp::interleaver with a non-LTE size throws");
+
+    permutation_ops();
+
+    // Puncturing (Codec::puncturing): index lists of paritySize() inputs.
+    {
+      auto all = s2.puncturing(fec::Ldpc::PunctureOptions());
+      expect(all.inputSize() == s2.paritySize() && distinct_indices(all, s2.paritySize(), true),
+             "Ldpc::puncturing with no mask keeps every bit");
+      auto half = s2.puncturing(fec::Ldpc::PunctureOptions().mask({true, false}));
+      expect(half.outputSize() == s2.paritySize() / 2 && distinct_indices(half, s2.paritySize(), false),
+             "Ldpc::puncturing with mask {1,0} keeps every other bit");
+      const size_t K = 1024;
+      std::vector<size_t> id(K);
+      for (size_t i = 0; i < K; ++i) id[i] = i;
+      fec::Turbo lte(fec::Turbo::EncoderOptions(rsc, {fec::Permutation(id), fec::Turbo::Lte3Gpp::interleaver(K)}),
+                     fec::Turbo::DecoderOptions().algorithm(fec::Approximate).iterations(6));
+      auto group = lte.puncturing(fec::Turbo::PunctureOptions().bitOrdering(fec::Turbo::Group));
+      bool identity = group.outputSize() == lte.paritySize();
+      for (size_t i = 0; identity && i < group.outputSize(); ++i) identity = group[i] == i;
+      expect(identity, "Turbo::puncturing, Group order with no mask is the identity");
+      auto alt = lte.puncturing(fec::Turbo::PunctureOptions());
+      expect(distinct_indices(alt, lte.paritySize(), true), "Turbo::puncturing, Alternate order is a permutation");
+      auto r12 = lte.puncturing(fec::Turbo::PunctureOptions().mask({{true}, {true, false}, {false, true}}));
+      expect(r12.outputSize() > 2 * K && r12.outputSize() < 2 * K + 12 && distinct_indices(r12, lte.paritySize(), false),
+             "Turbo::puncturing to rate 1/2 keeps 2K bits plus part of the tails");
+      expect_throw<std::invalid_argument>([&] { lte.puncturing(fec::Turbo::PunctureOptions().mask({{true}, {true}})); },
+                                          "Turbo::puncturing with a wrong mask count throws");
+      // the punctured stream goes back to full length with zeros (erasures) at punctured bits
+      std::vector<double> tx(r12.outputSize(), 1.0);
+      auto rx = r12.dePermute(tx);
+      size_t zeros = 0;
+      for (double v : rx) zeros += v == 0.0;
+      expect(rx.size() == lte.paritySize() && zeros == lte.paritySize() - r12.outputSize(),
+             "dePermute of a punctured frame leaves erasures");
+    }
+
+    // Convolutional: the (171, 133) code and the LTE RSC, Tail and Truncate.
+    fec::Convolutional cc(fec::Convolutional::EncoderOptions(fec::Trellis({7}, {{0171, 0133}}), 1000)
+                              .termination(fec::Trellis::Tail));
+    expect(cc.msgSize() == 1000 && cc.paritySize() == 2 * (1000 + 6), "Convolutional (171,133) Tail sizes");
+    encode_check(cc, "conv (171,133) tail", 3);
+    fec::Convolutional c75(fec::Convolutional::EncoderOptions(fec::Trellis({3}, {{07, 05}}), 512),
+                           fec::Convolutional::DecoderOptions().algorithm(fec::Linear).scalingFactor(0.9));
+    expect(c75.paritySize() == 1024 && c75.getDecoderOptions().scalingFactor() == 0.9,
+           "Convolutional (7,5) Truncate sizes and options");
+    encode_check(c75, "conv (7,5) truncate", 3);
+    auto cp = cc.puncturing(fec::Convolutional::PunctureOptions().mask({true, true, true, false}));
+    expect(cp.outputSize() == (cc.paritySize() * 3) / 4 && distinct_indices(cp, cc.paritySize(), false),
+           "Convolutional::puncturing to rate 2/3");
+
+    // Custom turbo scheduling: the serial order written as two stages.
+    fec::Turbo::Scheduling serial(2);
+    serial[0].activation = {0};
+    serial[0].transfer = {{1}};
+    serial[1].activation = {1};
+    serial[1].transfer = {{0}};
+    fec::Turbo custom(fec::Turbo::EncoderOptions(rsc, {fec::Permutation(std::vector<size_t>{}),
+                                                      fec::Turbo::Lte3Gpp::interleaver(1024)}),
+                      fec::Turbo::DecoderOptions().algorithm(fec::Approximate).iterations(6).scheduling(serial));
+    expect(custom.getDecoderOptions().schedulingType() == fec::Custom &&
+               custom.getDecoderOptions().scheduling().size() == 2,
+           "Turbo DecoderOptions::scheduling(stages) selects Custom");
+    fec::Turbo::Scheduling bad(1);
+    bad[0].activation = {0, 1};
+    bad[0].transfer = {{1}};
+    expect_throw<std::invalid_argument>(
+        [&] { custom.setDecoderOptions(fec::Turbo::DecoderOptions().scheduling(bad)); },
+        "Custom schedule with activation and transfer of different sizes throws");
+    if (gpu) {
+      decode_ops(custom, "lte K=1024 custom schedule", 2.5, 8);
+      decode_ops(cc, "conv (171,133) tail", 4.0, 6);
+      c75.setDecoderOptions(fec::Convolutional::DecoderOptions().algorithm(fec::Approximate));
+      decode_ops(c75, "conv (7,5) truncate", 6.0, 6);
+    }
 
     if (gpu) {
       decode_ops(s2, "dvbs2 16200 1/2", 2.5, 4);
