@@ -82,6 +82,15 @@ struct Gam {
     g[3] = lp + la;
   }
   __device__ __forceinline__ float of(int s, int u) const { return g[(u << 1) | lte_out(s, u)]; }
+  // x + gamma(s, u).  In max-log the branch with no 1 bits adds nothing: metrics are
+  // never -0 (the largest state normalises to +0, the others are below it), so x + 0
+  // is x and the add is skipped; the other algorithms keep the reference's adds.
+  template <int ALG>
+  __device__ __forceinline__ float plus(float x, int s, int u) const {
+    const int i = (u << 1) | lte_out(s, u);
+    if (ALG == kApproximate && i == 0) return x;
+    return x + g[i];
+  }
 };
 
 // alpha_{t+1} from alpha_t (MapDecoderImpl.cpp:117-139, :237-274), normalised by its max.
@@ -108,6 +117,27 @@ __device__ __forceinline__ void fwd_step(float a[8], const Gam& g) {
       }
 #pragma unroll
     for (int s = 0; s < 8; ++s) n[s] = esum2(c0[s], c1[s]);
+  } else if (ALG == kApproximate) {
+    // max(max(-inf, first), second) of the two branches into each state
+    float c0[8], c1[8];
+    bool first[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) first[s] = true;
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int d = lte_next(s, u);
+        const float v = g.plus<ALG>(a[s], s, u);
+        if (first[d]) {
+          c0[d] = v;
+          first[d] = false;
+        } else {
+          c1[d] = v;
+        }
+      }
+#pragma unroll
+    for (int s = 0; s < 8; ++s) n[s] = fmaxf(c0[s], c1[s]);
   } else {
 #pragma unroll
     for (int s = 0; s < 8; ++s) n[s] = kNegInf;
@@ -132,9 +162,10 @@ __device__ __forceinline__ void bwd_step(float b[8], const Gam& g) {
   float n[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
-    const float x0 = b[lte_next(s, 0)] + g.of(s, 0);
-    const float x1 = b[lte_next(s, 1)] + g.of(s, 1);
+    const float x0 = g.plus<ALG>(b[lte_next(s, 0)], s, 0);
+    const float x1 = g.plus<ALG>(b[lte_next(s, 1)], s, 1);
     if (ALG == kExact) n[s] = esum2(x0, x1);
+    else if (ALG == kApproximate) n[s] = fmaxf(x0, x1);
     else n[s] = lsum<ALG>(lsum<ALG>(kNegInf, x0), x1);
   }
   float m = kNegInf;
@@ -151,7 +182,7 @@ __device__ __forceinline__ float app_step(const float a[8], const float b[8], co
 #pragma unroll
   for (int s = 0; s < 8; ++s)
 #pragma unroll
-    for (int u = 0; u < 2; ++u) d[s * 2 + u] = g.of(s, u) + a[s] + b[lte_next(s, u)];
+    for (int u = 0; u < 2; ++u) d[s * 2 + u] = g.plus<ALG>(a[s], s, u) + b[lte_next(s, u)];
   if (ALG == kExact) {
     float mx0 = kNegInf, mx1 = kNegInf;
 #pragma unroll
@@ -166,6 +197,14 @@ __device__ __forceinline__ float app_step(const float a[8], const float b[8], co
       m1 = ((d[s * 2 + 1] == mx1) ? 1.0f : expf(d[s * 2 + 1] - mx1)) + m1;
     }
     return (logf(m1) + mx1) - (logf(m0) + mx0);
+  } else if (ALG == kApproximate) {
+    float m0 = d[0], m1 = d[1];
+#pragma unroll
+    for (int s = 1; s < 8; ++s) {
+      m0 = fmaxf(m0, d[s * 2]);
+      m1 = fmaxf(m1, d[s * 2 + 1]);
+    }
+    return m1 - m0;
   } else {
     float m0 = kNegInf, m1 = kNegInf;
 #pragma unroll
