@@ -269,15 +269,15 @@ int64_t group_bytes(const LdpcLanesParams& p) {
 
 // Groups decoded together: all iterations of a wave run before the next wave starts,
 // so that a wave whose working set fits in L2 never goes back to HBM for its messages.
-// A wave holds at least kWaveBytes of working set, and at most kWaveCap unless a single
-// group is larger: on B200 (126 MB of L2) DVB-S2 normal frames ran fastest with 71 to
-// 91 MB per wave and lost 15 % at 124 MB, where the passes re-read HBM.
-constexpr int64_t kWaveBytes = 64ll << 20, kWaveCap = 96ll << 20;
+// A wave is the most groups whose working set fits in kWaveCap (at least one group):
+// on B200 (126 MB of L2) DVB-S2 normal frames ran fastest at 91 to 95 MB per wave
+// (FP32 2 groups, int8 4 groups: 933 and 1029 Mbit/s against 877 and 987 with 46 and
+// 71 MB) and lost 15 % at 124 MB, where the passes re-read HBM.
+constexpr int64_t kWaveCap = 96ll << 20;
 
 int wave_for(const LdpcLanesParams& p, int64_t gb) {
   if (p.wave_groups > 0) return p.wave_groups < p.groups ? p.wave_groups : p.groups;
-  int64_t wave = (kWaveBytes + gb - 1) / gb;
-  while (wave > 1 && wave * gb > kWaveCap) --wave;
+  int64_t wave = kWaveCap / gb;
   if (wave < 1) wave = 1;
   return int(wave < p.groups ? wave : p.groups);
 }

@@ -293,17 +293,16 @@ dim3 grid_for(int64_t per_group, int groups) {
   return dim3(unsigned(x > 0 ? x : 1), unsigned(groups));
 }
 
-// Waves as in ldpc_lanes.cu: at least kWaveBytes of working set, at most kWaveCap
-// unless one group is larger (one packed group of DVB-S2 normal frames is 62 MB: one
-// group per wave ran 15 % faster than two).
-constexpr int64_t kWaveBytes = 64ll << 20, kWaveCap = 96ll << 20;
+// Waves as in ldpc_lanes.cu: the most groups whose working set fits in kWaveCap (one
+// packed group of DVB-S2 normal frames is 62 MB: one group per wave ran 15 % faster
+// than two).
+constexpr int64_t kWaveCap = 96ll << 20;
 
 template <int DMAX>
 cudaError_t run(const LdpcLanesParams& p, cudaStream_t s) {
   if (p.groups > 65535) return cudaErrorInvalidValue;
   const int64_t gb = int64_t(kLanes) * (2 * 8 * int64_t(p.N) + 4 * p.E);
-  int64_t wave = p.wave_groups > 0 ? p.wave_groups : (kWaveBytes + gb - 1) / gb;
-  while (p.wave_groups <= 0 && wave > 1 && wave * gb > kWaveCap) --wave;
+  int64_t wave = p.wave_groups > 0 ? p.wave_groups : kWaveCap / gb;
   if (wave < 1) wave = 1;
   if (wave > p.groups) wave = p.groups;
   const dim3 gs((148 * 8 + p.groups - 1) / p.groups, p.groups);
