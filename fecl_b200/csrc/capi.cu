@@ -387,10 +387,12 @@ void reserve_workspace(fecl_codec_s* c, size_t bytes) {
 }
 
 // Runs a decode.  Device-memory calls launch on the caller's stream.  Host-memory
-// calls pipeline the batch in chunks over the codec's streams -- copy in, decode,
-// copy out -- and return when every result is on the host.  A chunk's decode starts
-// as soon as its L-values are in, while later chunks are still being copied, and
-// the decodes of neighbouring chunks share the GPU, so the copy of the batch is
+// calls pipeline the batch in chunks and return when every result is on the host:
+// every chunk has its own device buffers; the chunks are copied in one after the
+// other on one stream, so each arrives at the full host link bandwidth and the first
+// one early; a chunk's decode (and its copy out) starts on one of the codec's decode
+// streams as soon as its inputs are in, while later chunks are still being copied,
+// and the decodes of neighbouring chunks share the GPU.  So the copy of the batch is
 // hidden behind decoding except for the first chunk.
 void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard, int32_t* iters, bool soft,
                 int32_t flags, cudaStream_t user_stream) {
@@ -423,12 +425,12 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
     return;
   }
 
-  // Chunks of at least kMinChunk frames, at most kMaxChunks per call, one stream each
-  // (reused round robin once every stream has a chunk).
-  constexpr uint64_t kMinChunk = 64, kMaxChunks = 8;
+  // Chunks of at least kMinChunk frames, at most kMaxChunks per call, each with its own
+  // buffers; decodes go round robin over the decode streams.
+  constexpr uint64_t kMinChunk = 64, kMaxChunks = fecl_codec_s::kMaxChunks;
   const uint64_t nchunks = std::max<uint64_t>(1, std::min<uint64_t>(kMaxChunks, n / kMinChunk));
   const uint64_t chunk = (n + nchunks - 1) / nchunks;
-  const int nslots = int(std::min<uint64_t>(nchunks, fecl_codec_s::kPipe));
+  const int nslots = int(nchunks);
   Carver cv;
   const size_t o_llr = cv.take(chunk * P * isz);
   const size_t o_syst = io->syst ? cv.take(chunk * S * isz) : 0;
@@ -442,30 +444,35 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
   const ScratchPlan sp = plan_scratch(c, chunk, lte_fast);
   const size_t o_scr = cv.take(sp.bytes);
   const size_t slot_bytes = cv.off;
-  if (c->pending)
-    for (int q = 0; q < nslots; ++q) cuda_check(cudaStreamWaitEvent(c->pipe[q], c->done, 0), "cudaStreamWaitEvent");
+  if (c->pending) {
+    for (cudaStream_t st : c->pipe) cuda_check(cudaStreamWaitEvent(st, c->done, 0), "cudaStreamWaitEvent");
+    cuda_check(cudaStreamWaitEvent(c->copy_in, c->done, 0), "cudaStreamWaitEvent");
+  }
   reserve_workspace(c, slot_bytes * nslots);
   const char* hp = static_cast<const char*>(io->parity);
   for (uint64_t k = 0; k < nchunks; ++k) {
     const uint64_t f0 = k * chunk;
     if (f0 >= n) break;
     const uint64_t nk = std::min(chunk, n - f0);
-    const int slot = int(k % nslots);
-    cudaStream_t st = c->pipe[slot];
+    const int slot = int(k);
+    cudaStream_t st = c->pipe[k % fecl_codec_s::kPipe];
+    cudaStream_t in = c->copy_in;
     char* base = c->ws.as<char>() + slot * slot_bytes;
     Launch d;
-    cuda_check(cudaMemcpyAsync(base + o_llr, hp + f0 * P * isz, nk * P * isz, cudaMemcpyHostToDevice, st), "copy in");
+    cuda_check(cudaMemcpyAsync(base + o_llr, hp + f0 * P * isz, nk * P * isz, cudaMemcpyHostToDevice, in), "copy in");
     d.llr = base + o_llr;
     if (io->syst) {
       cuda_check(cudaMemcpyAsync(base + o_syst, static_cast<const char*>(io->syst) + f0 * S * isz, nk * S * isz,
-                                 cudaMemcpyHostToDevice, st), "copy in");
+                                 cudaMemcpyHostToDevice, in), "copy in");
       d.syst = base + o_syst;
     }
     if (io->state) {
       cuda_check(cudaMemcpyAsync(base + o_state, static_cast<const char*>(io->state) + f0 * X * isz, nk * X * isz,
-                                 cudaMemcpyHostToDevice, st), "copy in");
+                                 cudaMemcpyHostToDevice, in), "copy in");
       d.state = base + o_state;
     }
+    cuda_check(cudaEventRecord(c->arrived[k], in), "cudaEventRecord");
+    cuda_check(cudaStreamWaitEvent(st, c->arrived[k], 0), "cudaStreamWaitEvent");
     if (hard) d.hard = reinterpret_cast<uint8_t*>(base + o_hard);
     if (iters) d.iters = reinterpret_cast<int32_t*>(base + o_iters);
     if (io->msg) d.msg = base + o_msg;

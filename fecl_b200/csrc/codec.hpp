@@ -114,8 +114,10 @@ struct fecl_codec_s {
   std::unique_ptr<fecl::ConvCode> conv;  // kind 2
   fecl::TurboDeviceConstituent cdev{};   // the convolutional trellis on the device
   std::mutex mu;
-  static constexpr int kPipe = 4;
-  cudaStream_t pipe[kPipe] = {};  // host-memory calls: one stream per chunk in flight
+  static constexpr int kPipe = 4, kMaxChunks = 8;
+  cudaStream_t pipe[kPipe] = {};          // host-memory calls: decode and copy-out streams
+  cudaStream_t copy_in = nullptr;         // host-memory calls: every chunk's copy in, in order
+  cudaEvent_t arrived[kMaxChunks] = {};   // chunk k's inputs are on the device
   cudaEvent_t done = nullptr;
   bool pending = false;
   // device description
@@ -138,12 +140,19 @@ struct fecl_codec_s {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
       }
+    if (copy_in) {
+      cudaStreamSynchronize(copy_in);
+      cudaStreamDestroy(copy_in);
+    }
+    for (cudaEvent_t e : arrived)
+      if (e) cudaEventDestroy(e);
     if (done) cudaEventDestroy(done);
   }
 
   // Waits for every host-memory pipeline stream.
   void sync_pipes() const {
     for (cudaStream_t st : pipe) cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    cuda_check(cudaStreamSynchronize(copy_in), "cudaStreamSynchronize");
   }
 
   uint64_t msg() const { return kind == 0 ? ldpc->msg_size() : kind == 1 ? turbo->msg_size() : conv->msg_size(); }
@@ -159,6 +168,8 @@ struct fecl_codec_s {
     }
     cuda_check(cudaGetDevice(&device), "cudaGetDevice");
     for (cudaStream_t& st : pipe) cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaStreamCreateWithFlags(&copy_in, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (cudaEvent_t& e : arrived) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
     cuda_check(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "cudaEventCreate");
     cuda_check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attribute");
     cuda_check(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device), "attribute");
