@@ -765,13 +765,13 @@ int fecl_decode(fecl_codec_t codec, const void* llr, int32_t llr_dtype, uint64_t
                 int32_t flags, void* stream) {
   return guarded([&] {
     auto c = checked(codec);
+    if (nframes == 0) return;  // nothing to decode: empty buffers may be null
     if (!llr || !msg) fail(FECL_EINVAL, "null buffer");
     std::lock_guard<std::mutex> lk(c->mu);
     fecl_so_io io{};
     io.parity = llr;
     io.in_dtype = llr_dtype;
     io.out_dtype = FECL_F32;
-    if (nframes == 0) return;
     run_decode(c, &io, nframes, msg, iterations, false, flags, static_cast<cudaStream_t>(stream));
   });
 }
@@ -780,10 +780,10 @@ int fecl_so_decode(fecl_codec_t codec, const fecl_so_io* io, uint64_t nframes, i
   return guarded([&] {
     auto c = checked(codec);
     if (!io) fail(FECL_EINVAL, "null io");
-    if (!io->parity) fail(FECL_EINVAL, "Input must contains parity");
     if (io->out_dtype != FECL_F64 && io->out_dtype != FECL_F32) fail(FECL_EINVAL, "Invalid output element type");
+    if (nframes == 0) return;  // nothing to decode: empty buffers may be null
+    if (!io->parity) fail(FECL_EINVAL, "Input must contains parity");
     std::lock_guard<std::mutex> lk(c->mu);
-    if (nframes == 0) return;
     run_decode(c, io, nframes, nullptr, nullptr, true, flags, static_cast<cudaStream_t>(stream));
   });
 }
