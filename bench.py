@@ -12,7 +12,9 @@ e2e        the same metric through the public decode call with pinned host buffe
            host->device copy of the L-values and device->host copy of the bits inside
            the timed region.
 roofline   the dominant kernel against the measured HBM copy bandwidth, with the
-           algorithmic bytes of one decode over the decode's device time.
+           algorithmic bytes of one decode (algorithmic_bytes_per_frame: L-values once,
+           per half-iteration the systematic, parity and a-priori reads and the
+           extrinsic write, one byte per decoded bit) over the decode's device time.
 
 `--impl reference` times the reference FeCl decoder compiled from its sources
 (oracle/_ref) on this machine's host cores on the same workload.
