@@ -65,6 +65,18 @@ __device__ __forceinline__ float lsum(float a, float b) {
   return fmaxf(a, b) + lut_log1pexpm(c_lut, fabsf(a - b));
 }
 
+// out[s] = n[s] - m for the 8 states, as four packed f32x2 adds of -m (x - m is
+// x + (-m) exactly, so the values are those of scalar subtractions).
+__device__ __forceinline__ void sub_max(const float n[8], float m, float out[8]) {
+  const float2 nm = make_float2(-m, -m);
+#pragma unroll
+  for (int s = 0; s < 8; s += 2) {
+    const float2 r = __fadd2_rn(make_float2(n[s], n[s + 1]), nm);
+    out[s] = r.x;
+    out[s + 1] = r.y;
+  }
+}
+
 // Two-term log-sum in the Exact (LogSum) form: max, then exp-sum, then log.
 __device__ __forceinline__ float esum2(float x0, float x1) {
   const float m = fmaxf(x0, x1);
@@ -138,6 +150,11 @@ __device__ __forceinline__ void fwd_step(float a[8], const Gam& g) {
       }
 #pragma unroll
     for (int s = 0; s < 8; ++s) n[s] = fmaxf(c0[s], c1[s]);
+    float m = kNegInf;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) m = fmaxf(n[s], m);
+    sub_max(n, m, a);
+    return;
   } else {
 #pragma unroll
     for (int s = 0; s < 8; ++s) n[s] = kNegInf;
@@ -167,6 +184,13 @@ __device__ __forceinline__ void bwd_step(float b[8], const Gam& g) {
     if (ALG == kExact) n[s] = esum2(x0, x1);
     else if (ALG == kApproximate) n[s] = fmaxf(x0, x1);
     else n[s] = lsum<ALG>(lsum<ALG>(kNegInf, x0), x1);
+  }
+  if (ALG == kApproximate) {
+    float m = kNegInf;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) m = fmaxf(n[s], m);
+    sub_max(n, m, b);
+    return;
   }
   float m = kNegInf;
 #pragma unroll
