@@ -76,3 +76,32 @@ def test_lte_crc_stop_equals_shorter_decodes(K):
     assert torch.equal(out, bits) and np.array_equal(it2.cpu().numpy(), its)
     # without the CRC stop every frame runs all iterations
     assert (full.decode(llr, iterations=True)[1].cpu().numpy() == I).all()
+
+
+def test_server_applies_the_crc_stop():
+    """Requests of a CRC-stopping LTE codec through the decode server: the same bits
+    and the same iteration counts as the codec's own decode (so the stop fired in the
+    server's batches too), with some frames stopping before the last iteration."""
+    import torch
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    I = 8
+    codes = [F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(I).crc(F.CRC24A))
+             for K in (1024, 6144)]
+    srv = F.Server(device_budget=2 << 30, max_batch_frames=64, slots=2)
+    reqs = []
+    for i, code in enumerate(codes * 6):
+        K = code.msgSize()
+        info = ch.random_bits(3 * (K - 24), 200 + i)
+        msg = F.crc24_attach(torch.from_numpy(info).cuda(), F.CRC24A, 3).cpu().numpy()
+        llr = ch.awgn_llr(code.encode(msg), 0.6 + 0.3 * (i % 5), K / code.paritySize(), 200 + i, np.float32)
+        reqs.append((code, llr))
+    tickets = [srv.submit(c, llr, iterations=True) for c, llr in reqs]
+    stopped_early = 0
+    for (c, llr), t in zip(reqs, tickets):
+        bits, its, _ = srv.wait(t)
+        ref_bits, ref_its = c.decode(llr, iterations=True)
+        assert np.array_equal(bits, ref_bits) and np.array_equal(its, ref_its)
+        stopped_early += int(np.sum(its < I))
+    srv.close()
+    assert stopped_early > 0
