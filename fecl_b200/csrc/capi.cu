@@ -425,10 +425,12 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
     return;
   }
 
-  // Chunks of at least kMinChunk frames, at most kMaxChunks per call, each with its own
-  // buffers; decodes go round robin over the decode streams.
-  constexpr uint64_t kMinChunk = 64, kMaxChunks = fecl_codec_s::kMaxChunks;
-  const uint64_t nchunks = std::max<uint64_t>(1, std::min<uint64_t>(kMaxChunks, n / kMinChunk));
+  // Chunks of at least one frame group of the kernel that runs (32 frames, 64 for the
+  // packed FP16 LDPC kernel), at most kMaxChunks per call, each with its own buffers;
+  // decodes go round robin over the decode streams.
+  constexpr uint64_t kMaxChunks = fecl_codec_s::kMaxChunks;
+  const uint64_t min_chunk = (c->ldpc_h2_ok() && !io->state) ? 64 : 32;
+  const uint64_t nchunks = std::max<uint64_t>(1, std::min<uint64_t>(kMaxChunks, n / min_chunk));
   const uint64_t chunk = (n + nchunks - 1) / nchunks;
   const int nslots = int(nchunks);
   Carver cv;
