@@ -230,7 +230,9 @@ int fecl_check(fecl_codec_t codec, const uint8_t* parity, uint64_t nframes, int3
 
 /* Codec::decode -- src/Codec.h:210-238.  llr: [nframes][paritySize] of llr_dtype;
  * msg: [nframes][msgSize] bytes 0/1.  iterations (nullable): per frame, the number
- * of iterations the decoder ran (LDPC: check-node updates; turbo: iterations). */
+ * of iterations the decoder ran (LDPC: check-node updates; turbo: iterations).
+ * nframes == 0 returns FECL_OK at once and the buffers may then be null (this and
+ * fecl_so_decode), as the reference decodes an empty vector to an empty one. */
 int fecl_decode(fecl_codec_t codec, const void* llr, int32_t llr_dtype, uint64_t nframes, uint8_t* msg,
                 int32_t* iterations, int32_t flags, void* stream);
 
