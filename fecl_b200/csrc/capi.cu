@@ -347,8 +347,8 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
     r.crc = c->crc_table();
     e = fecl::launch_turbo_lte(r, s);
   } else {
-    if (!soft && c->turbo->decoder().crc) fail(FECL_EUNSUPPORTED, "CRC stop needs the LTE turbo code with serial scheduling");
     fecl::TurboRun r;
+    if (!soft) r.crc = c->crc_table();
     r.nframes = int64_t(n);
     r.soft = soft ? 1 : 0;
     r.llr = d.llr;

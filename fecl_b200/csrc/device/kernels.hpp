@@ -178,6 +178,7 @@ struct TurboRun {
   void* parity_out = nullptr;
   void* state_out = nullptr;
   int32_t out_dtype = 1;
+  const uint32_t* crc = nullptr;  // [msg] x^(msg-1-i) x^24 mod g: hard decode stops on a passing CRC (nullable)
   // scratch, FP32, per frame
   float* parity_in = nullptr;   // [nframes][parity]
   float* parity_buf = nullptr;  // [nframes][parity]

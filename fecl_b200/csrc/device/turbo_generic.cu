@@ -341,6 +341,20 @@ __device__ void aposteriori(const TurboDeviceCode& c, Frame& fr) {
   }
 }
 
+// CRC stop (an extension): the decisions the frame would end with after this
+// iteration -- channel systematic plus every constituent's extrinsic values, as at
+// the end of decodeBlock -- and whether their CRC syndrome, the xor of the table
+// entries of the bits that are 1, is zero.  Uses the systematic part of parity_buf,
+// which every transfer rewrites before it reads it.
+__device__ bool crc_passes(const TurboDeviceCode& c, Frame& fr, const uint32_t* crc) {
+  for (int k = 0; k < c.msg; ++k) fr.pout[k] = fr.pin[k];
+  aposteriori(c, fr);
+  uint32_t syn = 0;
+  for (int k = 0; k < c.msg; ++k)
+    if (fr.pout[k] > 0.0f) syn ^= __ldg(crc + k);
+  return syn == 0;
+}
+
 template <int ALG>
 __global__ void __launch_bounds__(64) turbo_generic_f32(TurboDeviceCode c, TurboRun p) {
   const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -362,6 +376,7 @@ __global__ void __launch_bounds__(64) turbo_generic_f32(TurboDeviceCode c, Turbo
   if (p.soft && c.iterations == 0 && want_parity)
     for (int k = c.syst; k < c.parity; ++k) fr.pout[k] = 0.0f;
 
+  int ran = c.iterations;
   for (int i = 0; i < c.iterations; ++i) {
     if (c.scheduling == 2) {
       for (int st = 0; st < c.n_stages; ++st) {
@@ -372,20 +387,24 @@ __global__ void __launch_bounds__(64) turbo_generic_f32(TurboDeviceCode c, Turbo
         fr.extb = t;
         custom_activation<ALG>(c, fr, i, st);
       }
-      continue;
+    } else {
+      if (c.scheduling == 1) parallel_transfer(c, fr);
+      const float* par = fr.pin + c.syst;
+      float* pout = fr.pout + c.syst;
+      float* ext = fr.ext;
+      for (int j = 0; j < c.n; ++j) {
+        if (c.scheduling == 0) serial_transfer(c, fr, j);
+        const float sf = p.soft ? 1.0f : c.sf[j * c.iterations + i];
+        const bool last = (i == c.iterations - 1);
+        map_pass<ALG>(c.c[j], par, ext, (want_parity && last) ? pout : nullptr, sf, fr.alpha);
+        ext += c.c[j].syst_size;
+        par += c.c[j].parity_size;
+        pout += c.c[j].parity_size;
+      }
     }
-    if (c.scheduling == 1) parallel_transfer(c, fr);
-    const float* par = fr.pin + c.syst;
-    float* pout = fr.pout + c.syst;
-    float* ext = fr.ext;
-    for (int j = 0; j < c.n; ++j) {
-      if (c.scheduling == 0) serial_transfer(c, fr, j);
-      const float sf = p.soft ? 1.0f : c.sf[j * c.iterations + i];
-      const bool last = (i == c.iterations - 1);
-      map_pass<ALG>(c.c[j], par, ext, (want_parity && last) ? pout : nullptr, sf, fr.alpha);
-      ext += c.c[j].syst_size;
-      par += c.c[j].parity_size;
-      pout += c.c[j].parity_size;
+    if (!p.soft && p.crc && i + 1 < c.iterations && crc_passes(c, fr, p.crc)) {
+      ran = i + 1;
+      break;
     }
   }
 
@@ -405,7 +424,7 @@ __global__ void __launch_bounds__(64) turbo_generic_f32(TurboDeviceCode c, Turbo
     if (p.msg_out)
       for (int k = 0; k < c.msg; ++k) store_llr(p.msg_out, p.out_dtype, f * c.msg + k, fr.pin[k] + fr.pout[k]);
   }
-  if (p.iters) p.iters[f] = c.iterations;
+  if (p.iters) p.iters[f] = ran;
 }
 
 // The convolutional codec's soDecode (Convolutional::soDecodeBlocks ->

@@ -168,7 +168,8 @@ typedef struct {
   /* An extension: FECL_CRC24A / FECL_CRC24B when the last 24 message bits are that CRC
    * of the others (3GPP TS 36.212 section 5.1.1): decode stops a frame after the first
    * iteration whose decisions pass the CRC (its bits are then those of a decode with
-   * that many iterations); 0 runs every iteration.  LTE turbo codes only. */
+   * that many iterations); 0 runs every iteration.  Any turbo code and scheduling;
+   * soft-output decoding (fecl_so_decode) runs every iteration. */
   int32_t crc;
 } fecl_turbo_options;
 

@@ -105,3 +105,47 @@ def test_server_applies_the_crc_stop():
         stopped_early += int(np.sum(its < I))
     srv.close()
     assert stopped_early > 0
+
+
+def _generic_code(which, iterations, crc):
+    import fecl_b200 as F
+    from goldens import ARRAYS, T17
+    if which == "lte-parallel":
+        d = F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(iterations).scheduling(F.Parallel)
+        if crc:
+            d = d.crc(F.CRC24A)
+        return F.Turbo.lte(1024, d)
+    d = F.Turbo.DecoderOptions().algorithm(F.Linear).iterations(iterations).scheduling(F.Serial)
+    if crc:
+        d = d.crc(F.CRC24A)
+    perms = [np.arange(1024, dtype=np.uint32), ARRAYS["perm_1024"]]
+    return F.Turbo(F.Turbo.EncoderOptions([F.Trellis(*T17)], perms).termination(0), d)
+
+
+@pytest.mark.parametrize("which", ["lte-parallel", "t17-serial-linear"])
+def test_generic_kernel_crc_stop_equals_shorter_decodes(which):
+    """The CRC stop in the generic turbo kernel (any code, any scheduling): a frame
+    that stops after t iterations has exactly the bits of a decode with t iterations,
+    its CRC passes, and frames whose CRC never passes run every iteration."""
+    import torch
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    I = 8
+    stop = _generic_code(which, I, True)
+    K, P = stop.msgSize(), stop.paritySize()
+    n = 40
+    info = torch.from_numpy(ch.random_bits(n * (K - 24), 210)).cuda()
+    msg = F.crc24_attach(info, F.CRC24A, n).cpu().numpy()
+    ebn0 = np.repeat(np.linspace(0.0, 2.5, 8), n // 8)
+    llr = ch.awgn_llr_per_frame(stop.encode(msg), P, ebn0, K / P, 211, np.float32)
+    bits, its = stop.decode(llr, iterations=True)
+    assert its.min() >= 1 and its.max() <= I and len(set(its.tolist())) > 1
+    ok = F.crc24_check(torch.from_numpy(bits).cuda(), F.CRC24A, n).cpu().numpy()
+    b = bits.reshape(n, K)
+    x = llr.reshape(n, -1)
+    for t in sorted(set(its.tolist())):
+        sel = np.nonzero(its == t)[0]
+        ref = _generic_code(which, t, False).decode(x[sel].ravel()).reshape(len(sel), K)
+        assert np.array_equal(b[sel], ref), t
+        if t < I:
+            assert ok[sel].all()
