@@ -85,18 +85,67 @@ def profiled_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region.  NVML is polled
+    from a thread every 2 ms (one sample also on entry and on exit), so even a timed
+    region of a tenth of a second has tens of samples; where NVML cannot be loaded,
+    nvidia-smi samples every 200 ms instead."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock event reason bits (nvmlClocksEventReason*) of the reasons reported
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+                   ("sw_power_cap", 0x4))
 
     def __init__(self, index):
         self.index = index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.rows = []
+        self.nvml = None
+        self.handle = None
+        self.max_mhz = None
+        self.f = None
         self.p = None
+        self.thread = None
+        self.stop = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _sample(self):
+        n = self.nvml
+        try:
+            sm = n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM)
+            get = getattr(n, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                n.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.rows.append((float(sm), int(get(self.handle))))
+        except Exception:
+            pass
+
+    def _poll(self):
+        while not self.stop.wait(0.002):
+            self._sample()
 
     def __enter__(self):
         try:
+            import threading
+            self.nvml, self.handle = self._nvml_handle()
+            self.max_mhz = float(self.nvml.nvmlDeviceGetMaxClockInfo(self.handle, self.nvml.NVML_CLOCK_SM))
+            self._sample()
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
                                        "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
@@ -105,6 +154,10 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self._sample()
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.p is not None:
             self.p.terminate()
             try:
@@ -113,6 +166,12 @@ class ClockSampler:
                 self.p.kill()
 
     def summary(self):
+        if self.nvml is not None:
+            if not self.rows:
+                return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "source": "nvml"}
+            reasons = sorted({name for _, mask in self.rows for name, bit in self.REASON_BITS if mask & bit})
+            return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(self.rows), "source": "nvml"}
         try:
             self.f.seek(0)
             rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
@@ -130,7 +189,7 @@ class ClockSampler:
                 if v.strip().lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
+                "reasons": sorted(reasons), "samples": len(rows), "source": "nvidia-smi"}
 
 
 def cpu_reference(frames_sample, llr, code_sizes):

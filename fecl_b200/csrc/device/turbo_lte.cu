@@ -601,25 +601,29 @@ __global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p
 }
 
 
-// Input [f][3K+12] in FeCl's turbo layout -> padded FP32 scratch.
+template <typename T>
+__device__ __forceinline__ float to_f32(T v) { return float(v); }
+template <>
+__device__ __forceinline__ float to_f32<__half>(__half v) { return __half2float(v); }
+
+// Input [f][3K+12] in FeCl's turbo layout -> padded FP32 scratch, one block per frame
+// (grid-strided over frames): the systematic, parity and tail regions are copied by
+// loops of their own, so no element needs a division to find its place, and the
+// element type is fixed per launch.
+template <typename T>
 __global__ void turbo_lte_stage(TurboLteParams p) {
-  const int K = p.K;
-  const int64_t total = p.nframes * p.frame_stride;
-  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total; idx += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t f = idx / p.frame_stride;
-    const int i = int(idx - f * p.frame_stride);
-    const int64_t in0 = f * int64_t(3 * K + 12);
-    float v = 0.0f;
-    if (i < p.Kp) {
-      if (i < K) v = load_llr(p.llr, p.llr_dtype, in0 + i);
-    } else if (i < p.Kp + 2 * p.Tp) {
-      const int c = (i - p.Kp) / p.Tp, t = (i - p.Kp) % p.Tp;
-      if (t < K + 3) v = load_llr(p.llr, p.llr_dtype, in0 + K + 6 + c * (K + 3) + t);
-    } else {
-      const int t = i - p.Kp - 2 * p.Tp;
-      if (t < 6) v = load_llr(p.llr, p.llr_dtype, in0 + K + t);
+  const T* llr = static_cast<const T*>(p.llr);
+  const int K = p.K, Kp = p.Kp, Tp = p.Tp;
+  for (int64_t f = blockIdx.x; f < p.nframes; f += gridDim.x) {
+    const T* in = llr + f * int64_t(3 * K + 12);
+    float* out = p.scratch + f * p.frame_stride;
+    for (int i = threadIdx.x; i < Kp; i += blockDim.x) out[i] = i < K ? to_f32(in[i]) : 0.0f;
+    for (int c = 0; c < 2; ++c) {
+      const T* src = in + K + 6 + c * (K + 3);  // parity (with its tail) of constituent c
+      float* dst = out + Kp + c * Tp;
+      for (int t = threadIdx.x; t < Tp; t += blockDim.x) dst[t] = t < K + 3 ? to_f32(src[t]) : 0.0f;
     }
-    p.scratch[idx] = v;
+    if (threadIdx.x < 8) out[Kp + 2 * Tp + threadIdx.x] = threadIdx.x < 6 ? to_f32(in[K + threadIdx.x]) : 0.0f;
   }
 }
 
@@ -732,7 +736,12 @@ cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
   L = (L + kBlk - 1) / kBlk * kBlk;
   p.seg_len = L;
   if (p.train < 0) p.train = 96;
-  turbo_lte_stage<<<1184, 256, 0, s>>>(p);
+  const unsigned stage_blocks = unsigned(p.nframes < 148 * 8 ? p.nframes : 148 * 8);
+  switch (p.llr_dtype) {
+    case kF64: turbo_lte_stage<double><<<stage_blocks, 256, 0, s>>>(p); break;
+    case kF16: turbo_lte_stage<__half><<<stage_blocks, 256, 0, s>>>(p); break;
+    default: turbo_lte_stage<float><<<stage_blocks, 256, 0, s>>>(p); break;
+  }
   const size_t smem = size_t(2 * p.Kp) * sizeof(float) + sizeof(Shared);
   auto launch = [&](auto kern) -> cudaError_t {
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
