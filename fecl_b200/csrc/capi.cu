@@ -452,6 +452,18 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
   }
   reserve_workspace(c, slot_bytes * nslots);
   const char* hp = static_cast<const char*>(io->parity);
+  // If a step fails part way, the copies already queued still read and write the
+  // caller's host buffers: let them finish before the error returns.
+  struct Drain {
+    fecl_codec_s* c;
+    bool armed = true;
+    ~Drain() {
+      if (!armed) return;
+      for (cudaStream_t st : c->pipe) cudaStreamSynchronize(st);
+      cudaStreamSynchronize(c->copy_in);
+      cudaGetLastError();
+    }
+  } drain{c};
   for (uint64_t k = 0; k < nchunks; ++k) {
     const uint64_t f0 = k * chunk;
     if (f0 >= n) break;
@@ -499,6 +511,7 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
                                  cudaMemcpyDeviceToHost, st), "copy out");
   }
   c->sync_pipes();
+  drain.armed = false;
   c->pending = false;
 }
 
