@@ -803,13 +803,115 @@ def run_serving(args):
     return 0
 
 
+SWEEP_SHIFTS = (0.1, 0.25)
+
+
+def run_fer_sweep(args):
+    """FER sweep of the DVB-S2 normal-frame decoder (fecl_b200/fer.py): rates 1/2, 3/4,
+    9/10, 512 frames per point, Eb/N0 1.0-4.0 dB in 0.25 dB steps, normalised min-sum
+    0.75, <= 50 iterations, FP32 / FP16 / int8 message storage, against the FP64
+    reference decoder's frame failures on the same L-values (tests/golden/
+    fer_sweep_oracle.json).  Each reduced-precision decoder also runs 0.1 and 0.25 dB
+    above every point on the same noise draws, so "loses at most 0.1 dB" is a
+    pointwise comparison (loss_check_points_over lists the points where it does not
+    hold).  One GPU: under torchrun only rank 0 runs the sweep."""
+    import numpy as np
+    import torch
+    from fecl_b200 import fer
+
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    with open(os.path.join(ROOT, "tests", "golden", "fer_sweep_oracle.json")) as f:
+        oracle = json.load(f)
+    precs = (("f32", 0), ("f16", 1), ("i8", 2))
+    stream = torch.cuda.current_stream()
+    ms = {p: 0.0 for p, _ in precs}
+    info_bits = 0
+    report, thresholds, losses, f32_equal, llr_err = {}, {}, {}, {}, {}
+    with ClockSampler(local) as clk:
+        for r, (num, den) in enumerate(fer.RATES):
+            name = "%d/%d" % (num, den)
+            codes = {p: fer.code(r, q) for p, q in precs}
+            K = codes["f32"].msgSize()
+            o_fer = oracle["rates"][name]["fer"]
+            curves = {p: [] for p, _ in precs}
+            curves.update({"%s_shift%g" % (pn, d): [] for pn in ("f16", "i8") for d in SWEEP_SHIFTS})
+            diff = []
+            mid = min(range(len(o_fer)), key=lambda i: abs(o_fer[i] - 0.5))
+            for p in range(len(fer.EBN0_DB)):
+                msg = fer.sweep_msg(K, r, p)
+                cw = codes["f32"].encode(msg)
+                d_llr = torch.from_numpy(fer.sweep_llr(cw, K, r, p)).cuda()
+                out = torch.empty(fer.FRAMES * K, dtype=torch.uint8, device="cuda")
+                for pn, _ in precs:
+                    codes[pn].decode(d_llr, out=out)  # warm-up of this shape
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    codes[pn].decode(d_llr, out=out)
+                    e1.record(stream)
+                    e1.synchronize()
+                    ms[pn] += e0.elapsed_time(e1)
+                    fails = fer.frame_fails(out.cpu().numpy(), msg, fer.FRAMES)
+                    curves[pn].append(float(fails.mean()))
+                    if pn == "f32":
+                        ofails = fer.unpack_fails(oracle["rates"][name]["fails"][p], fer.FRAMES)
+                        diff.append(int(np.sum(fails != ofails)))
+                if p == mid:
+                    # a-posteriori message L-values of the reduced precisions against FP32
+                    import fecl_b200 as F
+                    so = {pn: codes[pn].soDecode(F.Codec.Input().parity(d_llr), F.Codec.Output(np.float32).msg()).msg()
+                          for pn, _ in precs}
+                    ref = so["f32"].double()
+                    llr_err[name] = {"ebn0_db": fer.EBN0_DB[p]}
+                    for pn in ("f16", "i8"):
+                        d = so[pn].double() - ref
+                        llr_err[name][pn] = {
+                            "rel_rms": round(float(d.pow(2).mean().sqrt() / ref.pow(2).mean().sqrt()), 5),
+                            "sign_agree": round(float(((so[pn] >= 0) == (so["f32"] >= 0)).double().mean()), 6)}
+                for d in SWEEP_SHIFTS:
+                    s_llr = torch.from_numpy(fer.sweep_llr(cw, K, r, p, shift_db=d)).cuda()
+                    for pn in ("f16", "i8"):
+                        codes[pn].decode(s_llr, out=out)
+                        curves["%s_shift%g" % (pn, d)].append(
+                            float(fer.frame_fails(out.cpu().numpy(), msg, fer.FRAMES).mean()))
+                info_bits += fer.FRAMES * K
+            report[name] = {"oracle": o_fer, **{k: v for k, v in curves.items()}}
+            f32_equal[name] = {"frames_differing_per_point": diff}
+            thresholds[name] = {
+                "fer_%g" % t: {k: (None if (x := fer.threshold_db(fer.EBN0_DB, c, t)) is None else round(x, 3))
+                               for k, c in (("oracle", o_fer), ("f32", curves["f32"]), ("f16", curves["f16"]),
+                                            ("i8", curves["i8"]))}
+                for t in (0.1, 0.01)}
+            losses[name] = {"%s_shift%g" % (pn, d): fer.loss_check(curves["%s_shift%g" % (pn, d)], o_fer)
+                            for pn in ("f16", "i8") for d in SWEEP_SHIFTS}
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": round(info_bits / (ms["f16"] * 1e-3) / 1e6, 2), "unit": "Mbit/s", "n_gpus": 1,
+        "steps": 1, "warmup": 1, "ms_per_step": round(ms["f16"], 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f16", "data": "synthetic",
+        "config": {"workload": "FER sweep: DVB-S2 normal n=64800 r=1/2, 3/4, 9/10 x 512 frames per point, Eb/N0 "
+                               "1.0-4.0 dB in 0.25 dB steps, normalised min-sum 0.75, <=50 iterations with syndrome "
+                               "stop, FP32 L-values; FP32/FP16/int8 messages against the FP64 reference decoder",
+                   "l2": "inputs 133 MB per point (larger than L2)", "parallelism": "single GPU"},
+        "mbps_by_precision": {p: round(info_bits / (ms[p] * 1e-3) / 1e6, 2) for p, _ in precs},
+        "ebn0_db": list(fer.EBN0_DB), "fer": report, "f32_vs_oracle": f32_equal,
+        "threshold_db": thresholds, "shifts_db": list(SWEEP_SHIFTS),
+        "loss_check_points_over": losses, "llr_error_vs_f32": llr_err,
+        "gpu_launches": None, "clocks": clocks,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lte-turbo", choices=["lte-turbo", "mixed", "serving"] + sorted(LDPC_WORKLOADS),
+    ap.add_argument("--workload", default="lte-turbo", choices=["lte-turbo", "mixed", "serving", "fer-sweep"] + sorted(LDPC_WORKLOADS),
                     help="lte-turbo is the headline workload; the LDPC workloads print the same line for BP")
     ap.add_argument("--frames", type=int, default=0,
                     help="LDPC workloads: frames per code instead of the workload's (small cases for ncu)")
@@ -838,6 +940,8 @@ def main():
         return run_mixed(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "fer-sweep":
+        return run_fer_sweep(args)
 
     import numpy as np
     import torch
