@@ -33,6 +33,16 @@ constexpr uint32_t kSigns = 0x80008000u;
 __device__ __forceinline__ uint32_t bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
 __device__ __forceinline__ __half2 from_bits(uint32_t u) { return *reinterpret_cast<__half2*>(&u); }
 
+// (v.x, v.y) rounded to nearest FP16, overflow saturated to +-65504, as one
+// conversion: the same bits as rounding and then clamping to [-65504, 65504] for
+// every finite or infinite input.  The PTX operand order puts the first source in
+// the upper half.
+__device__ __forceinline__ __half2 half2_satfinite(float2 v) {
+  uint32_t r;
+  asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(v.y), "f"(v.x));
+  return from_bits(r);
+}
+
 // active[it & 1][g][2] and fail[it & 1][g][2]: .x and .y frame masks.
 __device__ __forceinline__ uint32_t* active_of(const LdpcLanesParams& p, int it) { return p.active + (it & 1) * 2 * p.groups; }
 __device__ __forceinline__ uint32_t* fail_of(const LdpcLanesParams& p, int it) { return p.fail + (it & 1) * 2 * p.groups; }
@@ -63,8 +73,7 @@ __device__ __forceinline__ void load_row(const LdpcLanesParams& p, int g, int r,
       w.px ^= unsigned(a.x >= 0.0f);
       w.py ^= unsigned(a.y >= 0.0f);
       // a - c in FP32, rounded to FP16 and kept finite (saturated at +-65504)
-      const __half2 vh = __float22half2_rn(__ffma2_rn(c, make_float2(-1.0f, -1.0f), a));
-      w.v[j] = __hmax2(__hmin2(vh, __float2half2_rn(65504.0f)), __float2half2_rn(-65504.0f));
+      w.v[j] = half2_satfinite(__ffma2_rn(c, make_float2(-1.0f, -1.0f), a));
     }
   }
 }
