@@ -80,7 +80,7 @@ __device__ __forceinline__ void load_row(const LdpcLanesParams& p, int g, int r,
 
 template <int DMAX>
 __device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, int lane, const Row<DMAX>& w, __half2 sf2,
-                                          bool mine_x, bool mine_y) {
+                                          bool mine_x, bool mine_y, bool keep_all) {
   __half2* c2v = static_cast<__half2*>(p.c2v);
   const __half2 inf2 = __floats2half2_rn(INFINITY, INFINITY);
   __half2 m1 = inf2, m2 = inf2;
@@ -96,9 +96,14 @@ __device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, int l
   }
   // d - 1 inputs per output: the sign is (d - 2) xor the parity of the others' signs.
   sg = (sg & kSigns) ^ (((w.d - 2) & 1) ? kSigns : 0u);
-  const uint32_t b1 = bits(m1), b2 = bits(m2);
-  // lanes whose frames are not decoding keep their messages
-  const uint32_t keep = (mine_x ? 0u : 0x0000ffffu) | (mine_y ? 0u : 0xffff0000u);
+  // The scaling is applied to the two magnitudes once per row: rounding to nearest is
+  // symmetric, so (-m) * s is -(m * s) bit for bit and the edge's sign can be xored
+  // into the scaled magnitude.
+  const uint32_t b1 = bits(__hmul2(m1, sf2)), b2 = bits(__hmul2(m2, sf2));
+  // Lanes whose frames are not decoding keep their messages where the soft outputs,
+  // which are sums of these messages, are wanted; a hard-decision decode reads only
+  // the a-posteriori values, which the bit pass freezes for retired frames.
+  const uint32_t keep = keep_all ? (mine_x ? 0u : 0x0000ffffu) | (mine_y ? 0u : 0xffff0000u) : 0u;
   __half2* cg = c2v + (int64_t(g) * p.E + w.e0) * kLanes + lane;
 #pragma unroll
   for (int j = 0; j < DMAX; ++j) {
@@ -106,7 +111,7 @@ __device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, int l
       const uint32_t eq = __heq2_mask(__habs2(w.v[j]), m1);
       const uint32_t mag = (b2 & eq) | (b1 & ~eq);
       const uint32_t sign = (sg ^ bits(w.v[j])) & kSigns;
-      const __half2 out = __hmul2(from_bits(mag | sign), sf2);
+      const __half2 out = from_bits(mag ^ sign);
       if (keep == 0u) {
         cg[j * kLanes] = out;
       } else if (keep != 0xffffffffu) {
@@ -127,6 +132,7 @@ __global__ void __launch_bounds__(kWarps * 32) h2_check(LdpcLanesParams p, int i
   const uint32_t ax = active_of(p, it)[2 * g], ay = active_of(p, it)[2 * g + 1];
   if ((ax | ay) == 0) return;
   const bool mx = (ax >> lane) & 1, my = (ay >> lane) & 1;
+  const bool keep_all = p.msg_out || p.syst_out || p.parity_out || p.state_out;
   uint32_t bx = 0, by = 0;
   const int w0 = int(blockIdx.x) * kWarps + (threadIdx.x >> 5);
   for (int r = w0 * kRows; r < p.M; r += warps * kRows) {
@@ -145,7 +151,7 @@ __global__ void __launch_bounds__(kWarps * 32) h2_check(LdpcLanesParams p, int i
         }
         // the scaling of rows of this degree (constant across iterations on this path)
         const float s = p.sf[size_t(it % p.n_sf) * p.sf_stride + (w[q].d >= 2 ? w[q].d - 2 : 0)];
-        store_row<DMAX>(p, g, lane, w[q], __float2half2_rn(s), mx, my);
+        store_row<DMAX>(p, g, lane, w[q], __float2half2_rn(s), mx, my, keep_all);
       }
     }
   }
