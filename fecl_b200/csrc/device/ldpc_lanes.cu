@@ -82,6 +82,31 @@ __device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, uint3
                                           const float v[DMAX], bool mine) {
   using M = Msg<MSG>;
   auto* c2v = static_cast<typename M::T*>(p.c2v);
+  if (ALG == kApproximate) {
+    // Min-sum: each output is sf * (+-m1) or sf * (+-m2).  The product and the storage
+    // encoding are odd in the sign, so the two magnitudes are scaled and encoded once
+    // per row and every edge selects one and negates it: the same stored values as
+    // encoding sf * (+-m) edge by edge.
+    float m1, m2;
+    int i1;
+    unsigned par;
+    ldpc::min_sum_scan<DMAX>(v, d, m1, m2, i1, par);
+    const float sf = sf_row[d >= 2 ? d - 2 : 0];
+    const typename M::T q1 = M::encode(sf * m1), q2 = M::encode(sf * m2);
+    // d - 1 inputs: the result's sign bit is (d - 2) xor the parity of the others' sign bits.
+    const unsigned base = unsigned((d - 2) & 1) ^ par;
+    if (mine) {
+      typename M::T* cg = c2v + (int64_t(g) * p.E + e0) * kLanes + lane;
+#pragma unroll
+      for (int j = 0; j < DMAX; ++j) {
+        if (j < d) {
+          const typename M::T q = (j == i1) ? q2 : q1;
+          cg[j * kLanes] = (base ^ unsigned(ldpc::neg(v[j]))) ? M::negate(q) : q;
+        }
+      }
+    }
+    return;
+  }
   float out[DMAX];
   ldpc::row_update<ALG, DMAX>(c_lut, v, out, d, sf_row[d >= 2 ? d - 2 : 0]);
   if (mine) {

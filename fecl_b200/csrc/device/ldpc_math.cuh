@@ -37,13 +37,17 @@ __device__ __forceinline__ float phi(float x) { return log1pf(2.0f / expm1f(x));
 
 // Storage of check-to-bit messages: FP32 (reference parity), saturated FP16 (+-65504),
 // or saturated int8 in Q5.2 (step 1/4, range +-31.75).  Arithmetic is FP32 in every case.
+// encode() is odd -- encode(-x) == negate(encode(x)) bit for bit -- because rounding
+// to nearest (even) and the saturation bounds are symmetric in sign.
 template <int MSG>
 struct Msg;
 template <>
 struct Msg<0> {
   using T = float;
   __device__ static float load(const T* p) { return *p; }
-  __device__ static void store(T* p, float v) { *p = v; }
+  __device__ static T encode(float v) { return v; }
+  __device__ static T negate(T q) { return -q; }
+  __device__ static void store(T* p, float v) { *p = encode(v); }
   __device__ static float from_bits(uint32_t b) { return __uint_as_float(b); }
 };
 template <>
@@ -51,19 +55,42 @@ struct Msg<1> {
   using T = __half;
   __device__ static float load(const T* p) { return __half2float(*p); }
   // saturated at the largest finite FP16 value, so that no message becomes infinite
-  __device__ static void store(T* p, float v) { *p = __float2half_rn(fminf(fmaxf(v, -65504.0f), 65504.0f)); }
+  __device__ static T encode(float v) { return __float2half_rn(fminf(fmaxf(v, -65504.0f), 65504.0f)); }
+  __device__ static T negate(T q) { return __ushort_as_half((unsigned short)(__half_as_ushort(q) ^ 0x8000u)); }
+  __device__ static void store(T* p, float v) { *p = encode(v); }
   __device__ static float from_bits(uint32_t b) { return __half2float(__ushort_as_half((unsigned short)b)); }
 };
 template <>
 struct Msg<2> {
   using T = int8_t;
   __device__ static float load(const T* p) { return float(*p) * 0.25f; }
-  __device__ static void store(T* p, float v) {
-    const float q = fminf(fmaxf(rintf(v * 4.0f), -127.0f), 127.0f);
-    *p = int8_t(q);
-  }
+  __device__ static T encode(float v) { return int8_t(fminf(fmaxf(rintf(v * 4.0f), -127.0f), 127.0f)); }
+  __device__ static T negate(T q) { return int8_t(-q); }
+  __device__ static void store(T* p, float v) { *p = encode(v); }
   __device__ static float from_bits(uint32_t b) { return float(int8_t(uint8_t(b))) * 0.25f; }
 };
+
+// Min-sum scan of one row: the two smallest magnitudes m1 <= m2, the index of the
+// first smallest, and the parity of the inputs' sign bits.
+template <int DMAX>
+__device__ __forceinline__ void min_sum_scan(const float v[DMAX], int d, float& m1, float& m2, int& i1,
+                                             unsigned& par) {
+  m1 = INFINITY;
+  m2 = INFINITY;
+  i1 = 0;
+  par = 0;
+#pragma unroll
+  for (int j = 0; j < DMAX; ++j) {
+    if (j < d) {
+      const float a = fabsf(v[j]);
+      par ^= unsigned(neg(v[j]));
+      const bool lt1 = a < m1;
+      m2 = lt1 ? m1 : fminf(m2, a);
+      i1 = lt1 ? j : i1;
+      m1 = lt1 ? a : m1;
+    }
+  }
+}
 
 // One check row: v[0..d) in, out[0..d) = sf * extrinsic boxplus out.
 template <int ALG, int DMAX>
@@ -120,20 +147,10 @@ __device__ __forceinline__ void row_update(const LinearLut& lut, const float v[D
     // values bit for bit with a handful of registers.
     // Written with selects, not branches: lanes hold different frames, and a branch
     // on the data would split the warp at every edge.
-    float m1 = INFINITY, m2 = INFINITY;
-    int i1 = 0;
-    unsigned par = 0;
-#pragma unroll
-    for (int j = 0; j < DMAX; ++j) {
-      if (j < d) {
-        const float a = fabsf(v[j]);
-        par ^= unsigned(neg(v[j]));
-        const bool lt1 = a < m1;
-        m2 = lt1 ? m1 : fminf(m2, a);
-        i1 = lt1 ? j : i1;
-        m1 = lt1 ? a : m1;
-      }
-    }
+    float m1, m2;
+    int i1;
+    unsigned par;
+    min_sum_scan<DMAX>(v, d, m1, m2, i1, par);
     // d - 1 inputs: the result's sign bit is (d - 2) xor the parity of the others' sign bits.
     const unsigned base = unsigned((d - 2) & 1);
 #pragma unroll
