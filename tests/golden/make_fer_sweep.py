@@ -7,8 +7,8 @@ For each rate (1/2, 3/4, 9/10 of the DVB-S2 normal frame) and each Eb/N0 point
 (1.0 to 4.0 dB in 0.25 dB steps) it decodes the 512 seeded frames with normalised
 min-sum (0.75, at most 50 iterations, syndrome stop), from the FP32-rounded
 L-values the GPU decoders see, and records which frames fail (packed bit flags).
-GPU decoders at FP32, FP16 and int8 message precision are compared with these
-flags, on the box where the reference is not available.
+The GPU tests compare the decoders at FP32, FP16 and int8 message precision with
+these flags, so they need neither the reference sources nor its compiled library.
 
 The reference's own DVB-S2 builder is correct only for (64800, 1/2), so the check
 matrix given to it is the standard one from fecl_b200's tables (identical edge for
