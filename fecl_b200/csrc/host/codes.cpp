@@ -139,6 +139,14 @@ void LdpcCode::compute_generator(Csr Hin) {
   std::vector<uint64_t> weight(N, 0);
   for (auto& row : rows)
     for (auto c : row) weight[c]++;
+  // The rows holding each column, by row identity, and each row's position, so that
+  // retiring a column visits only the rows that hold it.
+  std::vector<std::vector<uint32_t>> col_rows(N);
+  for (uint32_t r = 0; r < R; ++r)
+    for (auto c : rows[r]) col_rows[c].push_back(r);
+  std::vector<uint32_t> row_id(R), row_pos(R);
+  for (uint32_t r = 0; r < R; ++r) row_id[r] = row_pos[r] = r;
+  std::vector<uint32_t> holding;
   uint64_t active = R;
   int64_t retired_cursor = int64_t(R) - 1;
   uint64_t t = 0;
@@ -158,17 +166,35 @@ void LdpcCode::compute_generator(Csr Hin) {
         best = weight[j];
       }
     }
-    if (best_idx != i - 1)
+    if (best_idx != i - 1) {
       for (auto& row : rows) row_swap_cols(row, uint32_t(best_idx), uint32_t(i - 1));
+      std::swap(col_rows[best_idx], col_rows[i - 1]);
+    }
     std::swap(weight[best_idx], weight[i - 1]);
-    // Active rows holding column i-1 go to the end of the active block.
-    int64_t end = int64_t(active);
-    for (int64_t r = 0; r < end; ++r) {
-      if (row_has(rows[r], uint32_t(i - 1))) {
-        --end;
+    // Active rows holding column i-1 go to the end of the active block, as the
+    // reference's scan moves them: positions are visited in increasing order, and a
+    // row holding the column is swapped with the last active row, whose replacement
+    // at that position is examined next.  `holding` lists, in increasing order, the
+    // active positions whose row holds the column; its front is the scan's next stop,
+    // and the swapped-in row holds the column exactly when its position is the back.
+    holding.clear();
+    for (uint32_t rid : col_rows[i - 1])
+      if (row_pos[rid] < active) holding.push_back(row_pos[rid]);
+    std::sort(holding.begin(), holding.end());
+    uint64_t end = active;
+    size_t lo = 0, hi = holding.size();
+    while (lo < hi) {
+      const uint32_t r = holding[lo];
+      --end;
+      const bool end_holds = holding[hi - 1] == end;
+      if (end != r) {
         std::swap(rows[end], rows[r]);
-        --r;
+        std::swap(row_id[end], row_id[r]);
+        row_pos[row_id[end]] = uint32_t(end);
+        row_pos[row_id[r]] = r;
       }
+      if (end_holds && end != r) --hi;  // position r now holds the row from the end
+      else ++lo;
     }
     active -= std::max<uint64_t>(best, 1);
     if (active == 0) {
