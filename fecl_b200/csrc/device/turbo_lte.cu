@@ -257,7 +257,6 @@ struct Shared {
   float term[8];          // trellis termination: state 0
   int bad[2][kSegs];
   int any_bad;
-  float etail[2][4];
   uint32_t crc_part[kThreads / 32];  // per-warp CRC syndromes
 };
 
@@ -397,6 +396,7 @@ template <int ALG>
 __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
   const int K = q.K, T = q.K + 3;
   const int nblk = (T + kBlk - 1) / kBlk;
+  const int nblk_msg = (K + kBlk - 1) / kBlk;
   float* X = smem;
   float* Y = smem + q.Kp;
   Shared& sh = *reinterpret_cast<Shared*>(smem + 2 * q.Kp);
@@ -493,10 +493,13 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
         atomicAdd(q.stats + 0, 1ull);
         atomicAdd(q.stats + 1, (unsigned long long)rounds);
       }
-      // ---- B: 8-step blocks, extrinsic output
+      // ---- B: 8-step blocks, extrinsic output.  Only blocks holding message steps
+      // run: the tail steps' a-priori values are the channel's tail bits, so their
+      // extrinsic values are never read (with K a multiple of 8, as every LTE size
+      // is, the last block is all tail).
       const float sf = q.sf[j * q.iterations + it];
       float* out = j == 0 ? X : Y;
-      for (int b = tid; b < nblk; b += kThreads) {
+      for (int b = tid; b < nblk_msg; b += kThreads) {
         const int t0 = b * kBlk;
         const int n = min(kBlk, T - t0);
         float al[kBlk][8];
@@ -543,8 +546,6 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
             if (t < K) {
               if (j == 0) out[t] = fr.Ls[t] + ext[i];
               else out[perm[t]] = ext[i];
-            } else {
-              sh.etail[j][t - K] = ext[i];
             }
           }
         }
