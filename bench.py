@@ -192,18 +192,38 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows), "source": "nvidia-smi"}
 
 
+def channel_module():
+    """The seeded channel model (fecl_b200/channel.py, plain numpy), loaded from its
+    file so that the reference arm imports nothing that loads the GPU library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_fecl_channel", os.path.join(ROOT, "fecl_b200", "channel.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+APPROXIMATE, SERIAL = 2, 0  # fec::DecoderAlgorithm::Approximate, fec::SchedulingType::Serial
+
+
+def reference_lte_codec(workgroup):
+    """The reference's LTE turbo codec (oracle/_ref): RSC (13, 15) twice, the QPP
+    interleaver of its own Lte3Gpp table, Tail termination, max-log-MAP, serial."""
+    import numpy as np
+    from oracle import ref
+    return ref.RefCodec.turbo([([4], [[0o15]], [0o13])], [np.arange(K), ref.lte_interleaver(K)], 0,
+                              APPROXIMATE, SERIAL, ITERATIONS, workgroup=workgroup)
+
+
 def cpu_reference(frames_sample, llr, code_sizes):
     """Time the reference FeCl decoder (oracle/_ref) with all host threads on a
     bounded sample of the workload.  Falls back to the C restatement of the oracle."""
     import numpy as np
     from oracle import ref
-    import fecl_b200 as F
     cores = os.cpu_count() or 1
     n = frames_sample
     x = np.ascontiguousarray(llr[: n * code_sizes["parity"]], dtype=np.float64)
     if ref.available():
-        rc = ref.RefCodec.turbo([([4], [[0o15]], [0o13])], [np.arange(K), F.Turbo.Lte3Gpp.interleaver(K)], 0,
-                                F.Approximate, F.Serial, ITERATIONS, workgroup=cores)
+        rc = reference_lte_codec(cores)
         t = time.perf_counter()
         bits = rc.decode(x)
         dt = time.perf_counter() - t
@@ -213,7 +233,7 @@ def cpu_reference(frames_sample, llr, code_sizes):
         if not restated.available():
             return None, None
         t = time.perf_counter()
-        bits, _ = restated.turbo_lte_decode(K, F.Approximate, ITERATIONS, F.Serial, x, threads=cores)
+        bits, _ = restated.turbo_lte_decode(K, APPROXIMATE, ITERATIONS, SERIAL, x, threads=cores)
         dt = time.perf_counter() - t
         kind = "port"
     return {"value": n * K / dt / 1e6, "unit": "Mbit/s", "cores": cores, "kind": kind,
@@ -228,20 +248,25 @@ def dist_setup():
 
 
 def run_reference_arm(args):
+    """The reference's own decoder (compiled from its sources into oracle/_ref) on the
+    host cores.  The inputs come from the reference's encoder and interleaver and the
+    numpy channel model, so this arm loads nothing of this repository's library."""
     world, rank, local = dist_setup()
     if rank != 0:
         return 0
     import numpy as np
-    import fecl_b200 as F
     from oracle import ref
-    code = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(ITERATIONS).scheduling(F.Serial))
-    sizes = {"parity": code.paritySize()}
-    cores = os.cpu_count() or 1
-    sample = max(8, min(FRAMES, cores * 8))
-    msg, llr = make_inputs(code, sample, SEED)
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfecl_ref.so was not built on this machine"}))
         return 0
+    ch = channel_module()
+    parity = 3 * K + 12
+    sizes = {"parity": parity}
+    cores = os.cpu_count() or 1
+    sample = max(8, min(FRAMES, cores * 8))
+    msg = ch.random_bits(sample * K, SEED)
+    cw = reference_lte_codec(cores).encode(msg)
+    llr = ch.awgn_llr(cw, EBN0_DB, K / parity, SEED, np.float32)
     vals = []
     for i in range(args.warmup + args.steps):
         cb, _ = cpu_reference(sample, llr, sizes)
@@ -279,14 +304,8 @@ LDPC_WORKLOADS = {
 PRECISIONS = {"f32": 0, "f16": 1, "i8": 2}
 
 
-def ldpc_algorithmic_bytes(N, E, K, iterations_run, s_llr, s_msg, soft):
-    """Flooding BP with message state in memory: the L-values once; per iteration each
-    check-to-bit message read and written once and each bit posterior read and written
-    once (FP32); the decoded bits (or a-posteriori values) once."""
-    return N * s_llr + iterations_run * (2 * E * s_msg + 2 * N * 4) + (K * 8 if soft else K)
-
-
-def run_ldpc(args):
+def run_ldpc(args, embedded=False):
+    """LDPC workloads; with `embedded` the line is returned instead of printed."""
     import numpy as np
     import torch
     from fractions import Fraction
@@ -430,6 +449,8 @@ def run_ldpc(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"], line["matched_hard_decisions_vs_reference"] = ldpc_cpu_reference(w, jobs)
+    if embedded:
+        return line
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:
@@ -533,6 +554,48 @@ def mixed_inputs(reqs, codes, seed):
     return out
 
 
+def build_mixed_batch(inputs, codes, autotune=True):
+    """One F.Batch over mixed requests: one job per code, its frames' L-values
+    contiguous in one device buffer, decisions and iteration counts likewise."""
+    import numpy as np
+    import torch
+    import fecl_b200 as F
+    by_key = {}
+    for idx, (key, msg, llr) in enumerate(inputs):
+        by_key.setdefault(key, []).append(idx)
+    keys = sorted(by_key, key=str)
+    llr_host = np.concatenate([inputs[i][2] for k in keys for i in by_key[k]])
+    msg_ref = [np.concatenate([inputs[i][1] for i in by_key[k]]) for k in keys]
+    d_llr = torch.from_numpy(llr_host).cuda()
+    n_bits_out = sum(codes.get(k).msgSize() * len(by_key[k]) for k in keys)
+    d_msg = torch.zeros(n_bits_out, dtype=torch.uint8, device="cuda")
+    d_its = torch.zeros(len(inputs), dtype=torch.int32, device="cuda")
+    jobs, lo, mo, fo = [], 0, 0, 0
+    for k in keys:
+        c, n = codes.get(k), len(by_key[k])
+        jobs.append((c, d_llr[lo:lo + n * c.paritySize()], d_msg[mo:mo + n * c.msgSize()], d_its[fo:fo + n]))
+        lo += n * c.paritySize()
+        mo += n * c.msgSize()
+        fo += n
+    t0 = time.perf_counter()
+    batch = F.Batch(jobs, autotune=autotune)
+    build_s = time.perf_counter() - t0
+    return {"by_key": by_key, "keys": keys, "llr_host": llr_host, "msg_ref": msg_ref, "d_llr": d_llr, "d_msg": d_msg,
+            "d_its": d_its, "n_bits_out": n_bits_out, "batch": batch, "build_s": build_s}
+
+
+def batch_frame_errors(mb, codes):
+    """Frames of a mixed batch whose decisions differ from their message bits."""
+    import numpy as np
+    bits = mb["d_msg"].cpu().numpy()
+    errs, mo = 0, 0
+    for k, ref in zip(mb["keys"], mb["msg_ref"]):
+        K, n = codes.get(k).msgSize(), len(mb["by_key"][k])
+        errs += int(np.sum(np.any(bits[mo:mo + n * K].reshape(n, K) != ref.reshape(n, K), axis=1)))
+        mo += n * K
+    return errs
+
+
 def run_mixed(args):
     import numpy as np
     import torch
@@ -550,27 +613,10 @@ def run_mixed(args):
     reqs = mixed_requests(total, SEED + rank)
     codes = MixedCodes(prec)
     inputs = mixed_inputs(reqs, codes, SEED + rank)
-    # one job per code: its frames' L-values contiguous in one device buffer
-    by_key = {}
-    for idx, (key, msg, llr) in enumerate(inputs):
-        by_key.setdefault(key, []).append(idx)
-    keys = sorted(by_key, key=str)
-    llr_host = np.concatenate([inputs[i][2] for k in keys for i in by_key[k]])
-    msg_ref = [np.concatenate([inputs[i][1] for i in by_key[k]]) for k in keys]
-    d_llr = torch.from_numpy(llr_host).cuda()
-    n_bits_out = sum(codes.get(k).msgSize() * len(by_key[k]) for k in keys)
-    d_msg = torch.zeros(n_bits_out, dtype=torch.uint8, device="cuda")
-    d_its = torch.zeros(total, dtype=torch.int32, device="cuda")
-    jobs, lo, mo, fo = [], 0, 0, 0
-    for k in keys:
-        c, n = codes.get(k), len(by_key[k])
-        jobs.append((c, d_llr[lo:lo + n * c.paritySize()], d_msg[mo:mo + n * c.msgSize()], d_its[fo:fo + n]))
-        lo += n * c.paritySize()
-        mo += n * c.msgSize()
-        fo += n
-    t0 = time.perf_counter()
-    batch = F.Batch(jobs, autotune=not args.no_autotune)
-    build_s = time.perf_counter() - t0
+    mb = build_mixed_batch(inputs, codes, autotune=not args.no_autotune)
+    by_key, keys, llr_host, msg_ref = mb["by_key"], mb["keys"], mb["llr_host"], mb["msg_ref"]
+    d_llr, d_msg, d_its, n_bits_out = mb["d_llr"], mb["d_msg"], mb["d_its"], mb["n_bits_out"]
+    batch, build_s = mb["batch"], mb["build_s"]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
 
@@ -720,7 +766,7 @@ def run_mixed(args):
 SERVING_RATES = [1000, 5000, 20000, 50000, 100000, 200000]
 
 
-def run_serving(args):
+def run_serving(args, embedded=False):
     """Poisson request streams at SERVING_RATES frames/s against the decode server
     (one frame per request, the mix of the mixed batch: 50 % LTE turbo, 40 % DVB-S2
     short, 10 % DVB-S2 normal, Eb/N0 U(0.5, 3.0), FP16 L-values, 40 GiB admission
@@ -781,6 +827,25 @@ def run_serving(args):
     perr = sum(int(np.any(o != m)) for o, (_, m, _) in zip(pouts, sample))
     plain = {"value": round(sum(m.size for _, m, _ in sample) / pt / 1e6, 2), "unit": "Mbit/s", "frames": len(sample),
              "fer": round(perr / len(sample), 4), "what": "one decode call per frame, FP32 messages, host L-values"}
+
+    # the same pool decoded as one batch with FP32 LDPC messages (not served): what
+    # batching alone gives at FP32, against which the FP16 server is also compared
+    mb = build_mixed_batch(pool, pcodes, autotune=False)
+    mb["batch"].run()
+    torch.cuda.synchronize()
+    bts = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        mb["batch"].run()
+        e1.record()
+        e1.synchronize()
+        bts.append(e0.elapsed_time(e1))
+    pool_bits = sum(m.size for _, m, _ in pool)
+    batched = {"value": round(pool_bits / (statistics.median(bts) * 1e-3) / 1e6, 2), "unit": "Mbit/s",
+               "frames": len(pool), "fer": round(batch_frame_errors(mb, pcodes) / len(pool), 4),
+               "what": "the whole pool as one batch (one CUDA graph), FP32 LDPC messages, device-resident L-values"}
+    del mb
     line = {
         "metric": METRIC, "value": peak["sustained_info_mbps"], "unit": "Mbit/s", "n_gpus": 1, "steps": len(SERVING_RATES),
         "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -796,9 +861,12 @@ def run_serving(args):
         "e2e": {"value": peak["sustained_info_mbps"], "unit": "Mbit/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                 "note": "every request goes host -> device -> host through the server"},
         "plain_per_request_fp32": plain,
+        "batched_fp32": batched,
         "speedup_vs_plain_per_request": round(peak["sustained_info_mbps"] / plain["value"], 1),
         "gpu_launches": None,
     }
+    if embedded:
+        return line
     print(json.dumps(line))
     return 0
 
@@ -905,6 +973,30 @@ def run_fer_sweep(args):
     return 0
 
 
+def extra_workloads(args):
+    """The other configurations of the metric, measured in the default run so that
+    every one of them is on record: DVB-S2 short-frame Exact BP (64 frames, FP64
+    L-values, soft output), DVB-S2 normal frames with FP16 messages (3 x 512 frames,
+    normalised min-sum) and the decode server under Poisson load, each bounded to a
+    few seconds of GPU time."""
+    import argparse
+    out = {}
+    base = dict(vars(args))
+    base.update(frames=0, kernel="auto", cluster=0, threads=0, wave=0, profile_decodes=0, warmup=3)
+    l1 = run_ldpc(argparse.Namespace(**dict(base, workload="ldpc-short", precision="f32", steps=10)), embedded=True)
+    l3 = run_ldpc(argparse.Namespace(**dict(base, workload="ldpc-normal", precision="f16", steps=5,
+                                            no_cpu_baseline=True)), embedded=True)
+    keep = ("value", "unit", "ms_per_step", "dtype", "config", "e2e", "roofline", "latency_ms", "clocks",
+            "cpu_baseline", "matched_hard_decisions_vs_reference")
+    out["ldpc"] = {"short_exact_f64_x64": {k: l1[k] for k in keep if k in l1},
+                   "normal_nms_f16_3x512": {k: l3[k] for k in keep if k in l3}}
+    sv = run_serving(argparse.Namespace(**dict(base, serve_seconds=0.25, serve_slots=3, serve_batch=2048,
+                                               plain_sample=256)), embedded=True)
+    out["serving"] = {k: sv[k] for k in ("value", "unit", "config", "serving", "latency_ms", "plain_per_request_fp32",
+                                         "batched_fp32", "speedup_vs_plain_per_request") if k in sv}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -929,6 +1021,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=0.25, help="serving: seconds of arrivals per rate")
     ap.add_argument("--serve-slots", type=int, default=3, help="serving: batches in flight")
     ap.add_argument("--serve-batch", type=int, default=2048, help="serving: frames per batch at most")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="lte-turbo: skip the LDPC and serving figures added to the default line")
     ap.add_argument("--profile-decodes", type=int, default=0,
                     help="only run this many decodes of the workload (for ncu captures) and exit")
     args = ap.parse_args()
@@ -1045,6 +1139,8 @@ def main():
         line["cpu_baseline"] = cb
         if ref_bits is not None:
             line["matched_hard_decisions_vs_reference"] = bool(np.array_equal(ref_bits, bits))
+    if world == 1 and not args.no_extras:
+        line.update(extra_workloads(args))
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

@@ -73,14 +73,14 @@ extern "C" int fecl_lte_turbo_decode_noalloc(uint32_t K, int32_t algorithm, uint
     return fail(FECL_EINVAL, "Invalid element type");
   if (nframes == 0) return FECL_OK;
   if (!llr || !msg) return fail(FECL_EINVAL, "null buffer");
-  const size_t need = fecl::turbo_lte_scratch_bytes(int(K), int64_t(nframes));
-  if (need > kScratchBytes) {
-    const size_t per_frame = fecl::turbo_lte_scratch_bytes(int(K), 1);
-    return fail(FECL_EINVAL, "batch needs " + std::to_string(need) + " bytes of scratch, more than the " +
-                                 std::to_string(kScratchBytes) + " bytes reserved; at most " +
-                                 std::to_string(kScratchBytes / per_frame) + " frames of K=" + std::to_string(K) +
-                                 " per call");
-  }
+  // The frame count is compared with the capacity before any multiplication, so no
+  // count, however large, can wrap the byte size into range.
+  const size_t per_frame = fecl::turbo_lte_scratch_bytes(int(K), 1);
+  const uint64_t max_frames = kScratchBytes / per_frame;
+  if (nframes > max_frames)
+    return fail(FECL_EINVAL, std::to_string(nframes) + " frames of K=" + std::to_string(K) + " need more than the " +
+                                 std::to_string(kScratchBytes) + " bytes of scratch reserved; at most " +
+                                 std::to_string(max_frames) + " frames of K=" + std::to_string(K) + " per call");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(FECL_ENODEV, std::string("cudaGetDevice: ") + cudaGetErrorString(e));

@@ -94,7 +94,12 @@ def _wrap(values, per_line=12):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) > 1:
+        ref = sys.argv[1]
+    elif os.environ.get("FECL_REFERENCE_DIR"):
+        ref = os.environ["FECL_REFERENCE_DIR"]
+    else:
+        sys.exit("usage: extract_tables.py <reference source tree> (or set FECL_REFERENCE_DIR)")
     here = os.path.dirname(os.path.abspath(__file__))
     codes, rows, addrs = dvbs2(ref)
     with open(os.path.join(here, "dvbs2_tables.h"), "w") as f:

@@ -102,3 +102,14 @@ def test_decode_without_gpu_reports_no_device():
     t = F.Turbo.lte(40)
     with pytest.raises(F.FeclError):
         t.decode(np.zeros(t.paritySize()))
+
+
+def test_noalloc_rejects_a_frame_count_that_would_wrap_the_scratch_size():
+    """A frame count whose byte size wraps around 2^64 (K=40: 1056 B a frame, so
+    2^59 + 1 frames wrap to 1056 B) must be rejected before anything is launched."""
+    from fecl_b200 import _lib
+    dummy = C.c_void_p(256)  # never dereferenced: the call returns before any device work
+    for K, n in ((40, (1 << 59) + 1), (6144, (1 << 64) - 1), (6144, 69)):
+        rc = _lib.lib.fecl_lte_turbo_decode_noalloc(K, 2, 6, dummy, _lib.F32, n, dummy, None)
+        assert rc == _lib.EINVAL, (K, n, rc)
+        assert b"scratch" in _lib.lib.fecl_last_error()
