@@ -589,6 +589,12 @@ class Ldpc(Codec):
         _check(_L.fecl_ldpc_set_wave(self._h, int(groups)))
         return self
 
+    def setPersistent(self, mode=0):
+        """Extension: run small batches as one persistent launch (1: wherever it
+        applies, 0: built-in choice, -1: never); results are identical either way."""
+        _check(_L.fecl_ldpc_set_persistent(self._h, int(mode)))
+        return self
+
     def checks(self):
         """The transformed check matrix (detail::Ldpc::Structure::checks); its edge
         order is the layout of the soft state."""
@@ -805,6 +811,11 @@ class Turbo(Codec):
         """Extension: training steps of the windowed LTE decoder (multiple of 8, -1 default)."""
         _check(_L.fecl_turbo_set_window_training(self._h, int(steps)))
 
+    def setWindowSegments(self, segments):
+        """Extension: forward/backward segments per frame of the windowed LTE decoder
+        (32 or 64, 0 for the built-in choice)."""
+        _check(_L.fecl_turbo_set_window_segments(self._h, int(segments)))
+
     def windowStats(self):
         """Extension: (passes, fix-up rounds, recomputed segments) since the last call."""
         a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
@@ -970,9 +981,10 @@ class Batch:
     uint8, iterations [nframes] int32.  The tensors stay bound to the batch: write new
     L-values into them and call run() again.  Results equal each codec's decode()
     bit for bit.  autotune=True times the equivalent LDPC kernel shapes on these
-    inputs at creation and keeps the fastest."""
+    inputs at creation and keeps the fastest.  shared_ldpc=False gives every LDPC job
+    its own launches instead of the shared persistent launch (same results)."""
 
-    def __init__(self, jobs, autotune=False):
+    def __init__(self, jobs, autotune=False, shared_ldpc=True):
         self._keep = []
         arr = (_lib.fecl_batch_job * len(jobs))()
         for i, job in enumerate(jobs):
@@ -993,7 +1005,8 @@ class Batch:
             arr[i].iterations = it.data_ptr() if it is not None else None
             self._keep.append((codec, llr, msg, it))
         h = C.c_void_p()
-        _check(_L.fecl_batch_create(arr, len(jobs), _lib.BATCH_AUTOTUNE if autotune else 0, C.byref(h)))
+        flags = (_lib.BATCH_AUTOTUNE if autotune else 0) | (0 if shared_ldpc else _lib.BATCH_PER_JOB)
+        _check(_L.fecl_batch_create(arr, len(jobs), flags, C.byref(h)))
         self._h = h
         self._device = jobs[0][1].device
 

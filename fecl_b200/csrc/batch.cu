@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "codec.hpp"
+#include "ldpc_shared.hpp"
 
 namespace {
 
@@ -166,6 +167,7 @@ struct JobState {
   const fecl_batch_job* job;
   fecl_codec_s* c;
   bool lte = false;
+  bool multi = false;  // in the shared persistent LDPC launch
   Choice choice;
   ScratchPlan sp;
   size_t off = 0;  // scratch offset in the workspace
@@ -222,7 +224,7 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
     if (!out) fail(FECL_EINVAL, "null output");
     *out = nullptr;
     if (!jobs || njobs == 0) fail(FECL_EINVAL, "empty batch");
-    if (flags & ~FECL_BATCH_AUTOTUNE) fail(FECL_EINVAL, "Invalid batch flags");
+    if (flags & ~(FECL_BATCH_AUTOTUNE | FECL_BATCH_PER_JOB)) fail(FECL_EINVAL, "Invalid batch flags");
     std::vector<JobState> js(njobs);
     std::set<fecl_codec_s*> codecs;
     for (uint32_t i = 0; i < njobs; ++i) {
@@ -284,6 +286,10 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
     std::ostringstream plan;
     for (auto& s : js) {
       if (s.lte) continue;
+      if (!(flags & FECL_BATCH_PER_JOB) && SharedLdpc::eligible(s.c)) {
+        s.multi = true;
+        continue;
+      }
       if ((flags & FECL_BATCH_AUTOTUNE) && s.c->kind == 0 && s.c->kernel_sel == FECL_KERNEL_AUTO) {
         const std::string key = signature(s.c, s.job->nframes, s.job->llr_dtype);
         bool found = false;
@@ -318,8 +324,24 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
 
     // ---- 3. workspace: job scratch | turbo frame scratch | descriptors | counters
     Carver cv;
-    for (auto& s : js)
-      if (!s.lte) s.off = cv.take(s.sp.bytes);
+    SharedLdpc shared;
+    for (auto& s : js) {
+      if (s.lte) continue;
+      if (s.multi) {
+        SharedLdpcJob j;
+        j.c = s.c;
+        j.n = s.job->nframes;
+        j.llr = s.job->llr;
+        j.dtype = s.job->llr_dtype;
+        j.msg = s.job->msg;
+        j.iters = s.job->iterations;
+        j.scratch_off = cv.take(SharedLdpc::scratch_bytes(j));
+        shared.jobs.push_back(j);
+      } else {
+        s.off = cv.take(s.sp.bytes);
+      }
+    }
+    shared.plan(cv);
     std::map<int, size_t> desc_off, cnt_off;
     std::vector<std::pair<size_t, size_t>> frame_scratch;  // per turbo frame: offset
     for (auto& kv : tframes) {
@@ -342,6 +364,12 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
                             cudaMemcpyHostToDevice),
                  "upload descriptors");
     }
+    if (!shared.empty()) {
+      const size_t t0 = shared.tables_begin(), t1 = shared.tables_end();
+      std::vector<char> image(t1);
+      shared.fill(base, image.data());
+      cuda_check(cudaMemcpy(base + t0, image.data() + t0, t1 - t0, cudaMemcpyHostToDevice), "upload LDPC tables");
+    }
 
     // ---- 4. capture
     cuda_check(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
@@ -358,10 +386,17 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
         cuda_check(fecl::launch_turbo_lte_batch(p, b->cap), "turbo batch launch");
         plan << "turbo LTE mixed-K x" << kv.second.size() << " (alg " << kv.first << ", max K " << p.max_K << ")\n";
       }
-      int branch = 0;
+      // the shared LDPC launches on branch 0: stage every job, run every class, finish
+      // every job
+      if (!shared.empty()) {
+        shared.launch(base, b->cap2[0]);
+        plan << shared.describe();
+      }
+      const int first = shared.empty() ? 0 : 1;  // branch 0 holds the shared launches
+      int k = 0;
       for (auto& s : js) {
-        if (s.lte) continue;
-        cudaStream_t st = b->cap2[branch++ % kBranches];
+        if (s.lte || s.multi) continue;
+        cudaStream_t st = b->cap2[first + k++ % (kBranches - first)];
         ChoiceScope scope(s.c, s.choice);
         Launch d;
         d.llr = s.job->llr;

@@ -197,6 +197,42 @@ ScratchPlan plan_scratch(fecl_codec_s* c, uint64_t n, bool lte_fast) {
   return sp;
 }
 
+fecl::LdpcLanesParams lanes_params(fecl_codec_s* c, const Launch& d, uint64_t n, int32_t in_dtype, int32_t out_dtype) {
+  fecl::LdpcLanesParams r;
+  const auto& L = c->ldev;
+  r.M = L.M;
+  r.N = L.N;
+  r.msg = L.msg;
+  r.d_max = L.d_max;
+  r.E = L.E;
+  r.row_ptr = L.row_ptr;
+  r.col_idx = L.col_idx;
+  r.col_ptr = L.col_ptr;
+  r.col_edges = L.col_edges;
+  r.sf = L.sf;
+  r.n_sf = L.n_sf;
+  r.sf_stride = L.sf_stride;
+  r.algorithm = L.algorithm;
+  r.iterations = L.iterations;
+  r.fixed_iterations = L.fixed_iterations;
+  r.msg_type = c->ldpc->decoder().precision;
+  r.wave_groups = c->lanes_wave;
+  r.persist = c->lanes_persist;
+  r.nframes = int64_t(n);
+  r.llr = d.llr;
+  r.llr_dtype = in_dtype;
+  r.syst_in = d.syst;
+  r.state_in = d.state;
+  r.hard = d.hard;
+  r.iters = d.iters;
+  r.msg_out = d.msg;
+  r.syst_out = d.syst_out;
+  r.parity_out = d.parity_out;
+  r.state_out = d.state_out;
+  r.out_dtype = out_dtype;
+  return r;
+}
+
 void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint64_t n, int32_t in_dtype,
                    int32_t out_dtype, bool soft, bool lte_fast, cudaStream_t s) {
   cudaError_t e;
@@ -271,37 +307,7 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
     r.out_dtype = out_dtype;
     e = fecl::launch_ldpc_cluster(r, s);
   } else if (c->kind == 0 && c->ldpc_lanes_ok()) {
-    fecl::LdpcLanesParams r;
-    const auto& L = c->ldev;
-    r.M = L.M;
-    r.N = L.N;
-    r.msg = L.msg;
-    r.d_max = L.d_max;
-    r.E = L.E;
-    r.row_ptr = L.row_ptr;
-    r.col_idx = L.col_idx;
-    r.col_ptr = L.col_ptr;
-    r.col_edges = L.col_edges;
-    r.sf = L.sf;
-    r.n_sf = L.n_sf;
-    r.sf_stride = L.sf_stride;
-    r.algorithm = L.algorithm;
-    r.iterations = L.iterations;
-    r.fixed_iterations = L.fixed_iterations;
-    r.msg_type = c->ldpc->decoder().precision;
-    r.wave_groups = c->lanes_wave;
-    r.nframes = int64_t(n);
-    r.llr = d.llr;
-    r.llr_dtype = in_dtype;
-    r.syst_in = d.syst;
-    r.state_in = d.state;
-    r.hard = d.hard;
-    r.iters = d.iters;
-    r.msg_out = d.msg;
-    r.syst_out = d.syst_out;
-    r.parity_out = d.parity_out;
-    r.state_out = d.state_out;
-    r.out_dtype = out_dtype;
+    const fecl::LdpcLanesParams r = lanes_params(c, d, n, in_dtype, out_dtype);
     if (c->ldpc_h2_ok() && !d.state) e = fecl::launch_ldpc_lanes_h2(r, at(sp.o1), s);
     else e = fecl::launch_ldpc_lanes(r, at(sp.o1), s);
   } else if (c->kind == 0) {
@@ -331,6 +337,7 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
     r.iterations = c->tdev.iterations;
     r.algorithm = c->tdev.algorithm;
     r.train = c->lte_train;
+    r.segs = c->lte_segs;
     r.perm[0] = c->tdev.c[0].perm;
     r.perm[1] = c->tdev.c[1].perm;
     r.sf = c->tdev.sf;
@@ -949,6 +956,16 @@ int fecl_ldpc_set_wave(fecl_codec_t codec, int32_t groups) {
   });
 }
 
+int fecl_ldpc_set_persistent(fecl_codec_t codec, int32_t mode) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 0) fail(FECL_EINVAL, "not an LDPC codec");
+    if (mode < -1 || mode > 1) fail(FECL_EINVAL, "persistent mode must be -1, 0 or 1");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->lanes_persist = mode;
+  });
+}
+
 int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps) {
   return guarded([&] {
     auto c = checked(codec);
@@ -956,6 +973,16 @@ int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps) {
     if (steps != -1 && (steps < 0 || steps % 8 != 0 || steps > 4096)) fail(FECL_EINVAL, "training steps must be a multiple of 8");
     std::lock_guard<std::mutex> lk(c->mu);
     c->lte_train = steps;
+  });
+}
+
+int fecl_turbo_set_window_segments(fecl_codec_t codec, int32_t segments) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 1) fail(FECL_EINVAL, "not a turbo codec");
+    if (segments != 0 && segments != 32 && segments != 64) fail(FECL_EINVAL, "window segments must be 0, 32 or 64");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->lte_segs = segments;
   });
 }
 

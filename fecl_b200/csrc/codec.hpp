@@ -339,6 +339,7 @@ struct fecl_codec_s {
   bool on_device = false;
   std::atomic<uint64_t> generation{0};  // bumped whenever the decoder options (and their device tables) change
   int lte_train = -1;
+  int lte_segs = 0;  // windowed LTE decoder: segments per direction (0: built-in choice)
   int kernel_sel = FECL_KERNEL_AUTO;
   bool force_generic_() const { return kernel_sel == FECL_KERNEL_GENERIC; }
 
@@ -352,6 +353,7 @@ struct fecl_codec_s {
   std::map<uint32_t, std::unique_ptr<ClusterDev>> cplans;
   int cluster_size_sel = 0, cluster_threads_sel = 0;  // 0: chosen by the heuristic
   int lanes_wave = 0;                                 // 0: chosen by the launcher
+  int lanes_persist = 0;                              // persistent launch: 0 where it pays, 1 where it applies, -1 never
   int smem_optin = 0, sm_count = 0;
 
   ClusterDev& cluster_plan(uint32_t C) {
@@ -487,6 +489,9 @@ struct ScratchPlan {
 // The kernel and scratch for a batch of n frames of codec c (lte_fast: the windowed
 // LTE turbo kernel applies).
 ScratchPlan plan_scratch(fecl_codec_s* c, uint64_t n, bool lte_fast);
+// The lane-batched LDPC decoder's parameters for n frames of codec c (pointers in d
+// are device memory); the launcher fills the scratch layout.
+fecl::LdpcLanesParams lanes_params(fecl_codec_s* c, const Launch& d, uint64_t n, int32_t in_dtype, int32_t out_dtype);
 // Launches the decode of n frames on stream s; pointers in d are device memory.
 void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint64_t n, int32_t in_dtype,
                    int32_t out_dtype, bool soft, bool lte_fast, cudaStream_t s);

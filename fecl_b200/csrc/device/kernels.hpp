@@ -60,6 +60,7 @@ struct LdpcLanesParams {
   int32_t algorithm = 2, iterations = 1, fixed_iterations = 0;
   int32_t msg_type = 0;  // 0 FP32, 1 FP16, 2 saturated int8 (Q5.2)
   int32_t wave_groups = 0;  // groups decoded together (0: as many as fit in 64 MiB of L2)
+  int32_t persist = 0;      // one persistent launch for small batches: 0 where it pays, 1 wherever it applies, -1 never
   // batch, frame-major caller buffers
   int64_t nframes = 0;
   const void* llr = nullptr;
@@ -81,15 +82,44 @@ struct LdpcLanesParams {
   uint32_t* active = nullptr;
   uint32_t* fail = nullptr;
   int32_t* iters_ws = nullptr;
+  unsigned* barrier = nullptr;  // [2] grid barrier counter and failure flag of the persistent launch
 };
 
 size_t ldpc_lanes_scratch_bytes(int64_t N, int64_t E, int64_t nframes, int msg_type);
+// Cooperative launch of a persistent LDPC kernel, ordered after the previous one on
+// this device (ldpc_lanes.cu).
+cudaError_t ldpc_persist_launch(cudaStream_t s, const void* kern, unsigned blocks, unsigned threads, void** args);
 cudaError_t launch_ldpc_lanes(LdpcLanesParams p, void* scratch, cudaStream_t stream);
 
 // Normalised min-sum with FP16 messages and packed half2 check-node arithmetic, two
 // frames per lane (ldpc_lanes_h2.cu).  Takes no soft state input.
 size_t ldpc_lanes_h2_scratch_bytes(int64_t N, int64_t E, int64_t nframes);
 cudaError_t launch_ldpc_lanes_h2(LdpcLanesParams p, void* scratch, cudaStream_t stream);
+
+// The packed FP16 decoder over several codes in one persistent launch (a mixed
+// batch's LDPC jobs of one check-degree class: d_max <= 8, <= 16 or <= 32): every
+// job keeps its own layout (ldpc_lanes_h2_layout over its scratch), staged and
+// finished by its own launches; the iterations of all of them run in one
+// cooperative launch, wave by wave.
+struct LdpcMultiGroup {
+  int32_t code = 0;   // index into LdpcMultiParams::codes
+  int32_t group = 0;  // group of 64 frames within that code's job
+};
+constexpr int kMultiMaxCodes = 16;       // codes per launch
+constexpr int kMultiMaxWaveGroups = 32;  // groups per wave
+struct LdpcMultiParams {
+  const LdpcLanesParams* codes = nullptr;  // [ncodes] in device memory, layouts filled
+  int32_t ncodes = 0;
+  const LdpcMultiGroup* groups = nullptr;  // [wave_ptr[nwaves]], wave by wave
+  const int32_t* wave_ptr = nullptr;       // [nwaves + 1]
+  int32_t nwaves = 0;
+  unsigned* barrier = nullptr;             // [2] zeroed by the launcher
+};
+void ldpc_lanes_h2_layout(LdpcLanesParams& p, void* scratch);
+int64_t ldpc_lanes_h2_group_bytes(int64_t N, int64_t E);
+cudaError_t launch_ldpc_h2_stage(const LdpcLanesParams& p, cudaStream_t s);
+cudaError_t launch_ldpc_h2_finish(const LdpcLanesParams& p, cudaStream_t s);
+cudaError_t launch_ldpc_h2_multi(LdpcMultiParams m, int d_max, cudaStream_t s);
 
 // Flooding BP with each frame's messages resident in the shared memory of a
 // thread-block cluster of `cluster` CTAs (ldpc_cluster.cu).  The address tables are
@@ -196,6 +226,7 @@ struct TurboLteParams {
   int32_t iterations = 6;
   int32_t algorithm = 2;
   int32_t train = -1;  // training steps before each segment (-1: default)
+  int32_t segs = 0;    // segments per direction, 32 or 64 (0: default)
   const uint32_t* perm[2] = {nullptr, nullptr};  // interleavers of the constituents
   const float* sf = nullptr;                     // [2][iterations]
   const void* llr = nullptr;

@@ -29,7 +29,10 @@
 #include <cuda_fp16.h>
 #include <math.h>
 
+#include <mutex>
+
 #include "common.cuh"
+#include "grid_sync.cuh"
 #include "kernels.hpp"
 #include "ldpc_math.cuh"
 
@@ -117,8 +120,36 @@ __device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, uint3
   }
 }
 
-// Check pass of iteration `it` over groups [g0, g0 + gridDim.y): a warp per row, two
-// rows at a time for short rows so that twice the loads are in flight.
+// Rows r .. r + kRows - 1 (kRows = 2 for short rows, so that twice the loads are in
+// flight) of group g at iteration `it`: the row updates, stored for the lanes in
+// `mine`; returns the ballot of lanes whose syndrome bit of one of these rows is set.
+template <int ALG, int MSG, int DMAX>
+__device__ __forceinline__ uint32_t check_rows(const LdpcLanesParams& p, int g, int r, int lane, bool mine,
+                                               bool check_syndrome, const float* sf_row) {
+  constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  float v[kRows][DMAX];
+  uint32_t e0[kRows];
+  int d[kRows];
+  unsigned parity[kRows];
+  uint32_t bad = 0;
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+    d[q] = 0;
+    parity[q] = 0;
+    if (r + q < p.M) load_row<ALG, MSG, DMAX>(p, g, r + q, lane, e0[q], d[q], v[q], parity[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+    if (d[q] > 0) {
+      if (check_syndrome) bad |= __ballot_sync(0xffffffffu, parity[q] != 0);
+      store_row<ALG, MSG, DMAX>(p, g, e0[q], d[q], lane, sf_row, v[q], mine);
+    }
+  }
+  return bad;
+}
+
+// Check pass of iteration `it` over groups [g0, g0 + gridDim.y): a warp per row (or
+// row pair).
 template <int ALG, int MSG, int DMAX>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_check(LdpcLanesParams p, int it, int g0) {
   constexpr int kRows = DMAX <= 8 ? 2 : 1;
@@ -132,70 +163,117 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_check(LdpcLanesPara
   const bool mine = (active >> lane) & 1;
   uint32_t bad = 0;
   const int w0 = int(blockIdx.x) * kWarpsPerBlock + (threadIdx.x >> 5);
-  for (int r = w0 * kRows; r < p.M; r += warps * kRows) {
-    float v[kRows][DMAX];
-    uint32_t e0[kRows];
-    int d[kRows];
-    unsigned parity[kRows];
-#pragma unroll
-    for (int q = 0; q < kRows; ++q) {
-      d[q] = 0;
-      parity[q] = 0;
-      if (r + q < p.M) load_row<ALG, MSG, DMAX>(p, g, r + q, lane, e0[q], d[q], v[q], parity[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < kRows; ++q) {
-      if (d[q] > 0) {
-        if (check_syndrome) bad |= __ballot_sync(0xffffffffu, parity[q] != 0);
-        store_row<ALG, MSG, DMAX>(p, g, e0[q], d[q], lane, sf_row, v[q], mine);
-      }
-    }
-  }
+  for (int r = w0 * kRows; r < p.M; r += warps * kRows)
+    bad |= check_rows<ALG, MSG, DMAX>(p, g, r, lane, mine, check_syndrome, sf_row);
   bad &= active;
   if (bad && lane == 0) atomicOr(fail_of(p, it) + g, bad);
 }
 
+// Retirement of group g after the check pass of iteration `it`: the frames whose
+// syndrome held, or all of them at the last iteration, record their iteration count
+// and leave the active mask of iteration it + 1.
+__device__ __forceinline__ void retire_group(const LdpcLanesParams& p, int it, int g, uint32_t active) {
+  uint32_t done = 0;
+  if (it == p.iterations - 1) done = active;
+  else if (it > 0 && !p.fixed_iterations) done = active & ~fail_of(p, it)[g];
+  for (uint32_t m = done; m; m &= m - 1) p.iters_ws[int64_t(g) * kLanes + (__ffs(m) - 1)] = it + 1;
+  active_of(p, it + 1)[g] = active & ~done;
+  fail_of(p, it + 1)[g] = 0;
+}
+
+// app = chan + sum of c2v over bit b's edges, in increasing edge order, for this lane.
+template <int MSG>
+__device__ __forceinline__ void bit_one(const LdpcLanesParams& p, int g, int b, int lane) {
+  using M = Msg<MSG>;
+  const typename M::T* cg = static_cast<const typename M::T*>(p.c2v) + int64_t(g) * p.E * kLanes + lane;
+  const int64_t base = (int64_t(g) * p.N + b) * kLanes + lane;
+  const uint32_t k0 = __ldg(p.col_ptr + b), k1 = __ldg(p.col_ptr + b + 1);
+  float acc = p.chan[base];
+  uint32_t k = k0;
+  for (; k + 4 <= k1; k += 4) {
+    const uint32_t e_0 = __ldg(p.col_edges + k), e_1 = __ldg(p.col_edges + k + 1);
+    const uint32_t e_2 = __ldg(p.col_edges + k + 2), e_3 = __ldg(p.col_edges + k + 3);
+    const float x0 = M::load(cg + int64_t(e_0) * kLanes), x1 = M::load(cg + int64_t(e_1) * kLanes);
+    const float x2 = M::load(cg + int64_t(e_2) * kLanes), x3 = M::load(cg + int64_t(e_3) * kLanes);
+    acc += x0;
+    acc += x1;
+    acc += x2;
+    acc += x3;
+  }
+  for (; k < k1; ++k) acc += M::load(cg + int64_t(__ldg(p.col_edges + k)) * kLanes);
+  p.app[base] = acc;
+}
+
 // Bit pass of iteration `it` (or, with it < 0, the initial APP from chan and the
-// staged c2v for every lane): app = chan + sum of c2v over the bit's edges, in
-// increasing edge order.  Block (0, y) of each group retires the frames whose
-// syndrome held at this iteration, or all of them at the last one, records their
-// iteration counts and writes the group's masks for iteration it + 1.
+// staged c2v for every lane).  Block (0, y) of each group retires its frames and
+// writes the group's masks for iteration it + 1.
 template <int MSG>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_bit(LdpcLanesParams p, int it, int g0) {
-  using M = Msg<MSG>;
-  const auto* c2v = static_cast<const typename M::T*>(p.c2v);
   const int lane = lane_id();
   const int warps = int(gridDim.x) * kWarpsPerBlock;
   const int g = g0 + int(blockIdx.y);
   const uint32_t active = it < 0 ? 0xffffffffu : active_of(p, it)[g];
-  if (it >= 0 && blockIdx.x == 0 && threadIdx.x == 0) {
-    uint32_t done = 0;
-    if (it == p.iterations - 1) done = active;
-    else if (it > 0 && !p.fixed_iterations) done = active & ~fail_of(p, it)[g];
-    for (uint32_t m = done; m; m &= m - 1) p.iters_ws[int64_t(g) * kLanes + (__ffs(m) - 1)] = it + 1;
-    active_of(p, it + 1)[g] = active & ~done;
-    fail_of(p, it + 1)[g] = 0;
-  }
+  if (it >= 0 && blockIdx.x == 0 && threadIdx.x == 0) retire_group(p, it, g, active);
   if (!((active >> lane) & 1)) return;
-  const typename M::T* cg = c2v + int64_t(g) * p.E * kLanes + lane;
-  for (int b = int(blockIdx.x) * kWarpsPerBlock + (threadIdx.x >> 5); b < p.N; b += warps) {
-    const int64_t base = (int64_t(g) * p.N + b) * kLanes + lane;
-    const uint32_t k0 = __ldg(p.col_ptr + b), k1 = __ldg(p.col_ptr + b + 1);
-    float acc = p.chan[base];
-    uint32_t k = k0;
-    for (; k + 4 <= k1; k += 4) {
-      const uint32_t e_0 = __ldg(p.col_edges + k), e_1 = __ldg(p.col_edges + k + 1);
-      const uint32_t e_2 = __ldg(p.col_edges + k + 2), e_3 = __ldg(p.col_edges + k + 3);
-      const float x0 = M::load(cg + int64_t(e_0) * kLanes), x1 = M::load(cg + int64_t(e_1) * kLanes);
-      const float x2 = M::load(cg + int64_t(e_2) * kLanes), x3 = M::load(cg + int64_t(e_3) * kLanes);
-      acc += x0;
-      acc += x1;
-      acc += x2;
-      acc += x3;
+  for (int b = int(blockIdx.x) * kWarpsPerBlock + (threadIdx.x >> 5); b < p.N; b += warps) bit_one<MSG>(p, g, b, lane);
+}
+
+// Persistent decoder for a small batch (at most kPersistGroups groups, all in one wave):
+// one launch runs the initial APP and every iteration, the check and bit passes of
+// all groups spread over the whole grid and separated by grid barriers, so a decode of
+// a few frame groups costs one launch instead of two per iteration.  It computes
+// exactly the rows, bits and retirements of lanes_check / lanes_bit.  A barrier that
+// gives up marks every frame's iteration count -1 (not decoded).
+constexpr int kPersistGroups = 16;
+
+template <int ALG, int MSG, int DMAX>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_persist(LdpcLanesParams p) {
+  constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  __shared__ uint32_t s_bad[kPersistGroups];
+  const int lane = lane_id();
+  const int warp = int(blockIdx.x) * kWarpsPerBlock + (threadIdx.x >> 5);
+  const int warps = int(gridDim.x) * kWarpsPerBlock;
+  const int ng = p.groups;
+  unsigned epoch = 0;
+  for (int64_t u = warp; u < int64_t(ng) * p.N; u += warps) bit_one<MSG>(p, int(u / p.N), int(u % p.N), lane);
+  bool ok = grid_barrier(p.barrier, p.barrier + 1, epoch);
+  const int rows = (p.M + kRows - 1) / kRows;
+  for (int it = 0; ok && it < p.iterations; ++it) {
+    const bool check_syndrome = it > 0 && !p.fixed_iterations;
+    const float* sf_row = p.sf + size_t(it % p.n_sf) * p.sf_stride;
+    if (threadIdx.x < kPersistGroups) s_bad[threadIdx.x] = 0;
+    __syncthreads();
+    // check pass: units (group, row pair) group-major; a warp's bad lanes ORed per group
+    int g_cur = -1;
+    uint32_t bad = 0, active = 0;
+    for (int64_t u = warp; u < int64_t(ng) * rows; u += warps) {
+      const int g = int(u / rows);
+      if (g != g_cur) {
+        if (bad && lane == 0) atomicOr(&s_bad[g_cur], bad & active);
+        g_cur = g;
+        bad = 0;
+        active = active_of(p, it)[g];
+      }
+      if (active == 0) continue;
+      bad |= check_rows<ALG, MSG, DMAX>(p, g, int(u % rows) * kRows, lane, (active >> lane) & 1, check_syndrome, sf_row);
     }
-    for (; k < k1; ++k) acc += M::load(cg + int64_t(__ldg(p.col_edges + k)) * kLanes);
-    p.app[base] = acc;
+    if (bad && lane == 0) atomicOr(&s_bad[g_cur], bad & active);
+    __syncthreads();
+    if (threadIdx.x < ng && s_bad[threadIdx.x]) atomicOr(fail_of(p, it) + threadIdx.x, s_bad[threadIdx.x]);
+    if (!(ok = grid_barrier(p.barrier, p.barrier + 1, epoch))) break;
+    // bit pass, and block 0 retires the frames
+    if (blockIdx.x == 0 && threadIdx.x < ng) retire_group(p, it, threadIdx.x, active_of(p, it)[threadIdx.x]);
+    for (int64_t u = warp; u < int64_t(ng) * p.N; u += warps) {
+      const int g = int(u / p.N);
+      if ((active_of(p, it)[g] >> lane) & 1) bit_one<MSG>(p, g, int(u % p.N), lane);
+    }
+    if (!(ok = grid_barrier(p.barrier, p.barrier + 1, epoch))) break;
+    uint32_t left = 0;
+    for (int g = 0; g < ng; ++g) left |= active_of(p, it + 1)[g];
+    if (left == 0) break;
   }
+  if (!ok && blockIdx.x == 0)
+    for (int i = threadIdx.x; i < ng * kLanes; i += blockDim.x) p.iters_ws[i] = -1;
 }
 
 // Frame-major inputs -> lane-minor scratch for group blockIdx.y: chan (+ a-priori on
@@ -307,13 +385,82 @@ int wave_for(const LdpcLanesParams& p, int64_t gb) {
   return int(wave < p.groups ? wave : p.groups);
 }
 
+// Whether a batch runs as one persistent launch: small enough (at most kPersistGroups
+// groups, one wave) and on a stream that is not being captured into a graph.  With
+// persist == 0 only batches of at most kPersistAuto groups do: there the two launches
+// per iteration cost more than the work they carry.
+constexpr int kPersistAuto = 4;
+
+bool use_persistent(const LdpcLanesParams& p, int wave, cudaStream_t s) {
+  if (p.persist < 0 || p.groups > kPersistGroups || wave < p.groups) return false;
+  if (p.persist == 0 && p.groups > kPersistAuto) return false;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+// Persistent launches of one device run one after the other, whatever their streams,
+// so that two of them never hold parts of the GPU while each waits for the rest: every
+// such launch waits for an event the previous one recorded.
+namespace {
+std::mutex g_persist_mu;
+cudaEvent_t g_persist_ev[64] = {};
+}  // namespace
+
+cudaError_t ldpc_persist_launch(cudaStream_t s, const void* kern, unsigned blocks, unsigned threads, void** args) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_persist_mu);
+  if (!g_persist_ev[dev] && (e = cudaEventCreateWithFlags(&g_persist_ev[dev], cudaEventDisableTiming)) != cudaSuccess)
+    return e;
+  if ((e = cudaStreamWaitEvent(s, g_persist_ev[dev], 0)) != cudaSuccess) return e;
+  if ((e = cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(threads), args, 0, s)) != cudaSuccess) return e;
+  return cudaEventRecord(g_persist_ev[dev], s);
+}
+
+namespace {
+
+template <int ALG, int MSG, int DMAX>
+cudaError_t launch_persistent(LdpcLanesParams p, cudaStream_t s) {
+  auto kern = lanes_persist<ALG, MSG, DMAX>;
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaError_t e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWarpsPerBlock * 32, 0)) != cudaSuccess) return e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  const int64_t rows = (p.M + kRows - 1) / kRows;
+  const int64_t units = int64_t(p.groups) * (int64_t(p.N) > rows ? int64_t(p.N) : rows);
+  int64_t blocks = (units + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (blocks > int64_t(per_sm) * sms) blocks = int64_t(per_sm) * sms;
+  if (blocks < 1) return cudaErrorInvalidConfiguration;
+  if ((e = cudaMemsetAsync(p.barrier, 0, 2 * sizeof(unsigned), s)) != cudaSuccess) return e;
+  void* args[] = {&p};
+  return ldpc_persist_launch(s, reinterpret_cast<const void*>(kern), unsigned(blocks), kWarpsPerBlock * 32, args);
+}
+
 template <int ALG, int MSG, int DMAX>
 cudaError_t run(const LdpcLanesParams& p, cudaStream_t s) {
   if (p.groups > 65535) return cudaErrorInvalidValue;
   const int wave = wave_for(p, group_bytes(p));
   const dim3 gs((148 * 8 + p.groups - 1) / p.groups, p.groups);
   lanes_stage<MSG><<<gs, 256, 0, s>>>(p);
-  for (int w0 = 0; w0 < p.groups; w0 += wave) {
+  bool done = false;
+  if (use_persistent(p, wave, s)) {
+    const cudaError_t e = launch_persistent<ALG, MSG, DMAX>(p, s);
+    if (e == cudaSuccess) done = true;
+    else if (e != cudaErrorCooperativeLaunchTooLarge && e != cudaErrorNotSupported && e != cudaErrorInvalidConfiguration)
+      return e;
+    else cudaGetLastError();
+  }
+  for (int w0 = 0; !done && w0 < p.groups; w0 += wave) {
     const int nw = p.groups - w0 < wave ? p.groups - w0 : wave;
     const dim3 gbit = grid_for(p.N, nw);
     const dim3 gchk = grid_for((p.M + (DMAX <= 8 ? 1 : 0)) / (DMAX <= 8 ? 2 : 1), nw);
@@ -359,7 +506,7 @@ size_t ldpc_lanes_scratch_bytes(int64_t N, int64_t E, int64_t nframes, int msg_t
   const size_t msg_bytes = msg_type == 1 ? 2 : (msg_type == 2 ? 1 : 4);
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   return al(size_t(groups) * N * kLanes * 4) * 2 + al(size_t(groups) * E * kLanes * msg_bytes) +
-         al(size_t(groups) * 16) + al(size_t(groups) * kLanes * 4);
+         al(size_t(groups) * 16) + al(size_t(groups) * kLanes * 4) + al(2 * sizeof(unsigned));
 }
 
 cudaError_t launch_ldpc_lanes(LdpcLanesParams p, void* scratch, cudaStream_t s) {
@@ -380,6 +527,8 @@ cudaError_t launch_ldpc_lanes(LdpcLanesParams p, void* scratch, cudaStream_t s) 
   p.fail = p.active + 2 * p.groups;          // [2][groups]
   q += al(size_t(p.groups) * 16);
   p.iters_ws = reinterpret_cast<int32_t*>(q);
+  q += al(size_t(p.groups) * kLanes * 4);
+  p.barrier = reinterpret_cast<unsigned*>(q);
   switch (p.algorithm) {
     case kExact: return run_m<kExact>(p, s);
     case kLinear: return run_m<kLinear>(p, s);

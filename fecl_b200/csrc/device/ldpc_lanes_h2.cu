@@ -21,6 +21,7 @@
 #include <math.h>
 
 #include "common.cuh"
+#include "grid_sync.cuh"
 #include "kernels.hpp"
 
 namespace fecl {
@@ -142,6 +143,32 @@ __device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, int l
   }
 }
 
+// Rows r .. r + kRows - 1 of group g at iteration `it` (kRows = 2 for rows of degree
+// <= 8): the row updates; bx / by collect the lanes whose syndrome bit is set.
+template <int DMAX>
+__device__ __forceinline__ void check_rows(const LdpcLanesParams& p, int it, int g, int r, int lane, bool mx, bool my,
+                                           bool keep_all, bool check_syndrome, uint32_t& bx, uint32_t& by) {
+  constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  Row<DMAX> w[kRows];
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+    w[q].d = 0;
+    if (r + q < p.M) load_row<DMAX>(p, g, r + q, lane, w[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+    if (w[q].d > 0) {
+      if (check_syndrome) {
+        bx |= __ballot_sync(0xffffffffu, w[q].px != 0);
+        by |= __ballot_sync(0xffffffffu, w[q].py != 0);
+      }
+      // the scaling of rows of this degree (constant across iterations on this path)
+      const float s = p.sf[size_t(it % p.n_sf) * p.sf_stride + (w[q].d >= 2 ? w[q].d - 2 : 0)];
+      store_row<DMAX>(p, g, lane, w[q], __float2half2_rn(s), mx, my, keep_all);
+    }
+  }
+}
+
 template <int DMAX>
 __global__ void __launch_bounds__(kWarps * 32) h2_check(LdpcLanesParams p, int it, int g0) {
   constexpr int kRows = DMAX <= 8 ? 2 : 1;
@@ -155,26 +182,8 @@ __global__ void __launch_bounds__(kWarps * 32) h2_check(LdpcLanesParams p, int i
   const bool keep_all = p.msg_out || p.syst_out || p.parity_out || p.state_out;
   uint32_t bx = 0, by = 0;
   const int w0 = int(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-  for (int r = w0 * kRows; r < p.M; r += warps * kRows) {
-    Row<DMAX> w[kRows];
-#pragma unroll
-    for (int q = 0; q < kRows; ++q) {
-      w[q].d = 0;
-      if (r + q < p.M) load_row<DMAX>(p, g, r + q, lane, w[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < kRows; ++q) {
-      if (w[q].d > 0) {
-        if (check_syndrome) {
-          bx |= __ballot_sync(0xffffffffu, w[q].px != 0);
-          by |= __ballot_sync(0xffffffffu, w[q].py != 0);
-        }
-        // the scaling of rows of this degree (constant across iterations on this path)
-        const float s = p.sf[size_t(it % p.n_sf) * p.sf_stride + (w[q].d >= 2 ? w[q].d - 2 : 0)];
-        store_row<DMAX>(p, g, lane, w[q], __float2half2_rn(s), mx, my, keep_all);
-      }
-    }
-  }
+  for (int r = w0 * kRows; r < p.M; r += warps * kRows)
+    check_rows<DMAX>(p, it, g, r, lane, mx, my, keep_all, check_syndrome, bx, by);
   bx &= ax;
   by &= ay;
   if (lane == 0) {
@@ -183,55 +192,213 @@ __global__ void __launch_bounds__(kWarps * 32) h2_check(LdpcLanesParams p, int i
   }
 }
 
+// Retirement of the .x (h = 0) or .y (h = 1) frames of group g after the check pass of
+// iteration `it`, and their masks for iteration it + 1.
+__device__ __forceinline__ void retire_half(const LdpcLanesParams& p, int it, int g, int h) {
+  const uint32_t a = active_of(p, it)[2 * g + h];
+  uint32_t done = 0;
+  if (it == p.iterations - 1) done = a;
+  else if (it > 0 && !p.fixed_iterations) done = a & ~fail_of(p, it)[2 * g + h];
+  for (uint32_t m = done; m; m &= m - 1) p.iters_ws[int64_t(g) * 64 + h * 32 + (__ffs(m) - 1)] = it + 1;
+  active_of(p, it + 1)[2 * g + h] = a & ~done;
+  fail_of(p, it + 1)[2 * g + h] = 0;
+}
+
+// app = chan + sum of c2v over bit b's edges (edge order, FP32) for this lane's two
+// frames; a retired frame's value stays.
+__device__ __forceinline__ void bit_one(const LdpcLanesParams& p, int g, int b, int lane, bool mx, bool my) {
+  const __half2* cg = static_cast<const __half2*>(p.c2v) + int64_t(g) * p.E * kLanes + lane;
+  const float2* chan = reinterpret_cast<const float2*>(p.chan);
+  float2* app = reinterpret_cast<float2*>(p.app);
+  const int64_t base = (int64_t(g) * p.N + b) * kLanes + lane;
+  const uint32_t k0 = __ldg(p.col_ptr + b), k1 = __ldg(p.col_ptr + b + 1);
+  float2 acc = chan[base];
+  uint32_t k = k0;
+  for (; k + 4 <= k1; k += 4) {
+    const uint32_t e_0 = __ldg(p.col_edges + k), e_1 = __ldg(p.col_edges + k + 1);
+    const uint32_t e_2 = __ldg(p.col_edges + k + 2), e_3 = __ldg(p.col_edges + k + 3);
+    const float2 x0 = __half22float2(cg[int64_t(e_0) * kLanes]), x1 = __half22float2(cg[int64_t(e_1) * kLanes]);
+    const float2 x2 = __half22float2(cg[int64_t(e_2) * kLanes]), x3 = __half22float2(cg[int64_t(e_3) * kLanes]);
+    acc = __fadd2_rn(acc, x0);
+    acc = __fadd2_rn(acc, x1);
+    acc = __fadd2_rn(acc, x2);
+    acc = __fadd2_rn(acc, x3);
+  }
+  for (; k < k1; ++k) acc = __fadd2_rn(acc, __half22float2(cg[int64_t(__ldg(p.col_edges + k)) * kLanes]));
+  if (mx && my) {
+    app[base] = acc;
+  } else {  // one of the lane's frames has retired: its APP stays
+    float2 out = app[base];
+    if (mx) out.x = acc.x;
+    if (my) out.y = acc.y;
+    app[base] = out;
+  }
+}
+
 // Bit pass; with it < 0 the initial APP for every lane.  Block (0, y) retires frames
 // and writes the group's masks for iteration it + 1.
 __global__ void __launch_bounds__(kWarps * 32) h2_bit(LdpcLanesParams p, int it, int g0) {
-  const __half2* c2v = static_cast<const __half2*>(p.c2v);
-  const float2* chan = reinterpret_cast<const float2*>(p.chan);
-  float2* app = reinterpret_cast<float2*>(p.app);
   const int lane = threadIdx.x & 31;
   const int warps = int(gridDim.x) * kWarps;
   const int g = g0 + int(blockIdx.y);
   const uint32_t ax = it < 0 ? 0xffffffffu : active_of(p, it)[2 * g];
   const uint32_t ay = it < 0 ? 0xffffffffu : active_of(p, it)[2 * g + 1];
-  if (it >= 0 && blockIdx.x == 0 && threadIdx.x < 2) {
-    const int h = threadIdx.x;  // 0: .x frames, 1: .y frames
-    const uint32_t a = h ? ay : ax;
-    uint32_t done = 0;
-    if (it == p.iterations - 1) done = a;
-    else if (it > 0 && !p.fixed_iterations) done = a & ~fail_of(p, it)[2 * g + h];
-    for (uint32_t m = done; m; m &= m - 1) p.iters_ws[int64_t(g) * 64 + h * 32 + (__ffs(m) - 1)] = it + 1;
-    active_of(p, it + 1)[2 * g + h] = a & ~done;
-    fail_of(p, it + 1)[2 * g + h] = 0;
-  }
+  if (it >= 0 && blockIdx.x == 0 && threadIdx.x < 2) retire_half(p, it, g, threadIdx.x);
   const bool mx = (ax >> lane) & 1, my = (ay >> lane) & 1;
   if (!mx && !my) return;
-  const __half2* cg = c2v + int64_t(g) * p.E * kLanes + lane;
-  for (int b = int(blockIdx.x) * kWarps + (threadIdx.x >> 5); b < p.N; b += warps) {
-    const int64_t base = (int64_t(g) * p.N + b) * kLanes + lane;
-    const uint32_t k0 = __ldg(p.col_ptr + b), k1 = __ldg(p.col_ptr + b + 1);
-    float2 acc = chan[base];
-    uint32_t k = k0;
-    for (; k + 4 <= k1; k += 4) {
-      const uint32_t e_0 = __ldg(p.col_edges + k), e_1 = __ldg(p.col_edges + k + 1);
-      const uint32_t e_2 = __ldg(p.col_edges + k + 2), e_3 = __ldg(p.col_edges + k + 3);
-      const float2 x0 = __half22float2(cg[int64_t(e_0) * kLanes]), x1 = __half22float2(cg[int64_t(e_1) * kLanes]);
-      const float2 x2 = __half22float2(cg[int64_t(e_2) * kLanes]), x3 = __half22float2(cg[int64_t(e_3) * kLanes]);
-      acc = __fadd2_rn(acc, x0);
-      acc = __fadd2_rn(acc, x1);
-      acc = __fadd2_rn(acc, x2);
-      acc = __fadd2_rn(acc, x3);
+  for (int b = int(blockIdx.x) * kWarps + (threadIdx.x >> 5); b < p.N; b += warps) bit_one(p, g, b, lane, mx, my);
+}
+
+// Persistent decoder for a small batch (at most kPersistGroups groups of 64 frames,
+// one wave): one launch runs the initial APP and every iteration, the passes of all
+// groups spread over the whole grid and separated by grid barriers.  It computes
+// exactly the rows, bits and retirements of h2_check / h2_bit.  A barrier that gives
+// up marks every frame's iteration count -1 (not decoded).
+constexpr int kPersistGroups = 16;
+
+template <int DMAX>
+__global__ void __launch_bounds__(kWarps * 32) h2_persist(LdpcLanesParams p) {
+  constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  __shared__ uint32_t s_bad[2 * kPersistGroups];
+  const int lane = threadIdx.x & 31;
+  const int warp = int(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  const int warps = int(gridDim.x) * kWarps;
+  const int ng = p.groups;
+  const bool keep_all = p.msg_out || p.syst_out || p.parity_out || p.state_out;
+  unsigned epoch = 0;
+  for (int64_t u = warp; u < int64_t(ng) * p.N; u += warps) bit_one(p, int(u / p.N), int(u % p.N), lane, true, true);
+  bool ok = grid_barrier(p.barrier, p.barrier + 1, epoch);
+  const int rows = (p.M + kRows - 1) / kRows;
+  for (int it = 0; ok && it < p.iterations; ++it) {
+    const bool check_syndrome = it > 0 && !p.fixed_iterations;
+    if (threadIdx.x < 2 * kPersistGroups) s_bad[threadIdx.x] = 0;
+    __syncthreads();
+    int g_cur = -1;
+    uint32_t bx = 0, by = 0, ax = 0, ay = 0;
+    for (int64_t u = warp; u < int64_t(ng) * rows; u += warps) {
+      const int g = int(u / rows);
+      if (g != g_cur) {
+        if (lane == 0 && (bx & ax)) atomicOr(&s_bad[2 * g_cur], bx & ax);
+        if (lane == 0 && (by & ay)) atomicOr(&s_bad[2 * g_cur + 1], by & ay);
+        g_cur = g;
+        bx = by = 0;
+        ax = active_of(p, it)[2 * g];
+        ay = active_of(p, it)[2 * g + 1];
+      }
+      if ((ax | ay) == 0) continue;
+      check_rows<DMAX>(p, it, g, int(u % rows) * kRows, lane, (ax >> lane) & 1, (ay >> lane) & 1, keep_all,
+                       check_syndrome, bx, by);
     }
-    for (; k < k1; ++k) acc = __fadd2_rn(acc, __half22float2(cg[int64_t(__ldg(p.col_edges + k)) * kLanes]));
-    if (mx && my) {
-      app[base] = acc;
-    } else {  // one of the lane's frames has retired: its APP stays
-      float2 out = app[base];
-      if (mx) out.x = acc.x;
-      if (my) out.y = acc.y;
-      app[base] = out;
+    if (lane == 0 && g_cur >= 0 && (bx & ax)) atomicOr(&s_bad[2 * g_cur], bx & ax);
+    if (lane == 0 && g_cur >= 0 && (by & ay)) atomicOr(&s_bad[2 * g_cur + 1], by & ay);
+    __syncthreads();
+    if (threadIdx.x < 2 * ng && s_bad[threadIdx.x]) atomicOr(fail_of(p, it) + threadIdx.x, s_bad[threadIdx.x]);
+    if (!(ok = grid_barrier(p.barrier, p.barrier + 1, epoch))) break;
+    if (blockIdx.x == 0 && threadIdx.x < 2 * ng) retire_half(p, it, threadIdx.x >> 1, threadIdx.x & 1);
+    for (int64_t u = warp; u < int64_t(ng) * p.N; u += warps) {
+      const int g = int(u / p.N);
+      const bool mx = (active_of(p, it)[2 * g] >> lane) & 1, my = (active_of(p, it)[2 * g + 1] >> lane) & 1;
+      if (mx || my) bit_one(p, g, int(u % p.N), lane, mx, my);
+    }
+    if (!(ok = grid_barrier(p.barrier, p.barrier + 1, epoch))) break;
+    uint32_t left = 0;
+    for (int i = 0; i < 2 * ng; ++i) left |= active_of(p, it + 1)[i];
+    if (left == 0) break;
+  }
+  if (!ok && blockIdx.x == 0)
+    for (int i = threadIdx.x; i < ng * 64; i += blockDim.x) p.iters_ws[i] = -1;
+}
+
+// ---- several codes in one launch ------------------------------------------------
+
+// The groups of every job of a mixed batch (each job one code, its own scratch) whose
+// check degrees are at most DMAX (8, 16 or 32) in one persistent launch: waves of
+// groups, from any codes, whose working sets fit in L2 together; per wave the initial
+// APP and every iteration, each pass spreading every group's rows (or bits) over the
+// whole grid, passes separated by grid barriers.  A group runs exactly the rows, bits
+// and retirements of h2_check / h2_bit with its own code's tables, scaling and
+// iteration limit, so every frame's result is that of its job decoded alone.  A
+// barrier that gives up marks the iteration counts of every frame -1 (not decoded).
+__device__ __forceinline__ bool wave_left(const LdpcMultiParams& m, const LdpcLanesParams* codes, int q0, int q1,
+                                          int it) {
+  uint32_t left = 0;
+  for (int q = q0; q < q1; ++q) {
+    const LdpcMultiGroup gr = m.groups[q];
+    const LdpcLanesParams& p = codes[gr.code];
+    left |= active_of(p, it)[2 * gr.group] | active_of(p, it)[2 * gr.group + 1];
+  }
+  return left != 0;
+}
+
+template <int DMAX>
+__global__ void __launch_bounds__(kWarps * 32, DMAX <= 16 ? 3 : 2) h2_multi(LdpcMultiParams m) {
+  constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  __shared__ LdpcLanesParams s_codes[kMultiMaxCodes];
+  __shared__ uint32_t s_bad[2 * kMultiMaxWaveGroups];
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(m.codes);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(s_codes);
+    const int words = int(m.ncodes * sizeof(LdpcLanesParams) / 4);
+    for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warp = int(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  const int warps = int(gridDim.x) * kWarps;
+  unsigned epoch = 0;
+  bool ok = true;
+  for (int w = 0; ok && w < m.nwaves; ++w) {
+    const int q0 = m.wave_ptr[w], q1 = m.wave_ptr[w + 1];
+    int max_it = 0;
+    for (int q = q0; q < q1; ++q) max_it = max(max_it, s_codes[m.groups[q].code].iterations);
+    for (int q = q0; q < q1; ++q) {
+      const LdpcMultiGroup gr = m.groups[q];
+      const LdpcLanesParams& p = s_codes[gr.code];
+      for (int b = warp; b < p.N; b += warps) bit_one(p, gr.group, b, lane, true, true);
+    }
+    ok = grid_barrier(m.barrier, m.barrier + 1, epoch);
+    for (int it = 0; ok && it < max_it; ++it) {
+      if (threadIdx.x < 2 * kMultiMaxWaveGroups) s_bad[threadIdx.x] = 0;
+      __syncthreads();
+      for (int q = q0; q < q1; ++q) {
+        const LdpcMultiGroup gr = m.groups[q];
+        const LdpcLanesParams& p = s_codes[gr.code];
+        const uint32_t ax = active_of(p, it)[2 * gr.group], ay = active_of(p, it)[2 * gr.group + 1];
+        if ((ax | ay) == 0) continue;
+        const bool keep_all = p.msg_out || p.syst_out || p.parity_out || p.state_out;
+        const bool check_syndrome = it > 0 && !p.fixed_iterations;
+        uint32_t bx = 0, by = 0;
+        for (int r = warp * kRows; r < p.M; r += warps * kRows)
+          check_rows<DMAX>(p, it, gr.group, r, lane, (ax >> lane) & 1, (ay >> lane) & 1, keep_all, check_syndrome, bx,
+                           by);
+        if (lane == 0 && (bx & ax)) atomicOr(&s_bad[2 * (q - q0)], bx & ax);
+        if (lane == 0 && (by & ay)) atomicOr(&s_bad[2 * (q - q0) + 1], by & ay);
+      }
+      __syncthreads();
+      if (threadIdx.x < 2 * (q1 - q0) && s_bad[threadIdx.x]) {
+        const LdpcMultiGroup gr = m.groups[q0 + (threadIdx.x >> 1)];
+        atomicOr(fail_of(s_codes[gr.code], it) + 2 * gr.group + (threadIdx.x & 1), s_bad[threadIdx.x]);
+      }
+      if (!(ok = grid_barrier(m.barrier, m.barrier + 1, epoch))) break;
+      if (blockIdx.x == 0 && threadIdx.x < 2 * (q1 - q0)) {
+        const LdpcMultiGroup gr = m.groups[q0 + (threadIdx.x >> 1)];
+        retire_half(s_codes[gr.code], it, gr.group, threadIdx.x & 1);
+      }
+      for (int q = q0; q < q1; ++q) {
+        const LdpcMultiGroup gr = m.groups[q];
+        const LdpcLanesParams& p = s_codes[gr.code];
+        const uint32_t ax = active_of(p, it)[2 * gr.group], ay = active_of(p, it)[2 * gr.group + 1];
+        const bool mx = (ax >> lane) & 1, my = (ay >> lane) & 1;
+        if (!mx && !my) continue;
+        for (int b = warp; b < p.N; b += warps) bit_one(p, gr.group, b, lane, mx, my);
+      }
+      if (!(ok = grid_barrier(m.barrier, m.barrier + 1, epoch))) break;
+      if (!wave_left(m, s_codes, q0, q1, it + 1)) break;
     }
   }
+  if (!ok && blockIdx.x == 0)
+    for (int c = 0; c < m.ncodes; ++c)
+      for (int i = threadIdx.x; i < s_codes[c].groups * 64; i += blockDim.x) s_codes[c].iters_ws[i] = -1;
 }
 
 // Frame f of group g sits in lane f % 32, half (f / 32) % 2.
@@ -333,6 +500,40 @@ dim3 grid_for(int64_t per_group, int groups) {
 // than two).
 constexpr int64_t kWaveCap = 96ll << 20;
 
+// One persistent launch for batches of at most kPersistAuto groups (or, with
+// persist == 1, kPersistGroups), all in one wave, on a stream that is not capturing.
+constexpr int kPersistAuto = 4;
+
+bool use_persistent(const LdpcLanesParams& p, int64_t wave, cudaStream_t s) {
+  if (p.persist < 0 || p.groups > kPersistGroups || wave < p.groups) return false;
+  if (p.persist == 0 && p.groups > kPersistAuto) return false;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return false;
+  }
+  return true;
+}
+
+template <int DMAX>
+cudaError_t launch_persistent(LdpcLanesParams p, cudaStream_t s) {
+  auto kern = h2_persist<DMAX>;
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaError_t e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWarps * 32, 0)) != cudaSuccess) return e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  const int64_t rows = (p.M + kRows - 1) / kRows;
+  const int64_t units = int64_t(p.groups) * (int64_t(p.N) > rows ? int64_t(p.N) : rows);
+  int64_t blocks = (units + kWarps - 1) / kWarps;
+  if (blocks > int64_t(per_sm) * sms) blocks = int64_t(per_sm) * sms;
+  if (blocks < 1) return cudaErrorInvalidConfiguration;
+  if ((e = cudaMemsetAsync(p.barrier, 0, 2 * sizeof(unsigned), s)) != cudaSuccess) return e;
+  void* args[] = {&p};
+  return ldpc_persist_launch(s, reinterpret_cast<const void*>(kern), unsigned(blocks), kWarps * 32, args);
+}
+
 template <int DMAX>
 cudaError_t run(const LdpcLanesParams& p, cudaStream_t s) {
   if (p.groups > 65535) return cudaErrorInvalidValue;
@@ -342,7 +543,15 @@ cudaError_t run(const LdpcLanesParams& p, cudaStream_t s) {
   if (wave > p.groups) wave = p.groups;
   const dim3 gs((148 * 8 + p.groups - 1) / p.groups, p.groups);
   h2_stage<<<gs, 256, 0, s>>>(p);
-  for (int w0 = 0; w0 < p.groups; w0 += int(wave)) {
+  bool done = false;
+  if (use_persistent(p, wave, s)) {
+    const cudaError_t e = launch_persistent<DMAX>(p, s);
+    if (e == cudaSuccess) done = true;
+    else if (e != cudaErrorCooperativeLaunchTooLarge && e != cudaErrorNotSupported && e != cudaErrorInvalidConfiguration)
+      return e;
+    else cudaGetLastError();
+  }
+  for (int w0 = 0; !done && w0 < p.groups; w0 += int(wave)) {
     const int nw = p.groups - w0 < wave ? p.groups - w0 : int(wave);
     const dim3 gbit = grid_for(p.N, nw);
     const dim3 gchk = grid_for((p.M + (DMAX <= 8 ? 1 : 0)) / (DMAX <= 8 ? 2 : 1), nw);
@@ -356,18 +565,55 @@ cudaError_t run(const LdpcLanesParams& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <int DMAX>
+int multi_blocks() {
+  int per_sm = 0, dev = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, h2_multi<DMAX>, kWarps * 32, 0) != cudaSuccess ||
+      cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return per_sm * sms;
+}
+
+template <int DMAX>
+cudaError_t launch_multi(LdpcMultiParams m, cudaStream_t s) {
+  const int blocks = multi_blocks<DMAX>();
+  if (blocks <= 0) return cudaErrorInvalidConfiguration;
+  cudaError_t e = cudaMemsetAsync(m.barrier, 0, 2 * sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  // A cooperative launch (all blocks resident, so the grid barriers are safe).  Outside
+  // a stream capture it is ordered after the device's previous persistent launch;
+  // under capture it goes through cudaLaunchKernelEx, which records a cooperative
+  // graph node.
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if ((e = cudaStreamIsCapturing(s, &cs)) != cudaSuccess) return e;
+  if (cs == cudaStreamCaptureStatusNone) {
+    void* args[] = {&m};
+    return ldpc_persist_launch(s, reinterpret_cast<const void*>(h2_multi<DMAX>), unsigned(blocks), kWarps * 32, args);
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(blocks));
+  cfg.blockDim = dim3(kWarps * 32);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, h2_multi<DMAX>, m);
+}
+
 }  // namespace
 
 size_t ldpc_lanes_h2_scratch_bytes(int64_t N, int64_t E, int64_t nframes) {
   const int64_t groups = (nframes + 63) / 64;
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   return al(size_t(groups) * N * kLanes * 8) * 2 + al(size_t(groups) * E * kLanes * 4) + al(size_t(groups) * 32) +
-         al(size_t(groups) * 64 * 4);
+         al(size_t(groups) * 64 * 4) + al(2 * sizeof(unsigned));
 }
 
-cudaError_t launch_ldpc_lanes_h2(LdpcLanesParams p, void* scratch, cudaStream_t s) {
-  if (p.nframes <= 0) return cudaSuccess;
-  if (p.state_in || p.algorithm != 2) return cudaErrorInvalidValue;
+void ldpc_lanes_h2_layout(LdpcLanesParams& p, void* scratch) {
   p.groups = int32_t((p.nframes + 63) / 64);
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   char* q = static_cast<char*>(scratch);
@@ -381,6 +627,37 @@ cudaError_t launch_ldpc_lanes_h2(LdpcLanesParams p, void* scratch, cudaStream_t 
   p.fail = p.active + 4 * p.groups;          // [2][groups][2]
   q += al(size_t(p.groups) * 32);
   p.iters_ws = reinterpret_cast<int32_t*>(q);
+  q += al(size_t(p.groups) * 64 * 4);
+  p.barrier = reinterpret_cast<unsigned*>(q);
+}
+
+int64_t ldpc_lanes_h2_group_bytes(int64_t N, int64_t E) { return int64_t(kLanes) * (2 * 8 * N + 4 * E); }
+
+cudaError_t launch_ldpc_h2_stage(const LdpcLanesParams& p, cudaStream_t s) {
+  if (p.groups <= 0) return cudaSuccess;
+  h2_stage<<<dim3((148 * 8 + p.groups - 1) / p.groups, p.groups), 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ldpc_h2_finish(const LdpcLanesParams& p, cudaStream_t s) {
+  if (p.groups <= 0) return cudaSuccess;
+  h2_finish<<<dim3((148 * 8 + p.groups - 1) / p.groups, p.groups), 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ldpc_h2_multi(LdpcMultiParams m, int d_max, cudaStream_t s) {
+  if (m.nwaves <= 0) return cudaSuccess;
+  if (m.ncodes <= 0 || m.ncodes > kMultiMaxCodes) return cudaErrorInvalidValue;
+  if (d_max <= 8) return launch_multi<8>(m, s);
+  if (d_max <= 16) return launch_multi<16>(m, s);
+  if (d_max <= 32) return launch_multi<32>(m, s);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_ldpc_lanes_h2(LdpcLanesParams p, void* scratch, cudaStream_t s) {
+  if (p.nframes <= 0) return cudaSuccess;
+  if (p.state_in || p.algorithm != 2) return cudaErrorInvalidValue;
+  ldpc_lanes_h2_layout(p, scratch);
   if (p.d_max <= 8) return run<8>(p, s);
   if (p.d_max <= 16) return run<16>(p, s);
   if (p.d_max <= 32) return run<32>(p, s);

@@ -7,30 +7,37 @@
 // (TurboDecoderImpl::decodeBlock, src/detail/TurboDecoder/TurboDecoderImpl.cpp:31-72);
 // how it computes it is B200-shaped:
 //
-//   One CTA decodes one frame for all iterations.  The frame's two exchange arrays
-//   live in shared memory in natural bit order:
+//   One CTA of 2 * SEGS threads decodes one frame for all iterations.  The frame's
+//   two exchange arrays live in shared memory in natural bit order:
 //     X[k] = Ls[k] + e0[k]          (a-priori of constituent 1 before interleaving;
 //                                    also the partial a-posteriori sum)
 //     Y[k] = e1 at natural index k  (constituent 1 writes e1(t) to Y[pi(t)])
 //   so constituent 0 reads Ls + Y contiguously and constituent 1 gathers X[pi(t)].
 //
 //   Per half-iteration:
-//   A. 64 forward and 64 backward segments run concurrently (one thread each).  A
-//      segment starts from metrics obtained by a training run of G steps from a
+//   A. SEGS forward and SEGS backward segments run concurrently (one thread each).
+//      A segment starts from metrics obtained by a training run of G steps from a
 //      flat start, walks its steps and leaves metric checkpoints every 8 steps in
 //      global memory (L2) plus its end metrics in shared memory.
 //   A2. Verification.  Segment 0 (forward) and the last segment (backward) start
 //      from the exact trellis termination.  The training start of segment w is
-//      accepted when it matches, within FP32 rounding (kCloseTol), the end metrics
+//      accepted when it matches, within FP32 rounding (close8), the end metrics
 //      that segment w-1 computed from its own accepted start; otherwise segment w
-//      is recomputed from that end.  Rounds repeat until every boundary is
-//      accepted, so every checkpoint equals the full-frame recursion up to
-//      rounding.  (Max-log and log-MAP forget their start exponentially fast;
-//      training merely makes fix-ups rare.)
+//      is walked again from that end, until its metrics reproduce a checkpoint of
+//      the earlier walk.  Rounds repeat until every boundary is accepted, so every
+//      checkpoint equals the full-frame recursion up to rounding.  (Max-log and
+//      log-MAP forget their start exponentially fast; training merely makes
+//      fix-ups rare.)
 //   B. Every 8-step block is then independent: a thread reloads the forward
 //      checkpoint at the block start and the backward checkpoint at its end,
 //      recomputes the 8 forward vectors in registers and walks backward emitting
 //      the extrinsic values, scaled, minus the a-priori (MapDecoderImpl.cpp:203-212).
+//
+// The recursions subtract the largest state metric once per 8-step chunk (at every
+// checkpoint) rather than after every step as the reference does: the subtraction
+// cancels in every difference the decoder takes, so this changes FP32 rounding only,
+// and it removes the eight-way maximum and the subtractions from seven steps of
+// eight.  Global loads of the next chunk are issued one chunk ahead.
 //
 // Inputs are first converted into a padded FP32 scratch layout so that every
 // block load is 16-byte aligned.
@@ -43,11 +50,14 @@ namespace fecl {
 namespace {
 
 constexpr int kExact = 0, kLinear = 1, kApproximate = 2;
-constexpr int kThreads = 128;
-constexpr int kSegs = 64;  // segments per direction (one thread each)
-constexpr int kBlk = 8;    // checkpoint spacing / APP block length
+constexpr int kBlk = 8;  // checkpoint spacing / APP block length
 constexpr float kNegInf = -INFINITY;
-constexpr float kCloseTol = 1e-3f;
+// Boundary acceptance: |x - y| <= kAbsTol + kRelTol * max(|x|, |y|).  Two walks that
+// have forgotten their starts differ by the rounding of the steps since, which grows
+// with the metrics' magnitude (strong a-priori values late in a decode).
+constexpr float kAbsTol = 1e-3f;
+constexpr float kRelTol = 1e-5f;
+constexpr int kDefaultSegs = 64;
 
 __constant__ LinearLut c_lut;
 
@@ -65,15 +75,16 @@ __device__ __forceinline__ float lsum(float a, float b) {
   return fmaxf(a, b) + lut_log1pexpm(c_lut, fabsf(a - b));
 }
 
-// out[s] = n[s] - m for the 8 states, as four packed f32x2 adds of -m (x - m is
-// x + (-m) exactly, so the values are those of scalar subtractions).
-__device__ __forceinline__ void sub_max(const float n[8], float m, float out[8]) {
+// v[s] -= max(v), with the subtraction as four packed f32x2 adds of -m (x - m is
+// x + (-m) exactly).
+__device__ __forceinline__ void normalize8(float v[8]) {
+  const float m = fmaxf(fmaxf(fmaxf(v[0], v[1]), fmaxf(v[2], v[3])), fmaxf(fmaxf(v[4], v[5]), fmaxf(v[6], v[7])));
   const float2 nm = make_float2(-m, -m);
 #pragma unroll
   for (int s = 0; s < 8; s += 2) {
-    const float2 r = __fadd2_rn(make_float2(n[s], n[s + 1]), nm);
-    out[s] = r.x;
-    out[s + 1] = r.y;
+    const float2 r = __fadd2_rn(make_float2(v[s], v[s + 1]), nm);
+    v[s] = r.x;
+    v[s + 1] = r.y;
   }
 }
 
@@ -93,10 +104,9 @@ struct Gam {
     g[2] = la;
     g[3] = lp + la;
   }
-  __device__ __forceinline__ float of(int s, int u) const { return g[(u << 1) | lte_out(s, u)]; }
-  // x + gamma(s, u).  In max-log the branch with no 1 bits adds nothing: metrics are
-  // never -0 (the largest state normalises to +0, the others are below it), so x + 0
-  // is x and the add is skipped; the other algorithms keep the reference's adds.
+  // x + gamma(s, u).  In max-log the branch with no 1 bits adds nothing: x + 0 is x for
+  // every metric but -0, and a -0 metric (x == 0) only ever meets +0 in a maximum or a
+  // difference, which treat both alike; the other algorithms keep the reference's adds.
   template <int ALG>
   __device__ __forceinline__ float plus(float x, int s, int u) const {
     const int i = (u << 1) | lte_out(s, u);
@@ -105,75 +115,35 @@ struct Gam {
   }
 };
 
-// alpha_{t+1} from alpha_t (MapDecoderImpl.cpp:117-139, :237-274), normalised by its max.
+// alpha_{t+1} from alpha_t (MapDecoderImpl.cpp:117-139, :237-274), not normalised.
 template <int ALG>
 __device__ __forceinline__ void fwd_step(float a[8], const Gam& g) {
-  float n[8];
-  if (ALG == kExact) {
-    float c0[8], c1[8];
-    bool first[8];
+  float c0[8], c1[8];
+  bool first[8];
 #pragma unroll
-    for (int s = 0; s < 8; ++s) first[s] = true;
+  for (int s = 0; s < 8; ++s) first[s] = true;
 #pragma unroll
-    for (int s = 0; s < 8; ++s)
+  for (int s = 0; s < 8; ++s)
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int d = lte_next(s, u);
-        const float v = a[s] + g.of(s, u);
-        if (first[d]) {
-          c0[d] = v;
-          first[d] = false;
-        } else {
-          c1[d] = v;
-        }
+    for (int u = 0; u < 2; ++u) {
+      const int d = lte_next(s, u);
+      const float v = g.plus<ALG>(a[s], s, u);
+      if (first[d]) {
+        c0[d] = v;
+        first[d] = false;
+      } else {
+        c1[d] = v;
       }
+    }
 #pragma unroll
-    for (int s = 0; s < 8; ++s) n[s] = esum2(c0[s], c1[s]);
-  } else if (ALG == kApproximate) {
-    // max(max(-inf, first), second) of the two branches into each state
-    float c0[8], c1[8];
-    bool first[8];
-#pragma unroll
-    for (int s = 0; s < 8; ++s) first[s] = true;
-#pragma unroll
-    for (int s = 0; s < 8; ++s)
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int d = lte_next(s, u);
-        const float v = g.plus<ALG>(a[s], s, u);
-        if (first[d]) {
-          c0[d] = v;
-          first[d] = false;
-        } else {
-          c1[d] = v;
-        }
-      }
-#pragma unroll
-    for (int s = 0; s < 8; ++s) n[s] = fmaxf(c0[s], c1[s]);
-    float m = kNegInf;
-#pragma unroll
-    for (int s = 0; s < 8; ++s) m = fmaxf(n[s], m);
-    sub_max(n, m, a);
-    return;
-  } else {
-#pragma unroll
-    for (int s = 0; s < 8; ++s) n[s] = kNegInf;
-#pragma unroll
-    for (int s = 0; s < 8; ++s)
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int d = lte_next(s, u);
-        n[d] = lsum<ALG>(n[d], a[s] + g.of(s, u));
-      }
+  for (int s = 0; s < 8; ++s) {
+    if (ALG == kExact) a[s] = esum2(c0[s], c1[s]);
+    else if (ALG == kApproximate) a[s] = fmaxf(c0[s], c1[s]);
+    else a[s] = lsum<ALG>(lsum<ALG>(kNegInf, c0[s]), c1[s]);
   }
-  float m = kNegInf;
-#pragma unroll
-  for (int s = 0; s < 8; ++s) m = fmaxf(n[s], m);
-#pragma unroll
-  for (int s = 0; s < 8; ++s) a[s] = n[s] - m;
 }
 
-// beta_t from beta_{t+1} (MapDecoderImpl.cpp:141-172, :276-329), normalised by its max.
+// beta_t from beta_{t+1} (MapDecoderImpl.cpp:141-172, :276-329), not normalised.
 template <int ALG>
 __device__ __forceinline__ void bwd_step(float b[8], const Gam& g) {
   float n[8];
@@ -185,58 +155,64 @@ __device__ __forceinline__ void bwd_step(float b[8], const Gam& g) {
     else if (ALG == kApproximate) n[s] = fmaxf(x0, x1);
     else n[s] = lsum<ALG>(lsum<ALG>(kNegInf, x0), x1);
   }
-  if (ALG == kApproximate) {
-    float m = kNegInf;
 #pragma unroll
-    for (int s = 0; s < 8; ++s) m = fmaxf(n[s], m);
-    sub_max(n, m, b);
-    return;
-  }
-  float m = kNegInf;
-#pragma unroll
-  for (int s = 0; s < 8; ++s) m = fmaxf(n[s], m);
-#pragma unroll
-  for (int s = 0; s < 8; ++s) b[s] = n[s] - m;
+  for (int s = 0; s < 8; ++s) b[s] = n[s];
 }
 
-// L(u) = post(sum over u=1) - post(sum over u=0) (msgUpdateImpl, MapDecoderImpl.cpp:331-376).
+// Extrinsic value of one step, L(u) - La (msgUpdateImpl, MapDecoderImpl.cpp:331-376).
+// Max-log: L(u=1) = La + max_s(a[s] + b[next(s,1)] + p(s,1) Lp) and L(u=0) =
+// max_s(a[s] + b[next(s,0)] + p(s,0) Lp), so the a-priori value cancels and each
+// maximum splits by parity bit: the states with p(s,0) = 1 are 2..5 (and with
+// p(s,1) = 1 the others), so Lp is added once per maximum instead of once per state.
 template <int ALG>
-__device__ __forceinline__ float app_step(const float a[8], const float b[8], const Gam& g) {
-  float d[16];
-#pragma unroll
-  for (int s = 0; s < 8; ++s)
-#pragma unroll
-    for (int u = 0; u < 2; ++u) d[s * 2 + u] = g.plus<ALG>(a[s], s, u) + b[lte_next(s, u)];
-  if (ALG == kExact) {
-    float mx0 = kNegInf, mx1 = kNegInf;
+__device__ __forceinline__ float ext_step(const float a[8], const float b[8], const Gam& g) {
+  if constexpr (ALG == kApproximate) {
+    float w0[8], w1[8];
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
-      mx0 = fmaxf(d[s * 2], mx0);
-      mx1 = fmaxf(d[s * 2 + 1], mx1);
+      w0[s] = a[s] + b[lte_next(s, 0)];
+      w1[s] = a[s] + b[lte_next(s, 1)];
     }
-    float m0 = 0.0f, m1 = 0.0f;
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-      m0 = ((d[s * 2] == mx0) ? 1.0f : expf(d[s * 2] - mx0)) + m0;
-      m1 = ((d[s * 2 + 1] == mx1) ? 1.0f : expf(d[s * 2 + 1] - mx1)) + m1;
-    }
-    return (logf(m1) + mx1) - (logf(m0) + mx0);
-  } else if (ALG == kApproximate) {
-    float m0 = d[0], m1 = d[1];
-#pragma unroll
-    for (int s = 1; s < 8; ++s) {
-      m0 = fmaxf(m0, d[s * 2]);
-      m1 = fmaxf(m1, d[s * 2 + 1]);
-    }
+    const float lp = g.g[1];
+    // u = 0: parity 0 at s in {0,1,6,7}, parity 1 at {2,3,4,5}; u = 1 the reverse.
+    const float m0p0 = fmaxf(fmaxf(w0[0], w0[1]), fmaxf(w0[6], w0[7]));
+    const float m0p1 = fmaxf(fmaxf(w0[2], w0[3]), fmaxf(w0[4], w0[5]));
+    const float m1p0 = fmaxf(fmaxf(w1[2], w1[3]), fmaxf(w1[4], w1[5]));
+    const float m1p1 = fmaxf(fmaxf(w1[0], w1[1]), fmaxf(w1[6], w1[7]));
+    const float m0 = fmaxf(m0p0, m0p1 + lp);
+    const float m1 = fmaxf(m1p0, m1p1 + lp);
     return m1 - m0;
   } else {
-    float m0 = kNegInf, m1 = kNegInf;
+    float d[16];
 #pragma unroll
-    for (int s = 0; s < 8; ++s) {
-      m0 = lsum<ALG>(m0, d[s * 2]);
-      m1 = lsum<ALG>(m1, d[s * 2 + 1]);
+    for (int s = 0; s < 8; ++s)
+#pragma unroll
+      for (int u = 0; u < 2; ++u) d[s * 2 + u] = g.plus<ALG>(a[s], s, u) + b[lte_next(s, u)];
+    float l;
+    if (ALG == kExact) {
+      float mx0 = kNegInf, mx1 = kNegInf;
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        mx0 = fmaxf(d[s * 2], mx0);
+        mx1 = fmaxf(d[s * 2 + 1], mx1);
+      }
+      float m0 = 0.0f, m1 = 0.0f;
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        m0 = ((d[s * 2] == mx0) ? 1.0f : expf(d[s * 2] - mx0)) + m0;
+        m1 = ((d[s * 2 + 1] == mx1) ? 1.0f : expf(d[s * 2 + 1] - mx1)) + m1;
+      }
+      l = (logf(m1) + mx1) - (logf(m0) + mx0);
+    } else {
+      float m0 = kNegInf, m1 = kNegInf;
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        m0 = lsum<ALG>(m0, d[s * 2]);
+        m1 = lsum<ALG>(m1, d[s * 2 + 1]);
+      }
+      l = m1 - m0;
     }
-    return m1 - m0;
+    return l - g.g[2];
   }
 }
 
@@ -249,45 +225,58 @@ struct Frame {
   float* ckb;        // [nblk + 1][8]
 };
 
+template <int SEGS>
 struct Shared {
-  float sv[2][kSegs][8];  // metrics at the segment boundary after training (fwd, bwd)
-  float ev[2][kSegs][8];  // end metrics of each segment (fwd, bwd)
-  float in[2][kSegs][8];  // start metrics handed to a recomputed segment
-  float flat[8];          // training start: all states equal
-  float term[8];          // trellis termination: state 0
-  int bad[2][kSegs];
+  float sv[2][SEGS][8];  // metrics at the segment boundary after training (fwd, bwd)
+  float ev[2][SEGS][8];  // end metrics of each segment (fwd, bwd)
+  float flat[8];         // training start: all states equal
+  float term[8];         // trellis termination: state 0
+  int bad[2][SEGS];
   int any_bad;
-  uint32_t crc_part[kThreads / 32];  // per-warp CRC syndromes
+  uint32_t crc_part[2 * SEGS / 32];  // per-warp CRC syndromes
 };
 
-// Inputs of one 8-step chunk [8c, 8c + 8): a-priori and parity L-values.  Every
-// array read here is padded to Tp = 8 * nblk entries, so the vector loads stay
+// The global loads of one 8-step chunk [8c, 8c + 8): the parity L-values and either
+// the systematic L-values (constituent 0) or the interleaver entries (constituent 1).
+// Every array read here is padded to Tp = 8 * nblk entries, so the vector loads stay
 // inside the frame's scratch even for the chunk holding the tail steps.
+struct RawChunk {
+  float4 p0, p1;  // parity
+  uint4 q0, q1;   // systematic (as bits) or interleaver entries
+};
+
+__device__ __forceinline__ void load_raw(int j, int c, const Frame& fr, const uint32_t* __restrict__ perm,
+                                         RawChunk& r) {
+  const int t0 = c * kBlk;
+  const float* Lp = j == 0 ? fr.Lp0 : fr.Lp1;
+  r.p0 = __ldg(reinterpret_cast<const float4*>(Lp + t0));
+  r.p1 = __ldg(reinterpret_cast<const float4*>(Lp + t0) + 1);
+  const uint4* q = j == 0 ? reinterpret_cast<const uint4*>(fr.Ls + t0) : reinterpret_cast<const uint4*>(perm + t0);
+  r.q0 = __ldg(q);
+  r.q1 = __ldg(q + 1);
+}
+
+// A chunk's a-priori and parity L-values.
 struct Chunk {
   float la[kBlk];
   float lp[kBlk];
 };
 
-__device__ __forceinline__ void load_chunk(int j, int c, int K, const Frame& fr, const float* X, const float* Y,
-                                           const uint32_t* __restrict__ perm, Chunk& ch) {
+__device__ __forceinline__ void resolve(int j, int c, int K, const Frame& fr, const float* X, const float* Y,
+                                        const RawChunk& r, Chunk& ch) {
   const int t0 = c * kBlk;
-  const float* Lp = j == 0 ? fr.Lp0 : fr.Lp1;
-  const float4 p0 = __ldg(reinterpret_cast<const float4*>(Lp + t0));
-  const float4 p1 = __ldg(reinterpret_cast<const float4*>(Lp + t0) + 1);
-  ch.lp[0] = p0.x; ch.lp[1] = p0.y; ch.lp[2] = p0.z; ch.lp[3] = p0.w;
-  ch.lp[4] = p1.x; ch.lp[5] = p1.y; ch.lp[6] = p1.z; ch.lp[7] = p1.w;
+  ch.lp[0] = r.p0.x; ch.lp[1] = r.p0.y; ch.lp[2] = r.p0.z; ch.lp[3] = r.p0.w;
+  ch.lp[4] = r.p1.x; ch.lp[5] = r.p1.y; ch.lp[6] = r.p1.z; ch.lp[7] = r.p1.w;
   if (j == 0) {
-    const float4 s0 = __ldg(reinterpret_cast<const float4*>(fr.Ls + t0));
-    const float4 s1 = __ldg(reinterpret_cast<const float4*>(fr.Ls + t0) + 1);
     const float4 y0 = reinterpret_cast<const float4*>(Y + t0)[0];
     const float4 y1 = reinterpret_cast<const float4*>(Y + t0)[1];
-    ch.la[0] = s0.x + y0.x; ch.la[1] = s0.y + y0.y; ch.la[2] = s0.z + y0.z; ch.la[3] = s0.w + y0.w;
-    ch.la[4] = s1.x + y1.x; ch.la[5] = s1.y + y1.y; ch.la[6] = s1.z + y1.z; ch.la[7] = s1.w + y1.w;
+    ch.la[0] = __uint_as_float(r.q0.x) + y0.x; ch.la[1] = __uint_as_float(r.q0.y) + y0.y;
+    ch.la[2] = __uint_as_float(r.q0.z) + y0.z; ch.la[3] = __uint_as_float(r.q0.w) + y0.w;
+    ch.la[4] = __uint_as_float(r.q1.x) + y1.x; ch.la[5] = __uint_as_float(r.q1.y) + y1.y;
+    ch.la[6] = __uint_as_float(r.q1.z) + y1.z; ch.la[7] = __uint_as_float(r.q1.w) + y1.w;
   } else {
-    const uint4 q0 = __ldg(reinterpret_cast<const uint4*>(perm + t0));
-    const uint4 q1 = __ldg(reinterpret_cast<const uint4*>(perm + t0) + 1);
-    ch.la[0] = X[q0.x]; ch.la[1] = X[q0.y]; ch.la[2] = X[q0.z]; ch.la[3] = X[q0.w];
-    ch.la[4] = X[q1.x]; ch.la[5] = X[q1.y]; ch.la[6] = X[q1.z]; ch.la[7] = X[q1.w];
+    ch.la[0] = X[r.q0.x]; ch.la[1] = X[r.q0.y]; ch.la[2] = X[r.q0.z]; ch.la[3] = X[r.q0.w];
+    ch.la[4] = X[r.q1.x]; ch.la[5] = X[r.q1.y]; ch.la[6] = X[r.q1.z]; ch.la[7] = X[r.q1.w];
   }
   if (t0 + kBlk > K) {
 #pragma unroll
@@ -304,32 +293,66 @@ __device__ __forceinline__ void store_ck(float* ck, const float v[8]) {
   q[1] = make_float4(v[4], v[5], v[6], v[7]);
 }
 
+__device__ __forceinline__ void load_ck(const float* ck, float v[8]) {
+  const float4* q = reinterpret_cast<const float4*>(ck);
+  const float4 c0 = q[0], c1 = q[1];
+  v[0] = c0.x; v[1] = c0.y; v[2] = c0.z; v[3] = c0.w;
+  v[4] = c1.x; v[5] = c1.y; v[6] = c1.z; v[7] = c1.w;
+}
+
+__device__ __forceinline__ bool close8(const float* x, const float* y) {
+  bool ok = true;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    const float tol = kAbsTol + kRelTol * fmaxf(fabsf(x[s]), fabsf(y[s]));
+    ok = ok && ((x[s] == y[s]) || fabsf(x[s] - y[s]) <= tol);
+  }
+  return ok;
+}
+
 // One segment walk of constituent j, forward (fwd != 0) or backward.  The start
 // metrics are read from vin (shared memory).  Training steps outside the segment
 // run first without checkpoints -- forward over [t_train, a0), backward over
 // [a1, t_train) -- then the metrics at the segment boundary are written to vstart,
 // the segment's own steps run, leaving checkpoints at every multiple of 8 inside
 // [a0, a1) (and at T for the last backward segment), and the final metrics go to
-// vend.  Each 8-step chunk's inputs are fetched with 16-byte loads before its steps
-// run; other warps cover the latency.  Kept out of line so that Phase A and the
-// fix-up rounds share one copy of the code.
+// vend.  Metrics are normalised at the end of every chunk, so every checkpoint and
+// both boundary vectors have their largest state at 0.  The global loads of chunk
+// c + 1 are issued before chunk c runs.  A fix-up walk (`refine`) starts from a
+// corrected boundary over checkpoints an earlier walk of the same segment left; it
+// stops at the first checkpoint its metrics reproduce (close8): from there on the
+// earlier walk is the same recursion, so its checkpoints and end stand.  Kept out of
+// line so that Phase A and the fix-up rounds share one copy of the code.
 template <int ALG>
 __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, int a1, const float* vin, float* vstart,
                                           float* vend, int K, int T, Frame fr, const float* X, const float* Y,
-                                          const uint32_t* perm) {
+                                          const uint32_t* perm, bool refine) {
   float v[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) v[s] = vin[s];
   if (fwd) {
-    for (int c = t_train / kBlk; c * kBlk < a1; ++c) {
+    const int c_end = (a1 + kBlk - 1) / kBlk;
+    int c = t_train / kBlk;
+    RawChunk nxt;
+    load_raw(j, c, fr, perm, nxt);
+    for (; c < c_end; ++c) {
+      const RawChunk cur = nxt;
+      if (c + 1 < c_end) load_raw(j, c + 1, fr, perm, nxt);
       const int t0 = c * kBlk;
       if (t0 == a0) {
 #pragma unroll
         for (int s = 0; s < 8; ++s) vstart[s] = v[s];
       }
-      if (t0 >= a0) store_ck(fr.cka + c * 8, v);
+      if (t0 >= a0) {
+        if (refine && t0 > a0) {
+          float old[8];
+          load_ck(fr.cka + c * 8, old);
+          if (close8(v, old)) return;
+        }
+        store_ck(fr.cka + c * 8, v);
+      }
       Chunk ch;
-      load_chunk(j, c, K, fr, X, Y, perm, ch);
+      resolve(j, c, K, fr, X, Y, cur, ch);
       const int n = min(kBlk, a1 - t0);
 #pragma unroll
       for (int i = 0; i < kBlk; ++i) {
@@ -339,6 +362,7 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
           fwd_step<ALG>(v, g);
         }
       }
+      normalize8(v);
     }
   } else {
     const int nblk = (T + kBlk - 1) / kBlk;
@@ -347,9 +371,15 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
       for (int s = 0; s < 8; ++s) vstart[s] = v[s];
       if (a1 == T) store_ck(fr.ckb + nblk * 8, v);
     }
-    for (int c = (t_train - 1) / kBlk; c >= a0 / kBlk; --c) {
+    const int c_lo = a0 / kBlk;
+    int c = (t_train - 1) / kBlk;
+    RawChunk nxt;
+    load_raw(j, c, fr, perm, nxt);
+    for (; c >= c_lo; --c) {
+      const RawChunk cur = nxt;
+      if (c - 1 >= c_lo) load_raw(j, c - 1, fr, perm, nxt);
       Chunk ch;
-      load_chunk(j, c, K, fr, X, Y, perm, ch);
+      resolve(j, c, K, fr, X, Y, cur, ch);
       const int hi = min(kBlk, t_train - c * kBlk);
 #pragma unroll
       for (int i = kBlk - 1; i >= 0; --i) {
@@ -359,23 +389,24 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
           bwd_step<ALG>(v, g);
         }
       }
+      normalize8(v);
       const int tm = c * kBlk;  // v now holds the metrics at time tm
       if (tm == a1) {
 #pragma unroll
         for (int s = 0; s < 8; ++s) vstart[s] = v[s];
       }
-      if (tm >= a0 && tm < a1) store_ck(fr.ckb + c * 8, v);
+      if (tm >= a0 && tm < a1) {
+        if (refine) {
+          float old[8];
+          load_ck(fr.ckb + c * 8, old);
+          if (close8(v, old)) return;
+        }
+        store_ck(fr.ckb + c * 8, v);
+      }
     }
   }
 #pragma unroll
   for (int s = 0; s < 8; ++s) vend[s] = v[s];
-}
-
-__device__ __forceinline__ bool close8(const float* x, const float* y) {
-  bool ok = true;
-#pragma unroll
-  for (int s = 0; s < 8; ++s) ok = ok && ((x[s] == y[s]) || fabsf(x[s] - y[s]) <= kCloseTol);
-  return ok;
 }
 
 // One frame's geometry and buffers, as the decode loop below sees them.
@@ -391,15 +422,23 @@ struct LteJob {
   const uint32_t* crc = nullptr;        // [K] x^(K-1-i) mod g: stop when the decisions' CRC checks (nullable)
 };
 
-// Decodes one frame with the whole CTA; smem holds 2 * Kp floats + Shared.
-template <int ALG>
+// Segment length for a frame of T steps split into `segs` segments: a multiple of
+// the checkpoint spacing, so every segment boundary is a checkpoint.
+__host__ __device__ inline int lte_seg_len(int T, int segs) {
+  const int L = (T + segs - 1) / segs;
+  return (L + kBlk - 1) / kBlk * kBlk;
+}
+
+// Decodes one frame with the whole CTA; smem holds 2 * Kp floats + Shared<SEGS>.
+template <int ALG, int SEGS>
 __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
+  constexpr int kThreads = 2 * SEGS;
   const int K = q.K, T = q.K + 3;
   const int nblk = (T + kBlk - 1) / kBlk;
   const int nblk_msg = (K + kBlk - 1) / kBlk;
   float* X = smem;
   float* Y = smem + q.Kp;
-  Shared& sh = *reinterpret_cast<Shared*>(smem + 2 * q.Kp);
+  Shared<SEGS>& sh = *reinterpret_cast<Shared<SEGS>*>(smem + 2 * q.Kp);
   Frame fr;
   const float* base = q.scratch;
   fr.Ls = base;
@@ -428,8 +467,8 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
       const uint32_t* perm = q.perm;
       // ---- A: segments with training starts
       {
-        const bool fwd = tid < kSegs;
-        const int w = fwd ? tid : tid - kSegs;
+        const bool fwd = tid < SEGS;
+        const int w = fwd ? tid : tid - SEGS;
         if (w < S) {
           const int a0 = w * L, a1 = min(T, a0 + L);
           int t_train;
@@ -444,18 +483,18 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
             vin = exact ? sh.term : sh.flat;
           }
           segment_walk<ALG>(fwd, j, t_train, a0, a1, vin, sh.sv[fwd ? 0 : 1][w], sh.ev[fwd ? 0 : 1][w], K, T, fr, X,
-                            Y, perm);
+                            Y, perm, false);
         }
       }
       __syncthreads();
-      // ---- A2: verify boundaries; recompute segments whose start disagrees
+      // ---- A2: verify boundaries; walk again the segments whose start disagrees
       int rounds = 0;
       for (int round = 0; round < S; ++round) {
         if (tid == 0) sh.any_bad = 0;
         __syncthreads();
         {
-          const bool fwd = tid < kSegs;
-          const int w = fwd ? tid : tid - kSegs;
+          const bool fwd = tid < SEGS;
+          const int w = fwd ? tid : tid - SEGS;
           int bad = 0;
           if (w < S) {
             if (fwd && w > 0) bad = !close8(sh.sv[0][w], sh.ev[0][w - 1]);
@@ -468,23 +507,26 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
         if (!sh.any_bad) break;
         ++rounds;
         {
-          // Recompute every rejected segment from its neighbour's end.  The ends are
-          // copied before the barrier and rewritten after it, so a neighbour that is
-          // itself being recomputed is read in its old state; the next round checks
-          // the boundary again.
-          const bool fwd = tid < kSegs;
-          const int w = fwd ? tid : tid - kSegs;
+          // Walk every rejected segment again from its neighbour's end.  The end is
+          // copied to registers before the barrier and becomes the segment's start
+          // after it, so a neighbour that is itself being walked again is read in its
+          // old state; the next round checks the boundary again.
+          const bool fwd = tid < SEGS;
+          const int w = fwd ? tid : tid - SEGS;
           const bool mine = w < S && sh.bad[fwd ? 0 : 1][w];
+          float start[8];
           if (mine) {
 #pragma unroll
-            for (int s = 0; s < 8; ++s) sh.in[fwd ? 0 : 1][w][s] = fwd ? sh.ev[0][w - 1][s] : sh.ev[1][w + 1][s];
+            for (int s = 0; s < 8; ++s) start[s] = fwd ? sh.ev[0][w - 1][s] : sh.ev[1][w + 1][s];
           }
           __syncthreads();
           if (mine) {
             if (q.stats) atomicAdd(q.stats + 2, 1ull);
+            float* sv = sh.sv[fwd ? 0 : 1][w];
+#pragma unroll
+            for (int s = 0; s < 8; ++s) sv[s] = start[s];
             const int a0 = w * L, a1 = min(T, a0 + L);
-            segment_walk<ALG>(fwd, j, fwd ? a0 : a1, a0, a1, sh.in[fwd ? 0 : 1][w], sh.sv[fwd ? 0 : 1][w],
-                              sh.ev[fwd ? 0 : 1][w], K, T, fr, X, Y, perm);
+            segment_walk<ALG>(fwd, j, fwd ? a0 : a1, a0, a1, sv, sv, sh.ev[fwd ? 0 : 1][w], K, T, fr, X, Y, perm, true);
           }
         }
         __syncthreads();
@@ -502,15 +544,14 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
       for (int b = tid; b < nblk_msg; b += kThreads) {
         const int t0 = b * kBlk;
         const int n = min(kBlk, T - t0);
+        RawChunk raw;
+        load_raw(j, b, fr, perm, raw);
         float al[kBlk][8];
-        {
-          const float4* ck = reinterpret_cast<const float4*>(fr.cka + b * 8);
-          const float4 c0 = ck[0], c1 = ck[1];
-          al[0][0] = c0.x; al[0][1] = c0.y; al[0][2] = c0.z; al[0][3] = c0.w;
-          al[0][4] = c1.x; al[0][5] = c1.y; al[0][6] = c1.z; al[0][7] = c1.w;
-        }
+        load_ck(fr.cka + b * 8, al[0]);
+        float be[8];
+        load_ck(fr.ckb + (b + 1) * 8, be);
         Chunk in;
-        load_chunk(j, b, K, fr, X, Y, perm, in);
+        resolve(j, b, K, fr, X, Y, raw, in);
 #pragma unroll
         for (int i = 1; i < kBlk; ++i) {
           if (i < n) {
@@ -521,32 +562,21 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
             fwd_step<ALG>(al[i], g);
           }
         }
-        float be[8];
-        {
-          const float4* ck = reinterpret_cast<const float4*>(fr.ckb + (b + 1) * 8);
-          const float4 c0 = ck[0], c1 = ck[1];
-          be[0] = c0.x; be[1] = c0.y; be[2] = c0.z; be[3] = c0.w;
-          be[4] = c1.x; be[5] = c1.y; be[6] = c1.z; be[7] = c1.w;
-        }
-        float ext[kBlk];
+        const float ls[kBlk] = {__uint_as_float(raw.q0.x), __uint_as_float(raw.q0.y), __uint_as_float(raw.q0.z),
+                                __uint_as_float(raw.q0.w), __uint_as_float(raw.q1.x), __uint_as_float(raw.q1.y),
+                                __uint_as_float(raw.q1.z), __uint_as_float(raw.q1.w)};
+        const uint32_t pq[kBlk] = {raw.q0.x, raw.q0.y, raw.q0.z, raw.q0.w, raw.q1.x, raw.q1.y, raw.q1.z, raw.q1.w};
 #pragma unroll
         for (int i = kBlk - 1; i >= 0; --i) {
           if (i < n) {
             Gam g;
             g.set(in.la[i], in.lp[i]);
-            const float l = app_step<ALG>(al[i], be, g);
-            ext[i] = sf * (l - in.la[i]);
-            if (i > 0) bwd_step<ALG>(be, g);
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < kBlk; ++i) {
-          if (i < n) {
-            const int t = t0 + i;
-            if (t < K) {
-              if (j == 0) out[t] = fr.Ls[t] + ext[i];
-              else out[perm[t]] = ext[i];
+            const float e = sf * ext_step<ALG>(al[i], be, g);
+            if (t0 + i < K) {
+              if (j == 0) out[t0 + i] = ls[i] + e;
+              else out[pq[i]] = e;
             }
+            if (i > 0) bwd_step<ALG>(be, g);
           }
         }
       }
@@ -578,8 +608,8 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
   if (q.iters && tid == 0) *q.iters = ran;
 }
 
-template <int ALG>
-__global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p) {
+template <int ALG, int SEGS>
+__global__ void __launch_bounds__(2 * SEGS, SEGS == 32 ? 4 : 3) turbo_lte_kernel(TurboLteParams p) {
   extern __shared__ float smem[];
   const int64_t f = blockIdx.x;
   const int nblk = (p.K + 3 + kBlk - 1) / kBlk;
@@ -598,7 +628,7 @@ __global__ void __launch_bounds__(kThreads, 3) turbo_lte_kernel(TurboLteParams p
   q.iters = p.iters ? p.iters + f : nullptr;
   q.stats = p.stats;
   q.crc = p.crc;
-  decode_lte_frame<ALG>(q, smem);
+  decode_lte_frame<ALG, SEGS>(q, smem);
 }
 
 
@@ -630,17 +660,16 @@ __global__ void turbo_lte_stage(TurboLteParams p) {
 
 // Geometry of a frame of K message bits: T trellis steps, nblk 8-step blocks, the
 // padded systematic / parity lengths Kp = Tp, the staged-input stride and the
-// segment length of the 64 forward and 64 backward segments.
+// segment length of the `segs` forward and `segs` backward segments.
 struct LteGeometry {
   int T, nblk, Tp, Kp, stride, seg_len;
-  __host__ __device__ explicit LteGeometry(int K) {
+  __host__ __device__ LteGeometry(int K, int segs) {
     T = K + 3;
     nblk = (T + kBlk - 1) / kBlk;
     Tp = nblk * kBlk;
     Kp = Tp;
     stride = Kp + 2 * Tp + 8;
-    const int L = (T + kSegs - 1) / kSegs;
-    seg_len = (L + kBlk - 1) / kBlk * kBlk;
+    seg_len = lte_seg_len(T, segs);
   }
   // Staged inputs then checkpoints, rounded to 128 bytes so frames share no cache line.
   __host__ __device__ int frame_floats() const { return (stride + 2 * (nblk + 1) * 8 + 31) & ~31; }
@@ -662,7 +691,7 @@ __device__ __forceinline__ float staged_value(const void* llr, int dtype, int64_
 __global__ void turbo_lte_batch_stage(TurboLteBatchParams p) {
   for (int64_t f = blockIdx.x; f < p.nframes; f += gridDim.x) {
     const TurboLteBatchFrame d = p.frames[f];
-    const LteGeometry g(d.K);
+    const LteGeometry g(d.K, kDefaultSegs);
     for (int i = threadIdx.x; i < g.stride; i += blockDim.x)
       d.scratch[i] = staged_value(d.llr, d.llr_dtype, 0, d.K, g.Kp, g.Tp, i);
   }
@@ -671,8 +700,8 @@ __global__ void turbo_lte_batch_stage(TurboLteBatchParams p) {
 // Mixed-K batch, decoding: persistent CTAs take frames from a counter in the order
 // of the descriptor table (longest first), so frames of every size share one launch
 // and the long ones do not trail behind.  Shared memory is sized for the largest K.
-template <int ALG>
-__global__ void __launch_bounds__(kThreads, 3) turbo_lte_batch_kernel(TurboLteBatchParams p) {
+template <int ALG, int SEGS>
+__global__ void __launch_bounds__(2 * SEGS, SEGS == 32 ? 4 : 3) turbo_lte_batch_kernel(TurboLteBatchParams p) {
   extern __shared__ float smem[];
   __shared__ int next;
   for (;;) {
@@ -682,7 +711,7 @@ __global__ void __launch_bounds__(kThreads, 3) turbo_lte_batch_kernel(TurboLteBa
     const int64_t f = next;
     if (f >= p.nframes) break;
     const TurboLteBatchFrame d = p.frames[f];
-    const LteGeometry g(d.K);
+    const LteGeometry g(d.K, SEGS);
     LteJob q;
     q.K = d.K;
     q.Kp = g.Kp;
@@ -698,11 +727,16 @@ __global__ void __launch_bounds__(kThreads, 3) turbo_lte_batch_kernel(TurboLteBa
     q.iters = d.iters;
     q.stats = p.stats;
     q.crc = d.crc;
-    decode_lte_frame<ALG>(q, smem);
+    decode_lte_frame<ALG, SEGS>(q, smem);
   }
 }
 
-size_t batch_smem_bytes(int max_K) { return size_t(2 * LteGeometry(max_K).Kp) * sizeof(float) + sizeof(Shared); }
+template <int SEGS>
+size_t lte_smem_bytes(int max_K) {
+  return size_t(2 * LteGeometry(max_K, SEGS).Kp) * sizeof(float) + sizeof(Shared<SEGS>);
+}
+
+int resolve_segs(int segs) { return segs == 32 ? 32 : (segs == 64 ? 64 : kDefaultSegs); }
 
 }  // namespace
 
@@ -727,15 +761,13 @@ cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
   cudaError_t e0 = turbo_lte_init();
   if (e0 != cudaSuccess) return e0;
   if (p.nframes <= 0) return cudaSuccess;
-  const int T = p.K + 3;
-  const int nblk = (T + kBlk - 1) / kBlk;
-  p.Tp = nblk * kBlk;
-  p.Kp = p.Tp;  // the systematic region and the exchange arrays are padded like the parity
-  p.frame_stride = p.Kp + 2 * p.Tp + 8;
+  const int segs = resolve_segs(p.segs);
+  const LteGeometry g(p.K, segs);
+  p.Tp = g.Tp;
+  p.Kp = g.Kp;  // the systematic region and the exchange arrays are padded like the parity
+  p.frame_stride = g.stride;
   p.ck = p.scratch + p.nframes * p.frame_stride;
-  int L = (T + kSegs - 1) / kSegs;
-  L = (L + kBlk - 1) / kBlk * kBlk;
-  p.seg_len = L;
+  p.seg_len = g.seg_len;
   if (p.train < 0) p.train = 96;
   const unsigned stage_blocks = unsigned(p.nframes < 148 * 8 ? p.nframes : 148 * 8);
   switch (p.llr_dtype) {
@@ -743,36 +775,44 @@ cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
     case kF16: turbo_lte_stage<__half><<<stage_blocks, 256, 0, s>>>(p); break;
     default: turbo_lte_stage<float><<<stage_blocks, 256, 0, s>>>(p); break;
   }
-  const size_t smem = size_t(2 * p.Kp) * sizeof(float) + sizeof(Shared);
-  auto launch = [&](auto kern) -> cudaError_t {
+  auto launch = [&](auto kern, int threads, size_t smem) -> cudaError_t {
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (err != cudaSuccess) return err;
-    kern<<<unsigned(p.nframes), kThreads, smem, s>>>(p);
+    kern<<<unsigned(p.nframes), threads, smem, s>>>(p);
     return cudaGetLastError();
   };
+  if (segs == 32) {
+    const size_t smem = lte_smem_bytes<32>(p.K);
+    switch (p.algorithm) {
+      case kExact: return launch(turbo_lte_kernel<kExact, 32>, 64, smem);
+      case kLinear: return launch(turbo_lte_kernel<kLinear, 32>, 64, smem);
+      default: return launch(turbo_lte_kernel<kApproximate, 32>, 64, smem);
+    }
+  }
+  const size_t smem = lte_smem_bytes<64>(p.K);
   switch (p.algorithm) {
-    case kExact: return launch(turbo_lte_kernel<kExact>);
-    case kLinear: return launch(turbo_lte_kernel<kLinear>);
-    default: return launch(turbo_lte_kernel<kApproximate>);
+    case kExact: return launch(turbo_lte_kernel<kExact, 64>, 128, smem);
+    case kLinear: return launch(turbo_lte_kernel<kLinear, 64>, 128, smem);
+    default: return launch(turbo_lte_kernel<kApproximate, 64>, 128, smem);
   }
 }
 
-size_t turbo_lte_frame_floats(int K) { return size_t(LteGeometry(K).frame_floats()); }
+size_t turbo_lte_frame_floats(int K) { return size_t(LteGeometry(K, kDefaultSegs).frame_floats()); }
 
 int turbo_lte_batch_max_ctas(int max_K, int algorithm) {
-  const size_t smem = batch_smem_bytes(max_K);
+  const size_t smem = lte_smem_bytes<kDefaultSegs>(max_K);
   int per_sm = 0, sms = 0, dev = 0;
   auto q = [&](auto kern) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem) != cudaSuccess) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 2 * kDefaultSegs, smem) != cudaSuccess) {
       cudaGetLastError();
       per_sm = 0;
     }
   };
   switch (algorithm) {
-    case kExact: q(turbo_lte_batch_kernel<kExact>); break;
-    case kLinear: q(turbo_lte_batch_kernel<kLinear>); break;
-    default: q(turbo_lte_batch_kernel<kApproximate>); break;
+    case kExact: q(turbo_lte_batch_kernel<kExact, kDefaultSegs>); break;
+    case kLinear: q(turbo_lte_batch_kernel<kLinear, kDefaultSegs>); break;
+    default: q(turbo_lte_batch_kernel<kApproximate, kDefaultSegs>); break;
   }
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
     cudaGetLastError();
@@ -792,20 +832,20 @@ cudaError_t launch_turbo_lte_batch(const TurboLteBatchParams& p, cudaStream_t s)
   if (e != cudaSuccess) return e;
   const unsigned stage_blocks = unsigned(q.nframes < 148 * 8 ? q.nframes : 148 * 8);
   turbo_lte_batch_stage<<<stage_blocks, 256, 0, s>>>(q);
-  const size_t smem = batch_smem_bytes(q.max_K);
+  const size_t smem = lte_smem_bytes<kDefaultSegs>(q.max_K);
   int ctas = q.ctas > 0 ? q.ctas : turbo_lte_batch_max_ctas(q.max_K, q.algorithm);
   if (ctas <= 0) return cudaErrorInvalidConfiguration;
   if (int64_t(ctas) > q.nframes) ctas = int(q.nframes);
   auto launch = [&](auto kern) -> cudaError_t {
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (err != cudaSuccess) return err;
-    kern<<<unsigned(ctas), kThreads, smem, s>>>(q);
+    kern<<<unsigned(ctas), 2 * kDefaultSegs, smem, s>>>(q);
     return cudaGetLastError();
   };
   switch (q.algorithm) {
-    case kExact: return launch(turbo_lte_batch_kernel<kExact>);
-    case kLinear: return launch(turbo_lte_batch_kernel<kLinear>);
-    default: return launch(turbo_lte_batch_kernel<kApproximate>);
+    case kExact: return launch(turbo_lte_batch_kernel<kExact, kDefaultSegs>);
+    case kLinear: return launch(turbo_lte_batch_kernel<kLinear, kDefaultSegs>);
+    default: return launch(turbo_lte_batch_kernel<kApproximate, kDefaultSegs>);
   }
 }
 

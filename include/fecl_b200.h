@@ -315,11 +315,27 @@ int fecl_ldpc_set_cluster_shape(fecl_codec_t codec, int32_t cluster, int32_t thr
  * (the groups whose messages fit in 64 MiB of L2). */
 int fecl_ldpc_set_wave(fecl_codec_t codec, int32_t groups);
 
+/* Lane-batched LDPC decoder: run a small batch (at most 16 frame groups, one wave)
+ * as one persistent launch whose check and bit passes are separated by grid-wide
+ * barriers, instead of two launches per iteration.  mode 0: only for batches of at
+ * most 4 groups (where launches dominate); 1: wherever it applies; -1: never.  The
+ * results are those of the two-launch form bit for bit.  A barrier wait is bounded
+ * (2 s); a decode whose barrier gave up reports -1 iterations for its frames.
+ * Extension: no counterpart in the reference. */
+int fecl_ldpc_set_persistent(fecl_codec_t codec, int32_t mode);
+
 /* Windowed turbo decoder: training steps run before each segment's forward and
  * backward walk (a multiple of 8; -1 restores the default of 96).  Training only
  * sets how often a segment boundary fails verification and is recomputed; results
  * do not depend on it beyond FP32 rounding. */
 int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps);
+
+/* Windowed turbo decoder: forward (and backward) segments per frame, 32 or 64, one
+ * thread each (0 restores the built-in choice).  Fewer, longer segments spend a
+ * smaller share of each walk on training and fit more frames on an SM; results do
+ * not depend on it beyond FP32 rounding.  Extension: no counterpart in the
+ * reference. */
+int fecl_turbo_set_window_segments(fecl_codec_t codec, int32_t segments);
 
 /* Windowed turbo decoder counters since the previous call (which resets them):
  * constituent passes run, verification rounds that found a boundary to
@@ -352,7 +368,10 @@ int fecl_lte_turbo_decode_noalloc(uint32_t K, int32_t algorithm, uint32_t iterat
  * A batch decodes the frames of several codecs -- LDPC codes of any size and rate,
  * LTE turbo codes of any K, any other turbo code -- with one CUDA graph launch.
  * Every LTE turbo frame goes into one persistent launch over all K (longest
- * frames first); every other job gets the decoder fecl_decode would pick for it,
+ * frames first); the LDPC jobs that take the packed FP16 decoder run in one
+ * persistent launch per check-degree class (every code's frame groups, wave by
+ * wave, grid barriers between the passes); every other job gets the decoder
+ * fecl_decode would pick for it,
  * or, with FECL_BATCH_AUTOTUNE, the fastest of the LDPC kernel shapes that compute
  * the same bits, timed on the job's own data at creation and remembered for the
  * process.  Results equal those of fecl_decode on each job alone, bit for bit.
@@ -372,6 +391,10 @@ typedef struct {
   int32_t* iterations; /* [nframes] or NULL */
 } fecl_batch_job;
 #define FECL_BATCH_AUTOTUNE 1
+/* Every LDPC job runs its own launches.  By default the jobs that take the packed
+ * FP16 decoder share one persistent launch per check-degree class, wave by wave
+ * (the same bits either way). */
+#define FECL_BATCH_PER_JOB 2
 int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags, fecl_batch_t* out);
 /* Launches the batch's graph on `stream` (asynchronous). */
 int fecl_batch_run(fecl_batch_t batch, void* stream);

@@ -92,3 +92,40 @@ def test_batch_rerun_with_new_inputs_and_option_change():
     code.setDecoderOptions(F.Ldpc.DecoderOptions().algorithm(F.Approximate).iterations(10))
     with pytest.raises(ValueError):
         b.run()
+
+
+@pytest.mark.parametrize("shared", [True, False])
+def test_batch_shared_ldpc_launch_equals_each_codec_alone(shared):
+    """FP16-message LDPC jobs of several codes and check-degree classes, several
+    frame groups each and more than one wave, beside turbo frames: with the shared
+    persistent LDPC launch (and without it) every job's decisions and iteration
+    counts equal its codec's own decode bit for bit, on two runs in a row."""
+    import torch
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    dec = F.Ldpc.DecoderOptions().algorithm(F.Approximate).iterations(50).scalingFactor(0.75).precision(1)
+    specs = []
+    for (n, r, frames, ebn0) in ((16200, (1, 2), 70, 1.3), (16200, (3, 4), 130, 2.6), (16200, (5, 6), 20, 3.4),
+                                 (64800, (1, 2), 65, 1.5), (64800, (9, 10), 10, 3.9), (16200, (2, 3), 3, 2.0)):
+        H = F.Ldpc.DvbS2.matrix(n, Fraction(*r))
+        specs.append((F.Ldpc(F.Ldpc.EncoderOptions(H), dec), frames, ebn0))
+    specs.append((F.Turbo.lte(1024, F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(6)), 5, 0.8))
+    jobs = []
+    for i, (code, nf, ebn0) in enumerate(specs):
+        K, N = code.msgSize(), code.paritySize()
+        msg = ch.random_bits(nf * K, 300 + i)
+        llr = ch.awgn_llr(code.encode(msg), ebn0, K / N, 300 + i, np.float16)
+        jobs.append((code, torch.from_numpy(llr).cuda(), torch.zeros(nf * K, dtype=torch.uint8, device="cuda"),
+                     torch.zeros(nf, dtype=torch.int32, device="cuda")))
+    ref = _alone(jobs)
+    b = F.Batch(jobs, shared_ldpc=shared)
+    assert ("shared launch" in b.describe()) == shared
+    for rep in range(2):
+        for _, _, m, it in jobs:
+            m.fill_(7)
+            it.fill_(-7)
+        b.run()
+        torch.cuda.synchronize()
+        for (code, _, m, it), (rb, ri) in zip(jobs, ref):
+            assert np.array_equal(it.cpu().numpy(), ri), (rep, code.msgSize())
+            assert np.array_equal(m.cpu().numpy(), rb), (rep, code.msgSize())

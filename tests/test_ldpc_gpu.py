@@ -371,3 +371,35 @@ def test_packed_fp16_soft_state_falls_back_to_fp32_arithmetic():
     code.setKernel("lanes")
     b = code.soDecode(F.Codec.Input().parity(llr).state(st), F.Codec.Output(np.float32).msg()).msg()
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("alg,precision,frames,n", [(0, 0, 40, 16200), (1, 0, 40, 16200), (2, 0, 200, 16200),
+                                                    (2, 1, 130, 16200), (2, 2, 40, 16200), (2, 1, 64, 64800)])
+def test_persistent_launch_equals_launch_per_pass(alg, precision, frames, n):
+    """A small batch decoded by one persistent launch (check and bit passes separated
+    by grid barriers) and by two launches per iteration: the same outputs bit for bit,
+    iteration counts and soft outputs included, from device and from host memory (the
+    host path decodes its chunks on several streams)."""
+    import torch
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    H = F.Ldpc.DvbS2.matrix(n, Fraction(1, 2))
+    code = F.Ldpc(F.Ldpc.EncoderOptions(H), F.Ldpc.DecoderOptions().algorithm(alg).iterations(30)
+                  .scalingFactor(0.75 if alg == 2 else 1.0).precision(precision))
+    K, N = code.msgSize(), code.paritySize()
+    msg = ch.random_bits(frames * K, 40 + alg)
+    llr = ch.awgn_llr(code.encode(msg), 1.2 if n == 16200 else 1.0, K / N, 40 + alg, np.float32)
+    d_llr = torch.from_numpy(llr).cuda()
+    outs = {}
+    for mode in (1, -1):
+        code.setPersistent(mode)
+        bits, its = code.decode(d_llr, iterations=True)
+        hbits = code.decode(llr)
+        res = [bits.cpu().numpy(), its.cpu().numpy(), hbits]
+        if precision == 0:
+            so = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output(np.float32).msg().state())
+            res += [so.msg(), so.state()]
+        outs[mode] = res
+    assert np.all(outs[1][1] > 0)
+    for a, b in zip(outs[1], outs[-1]):
+        assert np.array_equal(a, b)
