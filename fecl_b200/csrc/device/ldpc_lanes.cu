@@ -182,25 +182,28 @@ __device__ __forceinline__ void retire_group(const LdpcLanesParams& p, int it, i
 }
 
 // app = chan + sum of c2v over bit b's edges, in increasing edge order, for this lane.
+// The edges go in runs of 8 (one run for most bits): every edge id of a run is loaded,
+// then every message, then they are added in order, so a bit costs three dependent
+// loads rather than two per edge.
 template <int MSG>
 __device__ __forceinline__ void bit_one(const LdpcLanesParams& p, int g, int b, int lane) {
   using M = Msg<MSG>;
+  constexpr uint32_t kRun = 8;
   const typename M::T* cg = static_cast<const typename M::T*>(p.c2v) + int64_t(g) * p.E * kLanes + lane;
   const int64_t base = (int64_t(g) * p.N + b) * kLanes + lane;
   const uint32_t k0 = __ldg(p.col_ptr + b), k1 = __ldg(p.col_ptr + b + 1);
   float acc = p.chan[base];
-  uint32_t k = k0;
-  for (; k + 4 <= k1; k += 4) {
-    const uint32_t e_0 = __ldg(p.col_edges + k), e_1 = __ldg(p.col_edges + k + 1);
-    const uint32_t e_2 = __ldg(p.col_edges + k + 2), e_3 = __ldg(p.col_edges + k + 3);
-    const float x0 = M::load(cg + int64_t(e_0) * kLanes), x1 = M::load(cg + int64_t(e_1) * kLanes);
-    const float x2 = M::load(cg + int64_t(e_2) * kLanes), x3 = M::load(cg + int64_t(e_3) * kLanes);
-    acc += x0;
-    acc += x1;
-    acc += x2;
-    acc += x3;
+  for (uint32_t k = k0; k < k1; k += kRun) {
+    uint32_t e[kRun];
+    float x[kRun];
+#pragma unroll
+    for (uint32_t j = 0; j < kRun; ++j) e[j] = k + j < k1 ? __ldg(p.col_edges + k + j) : 0u;
+#pragma unroll
+    for (uint32_t j = 0; j < kRun; ++j) x[j] = k + j < k1 ? M::load(cg + int64_t(e[j]) * kLanes) : 0.0f;
+#pragma unroll
+    for (uint32_t j = 0; j < kRun; ++j)
+      if (k + j < k1) acc += x[j];
   }
-  for (; k < k1; ++k) acc += M::load(cg + int64_t(__ldg(p.col_edges + k)) * kLanes);
   p.app[base] = acc;
 }
 
@@ -263,9 +266,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_persist(LdpcLanesPa
     if (!(ok = grid_barrier(p.barrier, p.barrier + 1, epoch))) break;
     // bit pass, and block 0 retires the frames
     if (blockIdx.x == 0 && threadIdx.x < ng) retire_group(p, it, threadIdx.x, active_of(p, it)[threadIdx.x]);
+    g_cur = -1;
     for (int64_t u = warp; u < int64_t(ng) * p.N; u += warps) {
       const int g = int(u / p.N);
-      if ((active_of(p, it)[g] >> lane) & 1) bit_one<MSG>(p, g, int(u % p.N), lane);
+      if (g != g_cur) {
+        g_cur = g;
+        active = active_of(p, it)[g];
+      }
+      if ((active >> lane) & 1) bit_one<MSG>(p, g, int(u % p.N), lane);
     }
     if (!(ok = grid_barrier(p.barrier, p.barrier + 1, epoch))) break;
     uint32_t left = 0;

@@ -205,26 +205,28 @@ __device__ __forceinline__ void retire_half(const LdpcLanesParams& p, int it, in
 }
 
 // app = chan + sum of c2v over bit b's edges (edge order, FP32) for this lane's two
-// frames; a retired frame's value stays.
+// frames; a retired frame's value stays.  The edges go in runs of 8 (one run for most
+// bits): every edge id of a run is loaded, then every message, then they are added in
+// order, so a bit costs three dependent loads rather than two per edge.
 __device__ __forceinline__ void bit_one(const LdpcLanesParams& p, int g, int b, int lane, bool mx, bool my) {
+  constexpr uint32_t kRun = 8;
   const __half2* cg = static_cast<const __half2*>(p.c2v) + int64_t(g) * p.E * kLanes + lane;
   const float2* chan = reinterpret_cast<const float2*>(p.chan);
   float2* app = reinterpret_cast<float2*>(p.app);
   const int64_t base = (int64_t(g) * p.N + b) * kLanes + lane;
   const uint32_t k0 = __ldg(p.col_ptr + b), k1 = __ldg(p.col_ptr + b + 1);
   float2 acc = chan[base];
-  uint32_t k = k0;
-  for (; k + 4 <= k1; k += 4) {
-    const uint32_t e_0 = __ldg(p.col_edges + k), e_1 = __ldg(p.col_edges + k + 1);
-    const uint32_t e_2 = __ldg(p.col_edges + k + 2), e_3 = __ldg(p.col_edges + k + 3);
-    const float2 x0 = __half22float2(cg[int64_t(e_0) * kLanes]), x1 = __half22float2(cg[int64_t(e_1) * kLanes]);
-    const float2 x2 = __half22float2(cg[int64_t(e_2) * kLanes]), x3 = __half22float2(cg[int64_t(e_3) * kLanes]);
-    acc = __fadd2_rn(acc, x0);
-    acc = __fadd2_rn(acc, x1);
-    acc = __fadd2_rn(acc, x2);
-    acc = __fadd2_rn(acc, x3);
+  for (uint32_t k = k0; k < k1; k += kRun) {
+    uint32_t e[kRun];
+    __half2 x[kRun];
+#pragma unroll
+    for (uint32_t j = 0; j < kRun; ++j) e[j] = k + j < k1 ? __ldg(p.col_edges + k + j) : 0u;
+#pragma unroll
+    for (uint32_t j = 0; j < kRun; ++j) x[j] = k + j < k1 ? cg[int64_t(e[j]) * kLanes] : __half2{};
+#pragma unroll
+    for (uint32_t j = 0; j < kRun; ++j)
+      if (k + j < k1) acc = __fadd2_rn(acc, __half22float2(x[j]));
   }
-  for (; k < k1; ++k) acc = __fadd2_rn(acc, __half22float2(cg[int64_t(__ldg(p.col_edges + k)) * kLanes]));
   if (mx && my) {
     app[base] = acc;
   } else {  // one of the lane's frames has retired: its APP stays
@@ -295,9 +297,15 @@ __global__ void __launch_bounds__(kWarps * 32) h2_persist(LdpcLanesParams p) {
     if (threadIdx.x < 2 * ng && s_bad[threadIdx.x]) atomicOr(fail_of(p, it) + threadIdx.x, s_bad[threadIdx.x]);
     if (!(ok = grid_barrier(p.barrier, p.barrier + 1, epoch))) break;
     if (blockIdx.x == 0 && threadIdx.x < 2 * ng) retire_half(p, it, threadIdx.x >> 1, threadIdx.x & 1);
+    g_cur = -1;
     for (int64_t u = warp; u < int64_t(ng) * p.N; u += warps) {
       const int g = int(u / p.N);
-      const bool mx = (active_of(p, it)[2 * g] >> lane) & 1, my = (active_of(p, it)[2 * g + 1] >> lane) & 1;
+      if (g != g_cur) {
+        g_cur = g;
+        ax = active_of(p, it)[2 * g];
+        ay = active_of(p, it)[2 * g + 1];
+      }
+      const bool mx = (ax >> lane) & 1, my = (ay >> lane) & 1;
       if (mx || my) bit_one(p, g, int(u % p.N), lane, mx, my);
     }
     if (!(ok = grid_barrier(p.barrier, p.barrier + 1, epoch))) break;

@@ -65,8 +65,11 @@ def test_config2_scale_parity(alg):
 
 
 def test_windowed_equals_generic_kernel():
-    """The windowed LTE kernel and the generic (reference-order) kernel agree bit for
-    bit on the hard decisions, whatever the training length."""
+    """The windowed LTE kernel and the generic kernel (the reference's operation order
+    in FP32) under the parity rules, whatever the training length: the same hard
+    decisions bit for bit in every frame the generic kernel decodes, the same frames
+    failing.  In a failed frame the decisions follow FP32 rounding (the windowed
+    kernel normalises its metrics once per 8 steps), so a few of them may differ."""
     import fecl_b200 as F
     from fecl_b200 import channel as ch
     K, n = 2048, 48
@@ -78,7 +81,9 @@ def test_windowed_equals_generic_kernel():
     code.setKernel("auto")
     for train in (0, 32, 96, 256):
         code.setWindowTraining(train)
-        assert np.array_equal(code.decode(llr), ref), train
+        for segs in (32, 64):
+            code.setWindowSegments(segs)
+            assert_hard_parity(code.decode(llr), ref, msg, K) > n // 4, (train, segs)
 
 
 @pytest.mark.parametrize("K", [40, 1008, 4096, 6144])
