@@ -354,12 +354,21 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
       Chunk ch;
       resolve(j, c, K, fr, X, Y, cur, ch);
       const int n = min(kBlk, a1 - t0);
+      if (n == kBlk) {  // every chunk but the frame's last: no per-step tests
 #pragma unroll
-      for (int i = 0; i < kBlk; ++i) {
-        if (i < n) {
+        for (int i = 0; i < kBlk; ++i) {
           Gam g;
           g.set(ch.la[i], ch.lp[i]);
           fwd_step<ALG>(v, g);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < kBlk; ++i) {
+          if (i < n) {
+            Gam g;
+            g.set(ch.la[i], ch.lp[i]);
+            fwd_step<ALG>(v, g);
+          }
         }
       }
       normalize8(v);
@@ -381,12 +390,21 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
       Chunk ch;
       resolve(j, c, K, fr, X, Y, cur, ch);
       const int hi = min(kBlk, t_train - c * kBlk);
+      if (hi == kBlk) {  // every chunk but the frame's last: no per-step tests
 #pragma unroll
-      for (int i = kBlk - 1; i >= 0; --i) {
-        if (i < hi) {
+        for (int i = kBlk - 1; i >= 0; --i) {
           Gam g;
           g.set(ch.la[i], ch.lp[i]);
           bwd_step<ALG>(v, g);
+        }
+      } else {
+#pragma unroll
+        for (int i = kBlk - 1; i >= 0; --i) {
+          if (i < hi) {
+            Gam g;
+            g.set(ch.la[i], ch.lp[i]);
+            bwd_step<ALG>(v, g);
+          }
         }
       }
       normalize8(v);
@@ -407,6 +425,52 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
   }
 #pragma unroll
   for (int s = 0; s < 8; ++s) vend[s] = v[s];
+}
+
+// Phase B for one 8-step block b of constituent j: reload the forward checkpoint at
+// the block start and the backward one at its end, recompute the block's forward
+// vectors in registers, walk backward emitting sf * extrinsic into out (X: Ls + e at
+// t, Y: e at pi(t)).  FULL: all 8 steps are message steps (no per-step tests).
+template <int ALG, bool FULL>
+__device__ __forceinline__ void ext_block(int j, int b, int K, int T, const Frame& fr, const float* X, const float* Y,
+                                          const uint32_t* perm, float sf, float* out) {
+  const int t0 = b * kBlk;
+  const int n = FULL ? kBlk : min(kBlk, T - t0);
+  RawChunk raw;
+  load_raw(j, b, fr, perm, raw);
+  float al[kBlk][8];
+  load_ck(fr.cka + b * 8, al[0]);
+  float be[8];
+  load_ck(fr.ckb + (b + 1) * 8, be);
+  Chunk in;
+  resolve(j, b, K, fr, X, Y, raw, in);
+#pragma unroll
+  for (int i = 1; i < kBlk; ++i) {
+    if (FULL || i < n) {
+#pragma unroll
+      for (int s = 0; s < 8; ++s) al[i][s] = al[i - 1][s];
+      Gam g;
+      g.set(in.la[i - 1], in.lp[i - 1]);
+      fwd_step<ALG>(al[i], g);
+    }
+  }
+  const float ls[kBlk] = {__uint_as_float(raw.q0.x), __uint_as_float(raw.q0.y), __uint_as_float(raw.q0.z),
+                          __uint_as_float(raw.q0.w), __uint_as_float(raw.q1.x), __uint_as_float(raw.q1.y),
+                          __uint_as_float(raw.q1.z), __uint_as_float(raw.q1.w)};
+  const uint32_t pq[kBlk] = {raw.q0.x, raw.q0.y, raw.q0.z, raw.q0.w, raw.q1.x, raw.q1.y, raw.q1.z, raw.q1.w};
+#pragma unroll
+  for (int i = kBlk - 1; i >= 0; --i) {
+    if (FULL || i < n) {
+      Gam g;
+      g.set(in.la[i], in.lp[i]);
+      const float e = sf * ext_step<ALG>(al[i], be, g);
+      if (FULL || t0 + i < K) {
+        if (j == 0) out[t0 + i] = ls[i] + e;
+        else out[pq[i]] = e;
+      }
+      if (i > 0) bwd_step<ALG>(be, g);
+    }
+  }
 }
 
 // One frame's geometry and buffers, as the decode loop below sees them.
@@ -542,43 +606,11 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
       const float sf = q.sf[j * q.iterations + it];
       float* out = j == 0 ? X : Y;
       for (int b = tid; b < nblk_msg; b += kThreads) {
-        const int t0 = b * kBlk;
-        const int n = min(kBlk, T - t0);
-        RawChunk raw;
-        load_raw(j, b, fr, perm, raw);
-        float al[kBlk][8];
-        load_ck(fr.cka + b * 8, al[0]);
-        float be[8];
-        load_ck(fr.ckb + (b + 1) * 8, be);
-        Chunk in;
-        resolve(j, b, K, fr, X, Y, raw, in);
-#pragma unroll
-        for (int i = 1; i < kBlk; ++i) {
-          if (i < n) {
-#pragma unroll
-            for (int s = 0; s < 8; ++s) al[i][s] = al[i - 1][s];
-            Gam g;
-            g.set(in.la[i - 1], in.lp[i - 1]);
-            fwd_step<ALG>(al[i], g);
-          }
-        }
-        const float ls[kBlk] = {__uint_as_float(raw.q0.x), __uint_as_float(raw.q0.y), __uint_as_float(raw.q0.z),
-                                __uint_as_float(raw.q0.w), __uint_as_float(raw.q1.x), __uint_as_float(raw.q1.y),
-                                __uint_as_float(raw.q1.z), __uint_as_float(raw.q1.w)};
-        const uint32_t pq[kBlk] = {raw.q0.x, raw.q0.y, raw.q0.z, raw.q0.w, raw.q1.x, raw.q1.y, raw.q1.z, raw.q1.w};
-#pragma unroll
-        for (int i = kBlk - 1; i >= 0; --i) {
-          if (i < n) {
-            Gam g;
-            g.set(in.la[i], in.lp[i]);
-            const float e = sf * ext_step<ALG>(al[i], be, g);
-            if (t0 + i < K) {
-              if (j == 0) out[t0 + i] = ls[i] + e;
-              else out[pq[i]] = e;
-            }
-            if (i > 0) bwd_step<ALG>(be, g);
-          }
-        }
+        // in max-log a block of 8 message steps (every block but, when K is not a
+        // multiple of 8, the last) runs without per-step tests (the log-MAP kernels keep
+        // one form, which their registers hold without spilling)
+        if (ALG == kApproximate && b * kBlk + kBlk <= K) ext_block<ALG, true>(j, b, K, T, fr, X, Y, perm, sf, out);
+        else ext_block<ALG, false>(j, b, K, T, fr, X, Y, perm, sf, out);
       }
       __syncthreads();
     }
