@@ -261,7 +261,7 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
     std::map<int, std::vector<fecl::TurboLteBatchFrame>> tframes;
     std::map<int, int> tmax_k;
     for (auto& s : js) {
-      s.lte = s.c->kind == 1 && s.c->lte_fast_ok();
+      s.lte = s.c->kind == 1 && s.c->lte_batch_ok();
       if (!s.lte) continue;
       const int K = int(s.c->msg());
       const int alg = s.c->tdev.algorithm;

@@ -138,7 +138,7 @@ fecl_codec_s* checked(fecl_codec_t c) {
 namespace fecl {
 namespace capi {
 
-ScratchPlan plan_scratch(fecl_codec_s* c, uint64_t n, bool lte_fast) {
+ScratchPlan plan_scratch(fecl_codec_s* c, uint64_t n, bool lte_fast, bool soft) {
   Carver cv;
   ScratchPlan sp;
   const uint64_t P = c->parity(), X = c->state();
@@ -181,7 +181,7 @@ ScratchPlan plan_scratch(fecl_codec_s* c, uint64_t n, bool lte_fast) {
     if (c->ldpc_h2_ok()) b = std::max(b, fecl::ldpc_lanes_h2_scratch_bytes(int64_t(P), int64_t(X), int64_t(n)));
     sp.o1 = cv.take(b);
   } else if (lte_fast) {
-    sp.o1 = cv.take(fecl::turbo_lte_scratch_bytes(int(c->msg()), int64_t(n)));
+    sp.o1 = cv.take(fecl::turbo_lte_scratch_bytes(int(c->msg()), int64_t(n), soft || c->tdev.scheduling == 1));
   } else if (c->kind == 0) {
     sp.o1 = cv.take(n * c->ldev.E * 4);
     sp.o2 = cv.take(n * P * 4);
@@ -351,7 +351,20 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
       cuda_check(cudaMemset(c->stats.ptr, 0, 3 * sizeof(unsigned long long)), "cudaMemset");
     }
     r.stats = c->stats.as<unsigned long long>();
-    r.crc = c->crc_table();
+    r.crc = soft ? nullptr : c->crc_table();
+    r.parallel = c->tdev.scheduling == 1 ? 1 : 0;
+    if (soft) {
+      r.soft = 1;
+      r.hard = nullptr;
+      r.iters = nullptr;
+      r.syst_in = d.syst;
+      r.state_in = d.state;
+      r.msg_out = d.msg;
+      r.syst_out = d.syst_out;
+      r.parity_out = d.parity_out;
+      r.state_out = d.state_out;
+      r.out_dtype = out_dtype;
+    }
     e = fecl::launch_turbo_lte(r, s);
   } else {
     fecl::TurboRun r;
@@ -410,10 +423,10 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
   const size_t isz = dsize(io->in_dtype);
   const size_t osz = soft ? dsize(io->out_dtype) : 4;
   const uint64_t P = c->parity(), S = c->syst(), M = c->msg(), X = c->state();
-  const bool lte_fast = c->kind == 1 && !soft && c->lte_fast_ok();
+  const bool lte_fast = c->kind == 1 && c->lte_fast_ok();
 
   if (!host) {
-    const ScratchPlan sp = plan_scratch(c, n, lte_fast);
+    const ScratchPlan sp = plan_scratch(c, n, lte_fast, soft);
     c->wait_previous(user_stream);
     reserve_workspace(c, sp.bytes);
     Launch d;
@@ -450,7 +463,7 @@ void run_decode(fecl_codec_s* c, const fecl_so_io* io, uint64_t n, uint8_t* hard
   const size_t o_so = io->syst_out ? cv.take(chunk * S * osz) : 0;
   const size_t o_po = io->parity_out ? cv.take(chunk * P * osz) : 0;
   const size_t o_sto = io->state_out ? cv.take(chunk * X * osz) : 0;
-  const ScratchPlan sp = plan_scratch(c, chunk, lte_fast);
+  const ScratchPlan sp = plan_scratch(c, chunk, lte_fast, soft);
   const size_t o_scr = cv.take(sp.bytes);
   const size_t slot_bytes = cv.off;
   if (c->pending) {

@@ -433,12 +433,14 @@ struct fecl_codec_s {
   bool lte_fast_ok() const {
     if (force_generic_() || kind != 1 || !turbo->is_lte_shape()) return false;
     const auto& d = turbo->decoder();
-    if (d.scheduling != 0 || d.precision != 0 || d.iterations == 0) return false;
+    if (d.scheduling > 1 || d.precision != 0 || d.iterations == 0) return false;
     static const fecl::Trellis lte = fecl::lte_trellis();
     for (const auto& c : turbo->constituents())
       if (c.trellis.next_state != lte.next_state || c.trellis.output != lte.output) return false;
     return turbo->msg_size() <= 12288;
   }
+  // The mixed-K batch kernel (batches and the server): serial scheduling only.
+  bool lte_batch_ok() const { return lte_fast_ok() && turbo->decoder().scheduling == 0; }
   // Device resources are created at the first decode, so that host-side operations
   // (encode, check, the transformed matrix) work without a GPU.
   void ensure_device() {
@@ -488,7 +490,7 @@ struct ScratchPlan {
 
 // The kernel and scratch for a batch of n frames of codec c (lte_fast: the windowed
 // LTE turbo kernel applies).
-ScratchPlan plan_scratch(fecl_codec_s* c, uint64_t n, bool lte_fast);
+ScratchPlan plan_scratch(fecl_codec_s* c, uint64_t n, bool lte_fast, bool soft = false);
 // The lane-batched LDPC decoder's parameters for n frames of codec c (pointers in d
 // are device memory); the launcher fills the scratch layout.
 fecl::LdpcLanesParams lanes_params(fecl_codec_s* c, const Launch& d, uint64_t n, int32_t in_dtype, int32_t out_dtype);

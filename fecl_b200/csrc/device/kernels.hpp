@@ -236,13 +236,29 @@ struct TurboLteParams {
   float* scratch = nullptr;  // turbo_lte_scratch_bytes(K, nframes)
   unsigned long long* stats = nullptr;  // [3] passes, fix-up rounds, recomputed segments (nullable)
   const uint32_t* crc = nullptr;        // [K] CRC syndrome table: stop a frame when its CRC checks (nullable)
+  // Parallel scheduling: both constituents take the other's extrinsic values of the
+  // previous iteration (scratch: turbo_lte_scratch_bytes(K, nframes, true)).
+  int32_t parallel = 0;
+  // soDecode (soft != 0): a-priori inputs added to the channel values and initial
+  // extrinsic state (both nullable), soft outputs in FeCl's turbo layouts (nullable),
+  // no scaling of the extrinsic values, no CRC stop and no hard decisions.
+  int32_t soft = 0;
+  const void* syst_in = nullptr;   // [nframes][K + 6]
+  const void* state_in = nullptr;  // [nframes][2 (K + 3)]
+  void* msg_out = nullptr;         // [nframes][K]
+  void* syst_out = nullptr;        // [nframes][K + 6]
+  void* parity_out = nullptr;      // [nframes][3 K + 12]
+  void* state_out = nullptr;       // [nframes][2 (K + 3)]
+  int32_t out_dtype = 1;
   // filled by the launcher
   int32_t Kp = 0, Tp = 0, seg_len = 0;
   int64_t frame_stride = 0;
   float* ck = nullptr;
+  float* ynew = nullptr;  // parallel: [nframes][Kp] the constituent-1 extrinsic values of this iteration
 };
 
-size_t turbo_lte_scratch_bytes(int K, int64_t nframes);
+// Scratch of the windowed decoder; `parallel` adds a buffer per frame.
+size_t turbo_lte_scratch_bytes(int K, int64_t nframes, bool parallel = false);
 cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s);
 
 // The same windowed decoder over a batch of frames of different K (any K <= 12288),

@@ -216,6 +216,66 @@ __device__ __forceinline__ float ext_step(const float a[8], const float b[8], co
   }
 }
 
+// Parity extrinsic value of one step, L(p) - Lp (parityUpdate, MapDecoderImpl.cpp:
+// 376-410), for soDecode's parity output.  Max-log: the branches with p = 1 are
+// (s in 2..5, u = 0) and (s in {0,1,6,7}, u = 1); Lp cancels and La is added once per
+// maximum.
+template <int ALG>
+__device__ __forceinline__ float par_step(const float a[8], const float b[8], const Gam& g) {
+  if constexpr (ALG == kApproximate) {
+    float w0[8], w1[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      w0[s] = a[s] + b[lte_next(s, 0)];
+      w1[s] = a[s] + b[lte_next(s, 1)];
+    }
+    const float la = g.g[2];
+    const float m0p0 = fmaxf(fmaxf(w0[0], w0[1]), fmaxf(w0[6], w0[7]));
+    const float m0p1 = fmaxf(fmaxf(w0[2], w0[3]), fmaxf(w0[4], w0[5]));
+    const float m1p0 = fmaxf(fmaxf(w1[2], w1[3]), fmaxf(w1[4], w1[5]));
+    const float m1p1 = fmaxf(fmaxf(w1[0], w1[1]), fmaxf(w1[6], w1[7]));
+    return fmaxf(m0p1, m1p1 + la) - fmaxf(m0p0, m1p0 + la);
+  } else {
+    float d[16];
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+#pragma unroll
+      for (int u = 0; u < 2; ++u) d[s * 2 + u] = g.plus<ALG>(a[s], s, u) + b[lte_next(s, u)];
+    float l;
+    if (ALG == kExact) {
+      float mx0 = kNegInf, mx1 = kNegInf;
+#pragma unroll
+      for (int s = 0; s < 8; ++s)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          if (lte_out(s, u)) mx1 = fmaxf(d[s * 2 + u], mx1);
+          else mx0 = fmaxf(d[s * 2 + u], mx0);
+        }
+      float m0 = 0.0f, m1 = 0.0f;
+#pragma unroll
+      for (int s = 0; s < 8; ++s)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const float x = d[s * 2 + u];
+          if (lte_out(s, u)) m1 = ((x == mx1) ? 1.0f : expf(x - mx1)) + m1;
+          else m0 = ((x == mx0) ? 1.0f : expf(x - mx0)) + m0;
+        }
+      l = (logf(m1) + mx1) - (logf(m0) + mx0);
+    } else {
+      float m0 = kNegInf, m1 = kNegInf;
+#pragma unroll
+      for (int s = 0; s < 8; ++s)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          if (lte_out(s, u)) m1 = lsum<ALG>(m1, d[s * 2 + u]);
+          else m0 = lsum<ALG>(m0, d[s * 2 + u]);
+        }
+      l = m1 - m0;
+    }
+    return l - g.g[1];
+  }
+}
+
 struct Frame {
   const float* Ls;   // [Tp] systematic L-values, zero past K
   const float* Lp0;  // [Tp]  parity (with tail parity) of constituent 0
@@ -427,13 +487,25 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
   for (int s = 0; s < 8; ++s) vend[s] = v[s];
 }
 
+// Where soDecode's last iteration leaves its values: the constituent's extrinsic values
+// of every trellis step (tail included) in its own order, and its parity extrinsic
+// values (nullable) at element offset par0 of par, of type dtype.
+struct SoftSink {
+  float* ext = nullptr;  // [T]
+  void* par = nullptr;
+  int64_t par0 = 0;
+  int32_t dtype = 1;
+};
+
 // Phase B for one 8-step block b of constituent j: reload the forward checkpoint at
 // the block start and the backward one at its end, recompute the block's forward
 // vectors in registers, walk backward emitting sf * extrinsic into out (X: Ls + e at
-// t, Y: e at pi(t)).  FULL: all 8 steps are message steps (no per-step tests).
-template <int ALG, bool FULL>
+// t, Y: e at pi(t)).  FULL: all 8 steps are message steps (no per-step tests).  SOFT:
+// soDecode's last iteration, which also records every step's extrinsic value (tail
+// steps too) and parity extrinsic value in `sink`.
+template <int ALG, bool FULL, bool SOFT>
 __device__ __forceinline__ void ext_block(int j, int b, int K, int T, const Frame& fr, const float* X, const float* Y,
-                                          const uint32_t* perm, float sf, float* out) {
+                                          const uint32_t* perm, float sf, float* out, const SoftSink& sink) {
   const int t0 = b * kBlk;
   const int n = FULL ? kBlk : min(kBlk, T - t0);
   RawChunk raw;
@@ -468,6 +540,10 @@ __device__ __forceinline__ void ext_block(int j, int b, int K, int T, const Fram
         if (j == 0) out[t0 + i] = ls[i] + e;
         else out[pq[i]] = e;
       }
+      if (SOFT) {
+        sink.ext[t0 + i] = e;
+        if (sink.par) store_llr(sink.par, sink.dtype, sink.par0 + t0 + i, par_step<ALG>(al[i], be, g));
+      }
       if (i > 0) bwd_step<ALG>(be, g);
     }
   }
@@ -484,6 +560,17 @@ struct LteJob {
   int32_t* iters = nullptr;             // nullable
   unsigned long long* stats = nullptr;  // nullable
   const uint32_t* crc = nullptr;        // [K] x^(K-1-i) mod g: stop when the decisions' CRC checks (nullable)
+  // Parallel scheduling: constituent 1 runs first and leaves its extrinsic values in
+  // ynew, copied into Y once constituent 0, which reads the old ones, is done.
+  int32_t parallel = 0;
+  float* ynew = nullptr;  // [Kp]
+  // soDecode (decode_lte_frame<.., SOFT = true>): this frame's inputs and outputs in
+  // FeCl's turbo layouts, as element offsets into the caller's buffers.
+  float* soft_ext = nullptr;  // [2][Tp] scratch: each constituent's last extrinsic values by step
+  const void* state_in = nullptr;
+  int32_t in_dtype = 1, out_dtype = 1;
+  void *msg_out = nullptr, *syst_out = nullptr, *parity_out = nullptr, *state_out = nullptr;
+  int64_t frame = 0;  // frame index within the caller's buffers
 };
 
 // Segment length for a frame of T steps split into `segs` segments: a multiple of
@@ -494,7 +581,8 @@ __host__ __device__ inline int lte_seg_len(int T, int segs) {
 }
 
 // Decodes one frame with the whole CTA; smem holds 2 * Kp floats + Shared<SEGS>.
-template <int ALG, int SEGS>
+// SOFT: soDecode (TurboDecoderImpl::soDecodeBlock, TurboDecoderImpl.cpp:75-150).
+template <int ALG, int SEGS, bool SOFT = false>
 __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
   constexpr int kThreads = 2 * SEGS;
   const int K = q.K, T = q.K + 3;
@@ -524,10 +612,22 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
     sh.term[tid] = tid == 0 ? 0.0f : kNegInf;  // Tail: the trellis starts and ends in state 0
   }
   __syncthreads();
+  if (SOFT && q.state_in) {
+    // the initial extrinsic values: X = Ls + e0, Y[pi(t)] = e1(t) (tail values are
+    // replaced by the channel's tail bits before every pass, as in the reference)
+    const int64_t s0 = q.frame * int64_t(2 * (K + 3));
+    for (int k = tid; k < K; k += kThreads) {
+      X[k] = fr.Ls[k] + load_llr(q.state_in, q.in_dtype, s0 + k);
+      Y[__ldg(q.perm + k)] = load_llr(q.state_in, q.in_dtype, s0 + K + 3 + k);
+    }
+    __syncthreads();
+  }
 
   int ran = q.iterations;
   for (int it = 0; it < q.iterations; ++it) {
-    for (int j = 0; j < 2; ++j) {
+    const bool last_soft = SOFT && it == q.iterations - 1;
+    for (int jj = 0; jj < 2; ++jj) {
+      const int j = q.parallel ? 1 - jj : jj;  // parallel: constituent 1 first, on the old X
       const uint32_t* perm = q.perm;
       // ---- A: segments with training starts
       {
@@ -603,15 +703,34 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
       // run: the tail steps' a-priori values are the channel's tail bits, so their
       // extrinsic values are never read (with K a multiple of 8, as every LTE size
       // is, the last block is all tail).
-      const float sf = q.sf[j * q.iterations + it];
-      float* out = j == 0 ? X : Y;
-      for (int b = tid; b < nblk_msg; b += kThreads) {
-        // in max-log a block of 8 message steps (every block but, when K is not a
-        // multiple of 8, the last) runs without per-step tests (the log-MAP kernels keep
-        // one form, which their registers hold without spilling)
-        if (ALG == kApproximate && b * kBlk + kBlk <= K) ext_block<ALG, true>(j, b, K, T, fr, X, Y, perm, sf, out);
-        else ext_block<ALG, false>(j, b, K, T, fr, X, Y, perm, sf, out);
+      // soDecode does not scale the extrinsic values (TurboDecoderImpl.cpp:75-150)
+      const float sf = SOFT ? 1.0f : q.sf[j * q.iterations + it];
+      float* out = j == 0 ? X : (q.parallel ? q.ynew : Y);
+      if (last_soft) {
+        // soDecode's last iteration: every block, tail blocks too, recording the
+        // extrinsic and parity extrinsic values
+        SoftSink sink;
+        sink.ext = q.soft_ext + j * q.Tp;
+        sink.par = q.parity_out;
+        sink.par0 = q.frame * int64_t(3 * K + 12) + K + 6 + j * (K + 3);
+        sink.dtype = q.out_dtype;
+        for (int b = tid; b < nblk; b += kThreads) ext_block<ALG, false, true>(j, b, K, T, fr, X, Y, perm, sf, out, sink);
+      } else {
+        const SoftSink none;
+        for (int b = tid; b < nblk_msg; b += kThreads) {
+          // in max-log a block of 8 message steps (every block but, when K is not a
+          // multiple of 8, the last) runs without per-step tests (the log-MAP kernels
+          // keep one form, which their registers hold without spilling)
+          if (ALG == kApproximate && b * kBlk + kBlk <= K)
+            ext_block<ALG, true, false>(j, b, K, T, fr, X, Y, perm, sf, out, none);
+          else
+            ext_block<ALG, false, false>(j, b, K, T, fr, X, Y, perm, sf, out, none);
+        }
       }
+      __syncthreads();
+    }
+    if (q.parallel) {
+      for (int k = tid; k < K; k += kThreads) Y[k] = q.ynew[k];
       __syncthreads();
     }
     // CRC stop (an extension; LTE transport blocks end with a CRC-24): the decisions
@@ -635,12 +754,35 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
       }
     }
   }
-  // a-posteriori and hard decision, TurboDecoderImpl.cpp:64-71
-  for (int k = tid; k < K; k += kThreads) q.hard[k] = uint8_t((X[k] + Y[k]) > 0.0f);
-  if (q.iters && tid == 0) *q.iters = ran;
+  if constexpr (SOFT) {
+    // aPosterioriUpdate (TurboDecoderImpl.cpp:152-168) and the soDecode outputs: syst =
+    // (0 + e0) + e1 at natural positions, the tails' extrinsic values after them;
+    // parity = syst | both constituents' parity extrinsic values (written above);
+    // msg = channel (+ a-priori) + syst; state = e0 | e1 in each constituent's order.
+    const float* e0 = q.soft_ext;
+    const float* e1 = q.soft_ext + q.Tp;
+    const int64_t f = q.frame;
+    for (int k = tid; k < K + 6; k += kThreads) {
+      float v;
+      if (k < K) v = e0[k] + Y[k];
+      else v = k < K + 3 ? e0[k] : e1[k - 3];
+      if (q.syst_out) store_llr(q.syst_out, q.out_dtype, f * int64_t(K + 6) + k, v);
+      if (q.parity_out) store_llr(q.parity_out, q.out_dtype, f * int64_t(3 * K + 12) + k, v);
+      if (q.msg_out && k < K) store_llr(q.msg_out, q.out_dtype, f * int64_t(K) + k, fr.Ls[k] + v);
+    }
+    if (q.state_out)
+      for (int t = tid; t < 2 * (K + 3); t += kThreads) {
+        const float v = t < K + 3 ? e0[t] : e1[t - (K + 3)];
+        store_llr(q.state_out, q.out_dtype, f * int64_t(2 * (K + 3)) + t, v);
+      }
+  } else {
+    // a-posteriori and hard decision, TurboDecoderImpl.cpp:64-71
+    for (int k = tid; k < K; k += kThreads) q.hard[k] = uint8_t((X[k] + Y[k]) > 0.0f);
+    if (q.iters && tid == 0) *q.iters = ran;
+  }
 }
 
-template <int ALG, int SEGS>
+template <int ALG, int SEGS, bool SOFT = false>
 __global__ void __launch_bounds__(2 * SEGS, SEGS == 32 ? 4 : 3) turbo_lte_kernel(TurboLteParams p) {
   extern __shared__ float smem[];
   const int64_t f = blockIdx.x;
@@ -660,7 +802,20 @@ __global__ void __launch_bounds__(2 * SEGS, SEGS == 32 ? 4 : 3) turbo_lte_kernel
   q.iters = p.iters ? p.iters + f : nullptr;
   q.stats = p.stats;
   q.crc = p.crc;
-  decode_lte_frame<ALG, SEGS>(q, smem);
+  q.parallel = p.parallel;
+  if (p.ynew) {  // per frame: ynew [Tp] | soft_ext [2][Tp]
+    q.ynew = p.ynew + f * int64_t(3 * p.Tp);
+    q.soft_ext = q.ynew + p.Tp;
+  }
+  q.state_in = p.state_in;
+  q.in_dtype = p.llr_dtype;
+  q.out_dtype = p.out_dtype;
+  q.msg_out = p.msg_out;
+  q.syst_out = p.syst_out;
+  q.parity_out = p.parity_out;
+  q.state_out = p.state_out;
+  q.frame = f;
+  decode_lte_frame<ALG, SEGS, SOFT>(q, smem);
 }
 
 
@@ -680,13 +835,21 @@ __global__ void turbo_lte_stage(TurboLteParams p) {
   for (int64_t f = blockIdx.x; f < p.nframes; f += gridDim.x) {
     const T* in = llr + f * int64_t(3 * K + 12);
     float* out = p.scratch + f * p.frame_stride;
-    for (int i = threadIdx.x; i < Kp; i += blockDim.x) out[i] = i < K ? to_f32(in[i]) : 0.0f;
+    // soDecode's a-priori input is added to the channel's systematic values and tails
+    // (TurboDecoderImpl.cpp:77-82)
+    const T* sys = p.syst_in ? static_cast<const T*>(p.syst_in) + f * int64_t(K + 6) : nullptr;
+    for (int i = threadIdx.x; i < Kp; i += blockDim.x)
+      out[i] = i < K ? (sys ? to_f32(in[i]) + to_f32(sys[i]) : to_f32(in[i])) : 0.0f;
     for (int c = 0; c < 2; ++c) {
       const T* src = in + K + 6 + c * (K + 3);  // parity (with its tail) of constituent c
       float* dst = out + Kp + c * Tp;
       for (int t = threadIdx.x; t < Tp; t += blockDim.x) dst[t] = t < K + 3 ? to_f32(src[t]) : 0.0f;
     }
-    if (threadIdx.x < 8) out[Kp + 2 * Tp + threadIdx.x] = threadIdx.x < 6 ? to_f32(in[K + threadIdx.x]) : 0.0f;
+    if (threadIdx.x < 8) {
+      float v = 0.0f;
+      if (threadIdx.x < 6) v = sys ? to_f32(in[K + threadIdx.x]) + to_f32(sys[K + threadIdx.x]) : to_f32(in[K + threadIdx.x]);
+      out[Kp + 2 * Tp + threadIdx.x] = v;
+    }
   }
 }
 
@@ -780,13 +943,13 @@ cudaError_t turbo_lte_init() {
   });
 }
 
-size_t turbo_lte_scratch_bytes(int K, int64_t nframes) {
+size_t turbo_lte_scratch_bytes(int K, int64_t nframes, bool extra) {
   const int T = K + 3;
   const int nblk = (T + kBlk - 1) / kBlk;
   const int Tp = nblk * kBlk;
   const int Kp = Tp;
   const int64_t stride = Kp + 2 * Tp + 8;
-  return size_t(nframes) * (size_t(stride) + size_t(2 * (nblk + 1) * 8)) * sizeof(float);
+  return size_t(nframes) * (size_t(stride) + size_t(2 * (nblk + 1) * 8) + (extra ? size_t(3 * Tp) : 0)) * sizeof(float);
 }
 
 cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
@@ -799,6 +962,10 @@ cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
   p.Kp = g.Kp;  // the systematic region and the exchange arrays are padded like the parity
   p.frame_stride = g.stride;
   p.ck = p.scratch + p.nframes * p.frame_stride;
+  // parallel scheduling and soDecode: per frame ynew [Tp] | soft_ext [2][Tp] after the
+  // checkpoints (turbo_lte_scratch_bytes(K, n, true))
+  p.ynew = (p.parallel || p.soft) ? p.ck + p.nframes * int64_t(2 * (g.nblk + 1) * 8) : nullptr;
+  if (p.soft) p.crc = nullptr;
   p.seg_len = g.seg_len;
   if (p.train < 0) p.train = 96;
   const unsigned stage_blocks = unsigned(p.nframes < 148 * 8 ? p.nframes : 148 * 8);
@@ -813,6 +980,14 @@ cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
     kern<<<unsigned(p.nframes), threads, smem, s>>>(p);
     return cudaGetLastError();
   };
+  if (p.soft) {
+    const size_t smem = lte_smem_bytes<64>(p.K);
+    switch (p.algorithm) {
+      case kExact: return launch(turbo_lte_kernel<kExact, 64, true>, 128, smem);
+      case kLinear: return launch(turbo_lte_kernel<kLinear, 64, true>, 128, smem);
+      default: return launch(turbo_lte_kernel<kApproximate, 64, true>, 128, smem);
+    }
+  }
   if (segs == 32) {
     const size_t smem = lte_smem_bytes<32>(p.K);
     switch (p.algorithm) {

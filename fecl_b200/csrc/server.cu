@@ -528,7 +528,7 @@ int fecl_server_submit(fecl_server_t server, fecl_codec_t codec, const void* llr
       std::lock_guard<std::mutex> lk(codec->mu);
       codec->ensure_device();
       if (codec->device != server->device) fail(FECL_EINVAL, "the codec lives on another device than the server");
-      r->lte = codec->kind == 1 && codec->lte_fast_ok();
+      r->lte = codec->kind == 1 && codec->lte_batch_ok();
     }
     r->c = codec;
     r->llr = llr;
