@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <utility>
 
 namespace fecl {
 
@@ -57,6 +58,32 @@ inline cudaError_t once_per_device(std::atomic<unsigned long long>& done, F&& up
   e = upload();
   if (e == cudaSuccess) done.fetch_or(bit);
   return e;
+}
+
+// Programmatic dependent launch.  A kernel launched with launch_pdl may be scheduled
+// while the previous kernel of its stream is still running; pdl_enter, its first
+// statement, waits until that kernel has completed and its writes are visible (a
+// no-op for a kernel launched without the attribute), then lets the next kernel of the
+// stream start launching.  Consecutive passes of a decoder thus overlap their launch
+// latency with the previous pass's tail, and compute exactly what sequential
+// launches compute.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
 __device__ __forceinline__ float lut_log1pexpm(const LinearLut& t, float x) {

@@ -152,6 +152,7 @@ __device__ __forceinline__ uint32_t check_rows(const LdpcLanesParams& p, int g, 
 // row pair).
 template <int ALG, int MSG, int DMAX>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_check(LdpcLanesParams p, int it, int g0) {
+  pdl_enter();
   constexpr int kRows = DMAX <= 8 ? 2 : 1;
   const int lane = lane_id();
   const int warps = int(gridDim.x) * kWarpsPerBlock;
@@ -212,6 +213,7 @@ __device__ __forceinline__ void bit_one(const LdpcLanesParams& p, int g, int b, 
 // writes the group's masks for iteration it + 1.
 template <int MSG>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_bit(LdpcLanesParams p, int it, int g0) {
+  pdl_enter();
   const int lane = lane_id();
   const int warps = int(gridDim.x) * kWarpsPerBlock;
   const int g = g0 + int(blockIdx.y);
@@ -472,11 +474,12 @@ cudaError_t run(const LdpcLanesParams& p, cudaStream_t s) {
     const int nw = p.groups - w0 < wave ? p.groups - w0 : wave;
     const dim3 gbit = grid_for(p.N, nw);
     const dim3 gchk = grid_for((p.M + (DMAX <= 8 ? 1 : 0)) / (DMAX <= 8 ? 2 : 1), nw);
-    lanes_bit<MSG><<<gbit, kWarpsPerBlock * 32, 0, s>>>(p, -1, w0);
-    for (int it = 0; it < p.iterations; ++it) {
-      lanes_check<ALG, MSG, DMAX><<<gchk, kWarpsPerBlock * 32, 0, s>>>(p, it, w0);
-      lanes_bit<MSG><<<gbit, kWarpsPerBlock * 32, 0, s>>>(p, it, w0);
+    cudaError_t e = launch_pdl(lanes_bit<MSG>, gbit, dim3(kWarpsPerBlock * 32), s, p, -1, w0);
+    for (int it = 0; e == cudaSuccess && it < p.iterations; ++it) {
+      e = launch_pdl(lanes_check<ALG, MSG, DMAX>, gchk, dim3(kWarpsPerBlock * 32), s, p, it, w0);
+      if (e == cudaSuccess) e = launch_pdl(lanes_bit<MSG>, gbit, dim3(kWarpsPerBlock * 32), s, p, it, w0);
     }
+    if (e != cudaSuccess) return e;
   }
   lanes_finish<MSG><<<gs, 256, 0, s>>>(p);
   return cudaGetLastError();

@@ -171,6 +171,7 @@ __device__ __forceinline__ void check_rows(const LdpcLanesParams& p, int it, int
 
 template <int DMAX>
 __global__ void __launch_bounds__(kWarps * 32) h2_check(LdpcLanesParams p, int it, int g0) {
+  pdl_enter();
   constexpr int kRows = DMAX <= 8 ? 2 : 1;
   const int lane = threadIdx.x & 31;
   const int warps = int(gridDim.x) * kWarps;
@@ -240,6 +241,7 @@ __device__ __forceinline__ void bit_one(const LdpcLanesParams& p, int g, int b, 
 // Bit pass; with it < 0 the initial APP for every lane.  Block (0, y) retires frames
 // and writes the group's masks for iteration it + 1.
 __global__ void __launch_bounds__(kWarps * 32) h2_bit(LdpcLanesParams p, int it, int g0) {
+  pdl_enter();
   const int lane = threadIdx.x & 31;
   const int warps = int(gridDim.x) * kWarps;
   const int g = g0 + int(blockIdx.y);
@@ -563,11 +565,12 @@ cudaError_t run(const LdpcLanesParams& p, cudaStream_t s) {
     const int nw = p.groups - w0 < wave ? p.groups - w0 : int(wave);
     const dim3 gbit = grid_for(p.N, nw);
     const dim3 gchk = grid_for((p.M + (DMAX <= 8 ? 1 : 0)) / (DMAX <= 8 ? 2 : 1), nw);
-    h2_bit<<<gbit, kWarps * 32, 0, s>>>(p, -1, w0);
-    for (int it = 0; it < p.iterations; ++it) {
-      h2_check<DMAX><<<gchk, kWarps * 32, 0, s>>>(p, it, w0);
-      h2_bit<<<gbit, kWarps * 32, 0, s>>>(p, it, w0);
+    cudaError_t e = launch_pdl(h2_bit, gbit, dim3(kWarps * 32), s, p, -1, w0);
+    for (int it = 0; e == cudaSuccess && it < p.iterations; ++it) {
+      e = launch_pdl(h2_check<DMAX>, gchk, dim3(kWarps * 32), s, p, it, w0);
+      if (e == cudaSuccess) e = launch_pdl(h2_bit, gbit, dim3(kWarps * 32), s, p, it, w0);
     }
+    if (e != cudaSuccess) return e;
   }
   h2_finish<<<gs, 256, 0, s>>>(p);
   return cudaGetLastError();

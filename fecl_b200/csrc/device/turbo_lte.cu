@@ -52,11 +52,18 @@ namespace {
 constexpr int kExact = 0, kLinear = 1, kApproximate = 2;
 constexpr int kBlk = 8;  // checkpoint spacing / APP block length
 constexpr float kNegInf = -INFINITY;
-// Boundary acceptance: |x - y| <= kAbsTol + kRelTol * max(|x|, |y|).  Two walks that
-// have forgotten their starts differ by the rounding of the steps since, which grows
-// with the metrics' magnitude (strong a-priori values late in a decode).
-constexpr float kAbsTol = 1e-3f;
-constexpr float kRelTol = 1e-5f;
+// Boundary acceptance: |x - y| <= abs + rel * max(|x|, |y|).  Two walks that have
+// forgotten their starts differ by the rounding of the steps since, which grows with
+// the metrics' magnitude (strong a-priori values late in a decode).  An accepted
+// difference reaches the extrinsic values at most doubled, so soDecode, whose soft
+// outputs must stay within 1e-4 relative of the reference, accepts only differences
+// two orders of magnitude below that; decode, which outputs hard decisions, accepts
+// 1e-3 (+ 1e-5 relative), which saves fix-up walks.
+struct Tol {
+  float abs, rel;
+};
+constexpr Tol kDecodeTol = {1e-3f, 1e-5f};
+constexpr Tol kSoftTol = {1e-6f, 1e-6f};
 constexpr int kDefaultSegs = 64;
 
 __constant__ LinearLut c_lut;
@@ -360,11 +367,11 @@ __device__ __forceinline__ void load_ck(const float* ck, float v[8]) {
   v[4] = c1.x; v[5] = c1.y; v[6] = c1.z; v[7] = c1.w;
 }
 
-__device__ __forceinline__ bool close8(const float* x, const float* y) {
+__device__ __forceinline__ bool close8(const float* x, const float* y, Tol t) {
   bool ok = true;
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
-    const float tol = kAbsTol + kRelTol * fmaxf(fabsf(x[s]), fabsf(y[s]));
+    const float tol = t.abs + t.rel * fmaxf(fabsf(x[s]), fabsf(y[s]));
     ok = ok && ((x[s] == y[s]) || fabsf(x[s] - y[s]) <= tol);
   }
   return ok;
@@ -386,7 +393,7 @@ __device__ __forceinline__ bool close8(const float* x, const float* y) {
 template <int ALG>
 __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, int a1, const float* vin, float* vstart,
                                           float* vend, int K, int T, Frame fr, const float* X, const float* Y,
-                                          const uint32_t* perm, bool refine) {
+                                          const uint32_t* perm, bool refine, Tol tol) {
   float v[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) v[s] = vin[s];
@@ -407,7 +414,7 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
         if (refine && t0 > a0) {
           float old[8];
           load_ck(fr.cka + c * 8, old);
-          if (close8(v, old)) return;
+          if (close8(v, old, tol)) return;
         }
         store_ck(fr.cka + c * 8, v);
       }
@@ -477,7 +484,7 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
         if (refine) {
           float old[8];
           load_ck(fr.ckb + c * 8, old);
-          if (close8(v, old)) return;
+          if (close8(v, old, tol)) return;
         }
         store_ck(fr.ckb + c * 8, v);
       }
@@ -602,9 +609,11 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
   const int tid = threadIdx.x;
   const int L = q.seg_len;
   const int S = (T + L - 1) / L;
+  const Tol tol = SOFT ? kSoftTol : kDecodeTol;
 
+  // X = Ls + e0 with e0 = 0 (constituent 1 reads it first under Parallel scheduling)
   for (int k = tid; k < q.Kp; k += kThreads) {
-    X[k] = 0.0f;
+    X[k] = fr.Ls[k];
     Y[k] = 0.0f;
   }
   if (tid < 8) {
@@ -647,7 +656,7 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
             vin = exact ? sh.term : sh.flat;
           }
           segment_walk<ALG>(fwd, j, t_train, a0, a1, vin, sh.sv[fwd ? 0 : 1][w], sh.ev[fwd ? 0 : 1][w], K, T, fr, X,
-                            Y, perm, false);
+                            Y, perm, false, tol);
         }
       }
       __syncthreads();
@@ -661,8 +670,8 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
           const int w = fwd ? tid : tid - SEGS;
           int bad = 0;
           if (w < S) {
-            if (fwd && w > 0) bad = !close8(sh.sv[0][w], sh.ev[0][w - 1]);
-            if (!fwd && w < S - 1) bad = !close8(sh.sv[1][w], sh.ev[1][w + 1]);
+            if (fwd && w > 0) bad = !close8(sh.sv[0][w], sh.ev[0][w - 1], tol);
+            if (!fwd && w < S - 1) bad = !close8(sh.sv[1][w], sh.ev[1][w + 1], tol);
           }
           if (w < S) sh.bad[fwd ? 0 : 1][w] = bad;
           if (bad) sh.any_bad = 1;
@@ -690,7 +699,8 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
 #pragma unroll
             for (int s = 0; s < 8; ++s) sv[s] = start[s];
             const int a0 = w * L, a1 = min(T, a0 + L);
-            segment_walk<ALG>(fwd, j, fwd ? a0 : a1, a0, a1, sv, sv, sh.ev[fwd ? 0 : 1][w], K, T, fr, X, Y, perm, true);
+            segment_walk<ALG>(fwd, j, fwd ? a0 : a1, a0, a1, sv, sv, sh.ev[fwd ? 0 : 1][w], K, T, fr, X, Y, perm, true,
+                              tol);
           }
         }
         __syncthreads();
