@@ -353,7 +353,7 @@ struct fecl_codec_s {
   std::map<uint32_t, std::unique_ptr<ClusterDev>> cplans;
   int cluster_size_sel = 0, cluster_threads_sel = 0;  // 0: chosen by the heuristic
   int lanes_wave = 0;                                 // 0: chosen by the launcher
-  int lanes_persist = 0;                              // persistent launch: 0 where it pays, 1 where it applies, -1 never
+  int lanes_persist = 0;                              // persistent launch: 1 where it applies, 0 / -1 never
   int smem_optin = 0, sm_count = 0;
 
   ClusterDev& cluster_plan(uint32_t C) {

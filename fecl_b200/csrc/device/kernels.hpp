@@ -60,7 +60,7 @@ struct LdpcLanesParams {
   int32_t algorithm = 2, iterations = 1, fixed_iterations = 0;
   int32_t msg_type = 0;  // 0 FP32, 1 FP16, 2 saturated int8 (Q5.2)
   int32_t wave_groups = 0;  // groups decoded together (0: as many as fit in 64 MiB of L2)
-  int32_t persist = 0;      // one persistent launch for small batches: 0 where it pays, 1 wherever it applies, -1 never
+  int32_t persist = 0;      // one persistent launch for small batches: 1 wherever it applies, 0 / -1 never
   // batch, frame-major caller buffers
   int64_t nframes = 0;
   const void* llr = nullptr;

@@ -510,13 +510,12 @@ dim3 grid_for(int64_t per_group, int groups) {
 // than two).
 constexpr int64_t kWaveCap = 96ll << 20;
 
-// One persistent launch for batches of at most kPersistAuto groups (or, with
-// persist == 1, kPersistGroups), all in one wave, on a stream that is not capturing.
-constexpr int kPersistAuto = 4;
+// One persistent launch when asked for (persist == 1) for batches of at most
+// kPersistGroups groups, all in one wave, on a stream that is not capturing (the
+// per-pass launches are the built-in choice: see ldpc_lanes.cu).
 
 bool use_persistent(const LdpcLanesParams& p, int64_t wave, cudaStream_t s) {
-  if (p.persist < 0 || p.groups > kPersistGroups || wave < p.groups) return false;
-  if (p.persist == 0 && p.groups > kPersistAuto) return false;
+  if (p.persist <= 0 || p.groups > kPersistGroups || wave < p.groups) return false;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
     cudaGetLastError();

@@ -317,8 +317,9 @@ int fecl_ldpc_set_wave(fecl_codec_t codec, int32_t groups);
 
 /* Lane-batched LDPC decoder: run a small batch (at most 16 frame groups, one wave)
  * as one persistent launch whose check and bit passes are separated by grid-wide
- * barriers, instead of two launches per iteration.  mode 0: only for batches of at
- * most 4 groups (where launches dominate); 1: wherever it applies; -1: never.  The
+ * barriers, instead of two launches per iteration.  mode 1: wherever it applies;
+ * 0 (the built-in choice) and -1: never -- the per-pass launches, which overlap their
+ * launch latency through programmatic dependent launch, measured faster.  The
  * results are those of the two-launch form bit for bit.  A barrier wait is bounded
  * (2 s); a decode whose barrier gave up reports -1 iterations for its frames.
  * Extension: no counterpart in the reference. */

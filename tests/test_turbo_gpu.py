@@ -241,29 +241,37 @@ def test_custom_scheduling_matches_reference(stages, alg):
 
 @pytest.mark.parametrize("sched", [0, 1])
 @pytest.mark.parametrize("alg", [2, 1, 0])
-def test_windowed_soDecode_and_parallel_equal_generic(alg, sched):
+def test_windowed_soDecode_and_parallel_match_reference(alg, sched, has_ref):
     """LTE soDecode (with a-priori and state inputs, every soft output) and Parallel
-    scheduling on the windowed kernel against the generic kernel (the reference's
-    operation order in FP32), under the parity rules: hard decisions equal in every
-    decoded frame, soft outputs within 1e-4 relative there."""
+    scheduling on the windowed kernel against the compiled FP64 reference on the same
+    L-values, under the parity rules: hard decisions equal in every frame the
+    reference decodes, soft outputs within 1e-4 relative there."""
+    if not has_ref:
+        pytest.skip("the compiled reference (oracle/_ref) is not built")
     import fecl_b200 as F
     from fecl_b200 import channel as ch
+    from oracle import ref
     K, n = 1024, 24
     code = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(alg).iterations(5).scheduling(sched))
+    code.setKernel("auto")
     msg = ch.random_bits(n * K, 70 + alg)
     llr = ch.awgn_llr(code.encode(msg), 0.9, K / code.paritySize(), 70 + alg, np.float32)
     syst = (0.05 * ch.awgn_llr(ch.random_bits(n * code.systSize(), 9), 0.0, 1.0, 9)).astype(np.float32)
-    outs = {}
-    for kernel in ("generic", "auto"):
-        code.setKernel(kernel)
-        first = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output(np.float32).state())
-        so = code.soDecode(F.Codec.Input().parity(llr).syst(syst).state(first.state()),
-                           F.Codec.Output(np.float32).msg().syst().parity().state())
-        outs[kernel] = (code.decode(llr), first.state(), so.msg(), so.syst(), so.parity(), so.state())
-    g, w = outs["generic"], outs["auto"]
-    assert_hard_parity(w[0], g[0], msg, K)
-    ok = frame_ok(g[2] > 0, msg, K)
+    rc = ref.RefCodec.turbo([([4], [[0o15]], [0o13])], [np.arange(K), F.Turbo.Lte3Gpp.interleaver(K)], 0, alg, sched, 5,
+                            workgroup=8)
+    r_first = rc.so_decode(llr, outputs=("state",))
+    r_so = rc.so_decode(llr, syst=syst, state=r_first["state"].astype(np.float32),
+                        outputs=("msg", "syst", "parity", "state"))
+    r_bits, r_app = rc.decode(llr), rc.so_decode(llr, outputs=("msg",))["msg"]
+    bits = code.decode(llr)
+    assert_hard_parity(bits, r_bits, msg, K, ref_app=r_app)
+    first = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output(np.float32).state())
+    so = code.soDecode(F.Codec.Input().parity(llr).syst(syst).state(r_first["state"].astype(np.float32)),
+                       F.Codec.Output(np.float32).msg().syst().parity().state())
+    ok = frame_ok(r_app > 0, msg, K)
     assert ok.sum() >= n // 3
-    sizes = (code.stateSize(), K, code.systSize(), code.paritySize(), code.stateSize())
-    for name, a, b, size in zip(("state", "msg", "syst", "parity", "state2"), w[1:], g[1:], sizes):
+    for name, a, b, size in (("state", first.state(), r_first["state"], code.stateSize()),
+                             ("msg", so.msg(), r_so["msg"], K), ("syst", so.syst(), r_so["syst"], code.systSize()),
+                             ("parity", so.parity(), r_so["parity"], code.paritySize()),
+                             ("state2", so.state(), r_so["state"], code.stateSize())):
         assert_soft_parity(a, b, ok, size, what=name, exact=(alg == 0))
