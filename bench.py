@@ -817,7 +817,8 @@ def run_serving(args, embedded=False):
     rows = []
     rng = np.random.default_rng(SEED + 11)
     peak = None
-    for rate in SERVING_RATES:
+    rates = [int(r) for r in args.serve_rates.split(",")] if args.serve_rates else SERVING_RATES
+    for rate in rates:
         n = max(200, int(rate * args.serve_seconds))
         arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
         order = rng.integers(0, len(pool), size=n)
@@ -869,13 +870,13 @@ def run_serving(args, embedded=False):
                "what": "the whole pool as one batch (one CUDA graph), FP32 LDPC messages, device-resident L-values"}
     del mb
     line = {
-        "metric": METRIC, "value": peak["sustained_info_mbps"], "unit": "Mbit/s", "n_gpus": 1, "steps": len(SERVING_RATES),
+        "metric": METRIC, "value": peak["sustained_info_mbps"], "unit": "Mbit/s", "n_gpus": 1, "steps": len(rates),
         "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f16", "data": "synthetic",
         "config": {"workload": "decode server, Poisson arrivals of single-frame requests at %s frames/s: 50%% LTE turbo "
                                "(K uniform over the 188 QPP sizes), 40%% DVB-S2 short, 10%% DVB-S2 normal LDPC (rates "
                                "1/2..5/6), Eb/N0 U(0.5, 3.0) dB, FP16 L-values and LDPC messages, 40 GiB budget"
-                               % SERVING_RATES,
+                               % rates,
                    "pool_frames": len(pool), "slots": args.serve_slots, "max_batch_frames": args.serve_batch,
                    "seconds_per_rate": args.serve_seconds},
         "serving": rows,
@@ -1047,6 +1048,7 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=0.25, help="serving: seconds of arrivals per rate")
     ap.add_argument("--serve-slots", type=int, default=3, help="serving: batches in flight")
     ap.add_argument("--serve-batch", type=int, default=2048, help="serving: frames per batch at most")
+    ap.add_argument("--serve-rates", default="", help="serving: comma-separated offered rates (default: all)")
     ap.add_argument("--no-extras", action="store_true",
                     help="lte-turbo: skip the LDPC and serving figures added to the default line")
     ap.add_argument("--profile-decodes", type=int, default=0,

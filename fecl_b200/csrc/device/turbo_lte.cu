@@ -302,8 +302,6 @@ struct Shared {
   float in[2][SEGS][8];  // warm training starts: the previous pass's checkpoints
   float flat[8];         // training start: all states equal
   float term[8];         // trellis termination: state 0
-  int bad[2][SEGS];
-  int any_bad;
   uint32_t crc_part[2 * SEGS / 32];  // per-warp CRC syndromes
 };
 
@@ -683,48 +681,38 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
         }
       }
       __syncthreads();
-      // ---- A2: verify boundaries; walk again the segments whose start disagrees
+      // ---- A2: verify boundaries; walk again the segments whose start disagrees.
+      // One barrier both publishes and combines the checks; a round with a rejected
+      // boundary adds two more.
       int rounds = 0;
       for (int round = 0; round < S; ++round) {
-        if (tid == 0) sh.any_bad = 0;
-        __syncthreads();
-        {
-          const bool fwd = tid < SEGS;
-          const int w = fwd ? tid : tid - SEGS;
-          int bad = 0;
-          if (w < S) {
-            if (fwd && w > 0) bad = !close8(sh.sv[0][w], sh.ev[0][w - 1], tol);
-            if (!fwd && w < S - 1) bad = !close8(sh.sv[1][w], sh.ev[1][w + 1], tol);
-          }
-          if (w < S) sh.bad[fwd ? 0 : 1][w] = bad;
-          if (bad) sh.any_bad = 1;
+        const bool fwd = tid < SEGS;
+        const int w = fwd ? tid : tid - SEGS;
+        bool bad = false;
+        if (w < S) {
+          if (fwd && w > 0) bad = !close8(sh.sv[0][w], sh.ev[0][w - 1], tol);
+          if (!fwd && w < S - 1) bad = !close8(sh.sv[1][w], sh.ev[1][w + 1], tol);
+        }
+        if (!__syncthreads_or(bad)) break;
+        ++rounds;
+        // Walk every rejected segment again from its neighbour's end.  The end is
+        // copied to registers before the barrier and becomes the segment's start
+        // after it, so a neighbour that is itself being walked again is read in its
+        // old state; the next round checks the boundary again.
+        float start[8];
+        if (bad) {
+#pragma unroll
+          for (int s = 0; s < 8; ++s) start[s] = fwd ? sh.ev[0][w - 1][s] : sh.ev[1][w + 1][s];
         }
         __syncthreads();
-        if (!sh.any_bad) break;
-        ++rounds;
-        {
-          // Walk every rejected segment again from its neighbour's end.  The end is
-          // copied to registers before the barrier and becomes the segment's start
-          // after it, so a neighbour that is itself being walked again is read in its
-          // old state; the next round checks the boundary again.
-          const bool fwd = tid < SEGS;
-          const int w = fwd ? tid : tid - SEGS;
-          const bool mine = w < S && sh.bad[fwd ? 0 : 1][w];
-          float start[8];
-          if (mine) {
+        if (bad) {
+          if (q.stats) atomicAdd(q.stats + 2, 1ull);
+          float* sv = sh.sv[fwd ? 0 : 1][w];
 #pragma unroll
-            for (int s = 0; s < 8; ++s) start[s] = fwd ? sh.ev[0][w - 1][s] : sh.ev[1][w + 1][s];
-          }
-          __syncthreads();
-          if (mine) {
-            if (q.stats) atomicAdd(q.stats + 2, 1ull);
-            float* sv = sh.sv[fwd ? 0 : 1][w];
-#pragma unroll
-            for (int s = 0; s < 8; ++s) sv[s] = start[s];
-            const int a0 = w * L, a1 = min(T, a0 + L);
-            segment_walk<ALG>(fwd, j, fwd ? a0 : a1, a0, a1, sv, sv, sh.ev[fwd ? 0 : 1][w], K, T, fr, X, Y, perm, true,
-                              tol);
-          }
+          for (int s = 0; s < 8; ++s) sv[s] = start[s];
+          const int a0 = w * L, a1 = min(T, a0 + L);
+          segment_walk<ALG>(fwd, j, fwd ? a0 : a1, a0, a1, sv, sv, sh.ev[fwd ? 0 : 1][w], K, T, fr, X, Y, perm, true,
+                            tol);
         }
         __syncthreads();
       }
