@@ -575,7 +575,7 @@ def mixed_inputs(reqs, codes, seed):
     return out
 
 
-def build_mixed_batch(inputs, codes, autotune=True, shared_ldpc=True):
+def build_mixed_batch(inputs, codes, autotune=True, shared_ldpc=False):
     """One F.Batch over mixed requests: one job per code, its frames' L-values
     contiguous in one device buffer, decisions and iteration counts likewise."""
     import numpy as np
@@ -634,7 +634,7 @@ def run_mixed(args):
     reqs = mixed_requests(total, SEED + rank)
     codes = MixedCodes(prec)
     inputs = mixed_inputs(reqs, codes, SEED + rank)
-    mb = build_mixed_batch(inputs, codes, autotune=not args.no_autotune, shared_ldpc=not args.per_job_ldpc)
+    mb = build_mixed_batch(inputs, codes, autotune=not args.no_autotune, shared_ldpc=args.shared_ldpc)
     by_key, keys, llr_host, msg_ref = mb["by_key"], mb["keys"], mb["llr_host"], mb["msg_ref"]
     d_llr, d_msg, d_its, n_bits_out = mb["d_llr"], mb["d_msg"], mb["d_its"], mb["n_bits_out"]
     batch, build_s = mb["batch"], mb["build_s"]
@@ -756,7 +756,7 @@ def run_mixed(args):
                                "normalised min-sum 0.75, <=50 iterations), Eb/N0 U(0.5, 3.0) dB per frame, FP16 L-values, "
                                "one CUDA graph" % total,
                    "ldpc_message_storage": {0: "f32", 1: "f16", 2: "i8"}[prec], "codes": len(keys),
-                   "autotune": not args.no_autotune, "shared_ldpc_launch": not args.per_job_ldpc,
+                   "autotune": not args.no_autotune, "shared_ldpc_launch": args.shared_ldpc,
                    "build_s": round(build_s, 3),
                    "fer": {k: (v[0] / v[1] if v[1] else None) for k, v in fam.items()},
                    "l2": "flushed between timed steps (256 MiB write)",
@@ -1042,8 +1042,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="mixed: build the batch without autotuning")
     ap.add_argument("--no-plain", action="store_true", help="mixed: skip the per-request FP32 comparison")
-    ap.add_argument("--per-job-ldpc", action="store_true",
-                    help="mixed: every LDPC job its own launches instead of the shared persistent launch")
+    ap.add_argument("--shared-ldpc", action="store_true",
+                    help="mixed: the FP16 LDPC jobs share one persistent launch per check-degree class")
     ap.add_argument("--plain-sample", type=int, default=256, help="mixed: requests decoded one by one for the comparison")
     ap.add_argument("--serve-seconds", type=float, default=0.25, help="serving: seconds of arrivals per rate")
     ap.add_argument("--serve-slots", type=int, default=3, help="serving: batches in flight")

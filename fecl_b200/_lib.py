@@ -90,7 +90,7 @@ class fecl_batch_job(C.Structure):
 
 
 BATCH_AUTOTUNE = 1
-BATCH_PER_JOB = 2
+BATCH_SHARED_LDPC = 2
 
 
 class fecl_server_options(C.Structure):

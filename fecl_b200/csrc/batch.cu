@@ -224,7 +224,7 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
     if (!out) fail(FECL_EINVAL, "null output");
     *out = nullptr;
     if (!jobs || njobs == 0) fail(FECL_EINVAL, "empty batch");
-    if (flags & ~(FECL_BATCH_AUTOTUNE | FECL_BATCH_PER_JOB)) fail(FECL_EINVAL, "Invalid batch flags");
+    if (flags & ~(FECL_BATCH_AUTOTUNE | FECL_BATCH_SHARED_LDPC)) fail(FECL_EINVAL, "Invalid batch flags");
     std::vector<JobState> js(njobs);
     std::set<fecl_codec_s*> codecs;
     for (uint32_t i = 0; i < njobs; ++i) {
@@ -286,7 +286,7 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
     std::ostringstream plan;
     for (auto& s : js) {
       if (s.lte) continue;
-      if (!(flags & FECL_BATCH_PER_JOB) && SharedLdpc::eligible(s.c)) {
+      if ((flags & FECL_BATCH_SHARED_LDPC) && SharedLdpc::eligible(s.c)) {
         s.multi = true;
         continue;
       }

@@ -377,10 +377,9 @@ int fecl_lte_turbo_decode_noalloc(uint32_t K, int32_t algorithm, uint32_t iterat
  * A batch decodes the frames of several codecs -- LDPC codes of any size and rate,
  * LTE turbo codes of any K, any other turbo code -- with one CUDA graph launch.
  * Every LTE turbo frame goes into one persistent launch over all K (longest
- * frames first); the LDPC jobs that take the packed FP16 decoder run in one
- * persistent launch per check-degree class (every code's frame groups, wave by
- * wave, grid barriers between the passes); every other job gets the decoder
- * fecl_decode would pick for it,
+ * frames first); every other job gets the decoder fecl_decode would pick for it
+ * (with FECL_BATCH_SHARED_LDPC the packed FP16 LDPC jobs instead share one persistent
+ * launch per check-degree class),
  * or, with FECL_BATCH_AUTOTUNE, the fastest of the LDPC kernel shapes that compute
  * the same bits, timed on the job's own data at creation and remembered for the
  * process.  Results equal those of fecl_decode on each job alone, bit for bit.
@@ -400,10 +399,10 @@ typedef struct {
   int32_t* iterations; /* [nframes] or NULL */
 } fecl_batch_job;
 #define FECL_BATCH_AUTOTUNE 1
-/* Every LDPC job runs its own launches.  By default the jobs that take the packed
- * FP16 decoder share one persistent launch per check-degree class, wave by wave
- * (the same bits either way). */
-#define FECL_BATCH_PER_JOB 2
+/* The LDPC jobs that take the packed FP16 decoder share one persistent launch per
+ * check-degree class, wave by wave, grid barriers between the passes (the same bits
+ * as their own launches, which are the default: they measured faster). */
+#define FECL_BATCH_SHARED_LDPC 2
 int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags, fecl_batch_t* out);
 /* Launches the batch's graph on `stream` (asynchronous). */
 int fecl_batch_run(fecl_batch_t batch, void* stream);
