@@ -575,7 +575,7 @@ def mixed_inputs(reqs, codes, seed):
     return out
 
 
-def build_mixed_batch(inputs, codes, autotune=True, shared_ldpc=False):
+def build_mixed_batch(inputs, codes, autotune=True, shared_ldpc=None):
     """One F.Batch over mixed requests: one job per code, its frames' L-values
     contiguous in one device buffer, decisions and iteration counts likewise."""
     import numpy as np
@@ -1042,8 +1042,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="mixed: build the batch without autotuning")
     ap.add_argument("--no-plain", action="store_true", help="mixed: skip the per-request FP32 comparison")
-    ap.add_argument("--shared-ldpc", action="store_true",
-                    help="mixed: the FP16 LDPC jobs share one persistent launch per check-degree class")
+    ap.add_argument("--shared-ldpc", default=None, choices=["passes", "persistent"],
+                    help="mixed: the FP16 LDPC jobs share their launches (per pass, or one persistent launch per class)")
     ap.add_argument("--plain-sample", type=int, default=256, help="mixed: requests decoded one by one for the comparison")
     ap.add_argument("--serve-seconds", type=float, default=0.25, help="serving: seconds of arrivals per rate")
     ap.add_argument("--serve-slots", type=int, default=3, help="serving: batches in flight")

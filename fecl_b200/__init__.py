@@ -987,11 +987,11 @@ class Batch:
     uint8, iterations [nframes] int32.  The tensors stay bound to the batch: write new
     L-values into them and call run() again.  Results equal each codec's decode()
     bit for bit.  autotune=True times the equivalent LDPC kernel shapes on these
-    inputs at creation and keeps the fastest.  shared_ldpc=True runs the FP16 LDPC
-    jobs in one shared persistent launch per check-degree class instead of their own
-    launches (same results)."""
+    inputs at creation and keeps the fastest.  shared_ldpc="passes" runs the FP16
+    LDPC jobs with shared launches per pass, "persistent" with one shared persistent
+    launch per check-degree class, instead of their own launches (same results)."""
 
-    def __init__(self, jobs, autotune=False, shared_ldpc=False):
+    def __init__(self, jobs, autotune=False, shared_ldpc=None):
         self._keep = []
         arr = (_lib.fecl_batch_job * len(jobs))()
         for i, job in enumerate(jobs):
@@ -1012,7 +1012,13 @@ class Batch:
             arr[i].iterations = it.data_ptr() if it is not None else None
             self._keep.append((codec, llr, msg, it))
         h = C.c_void_p()
-        flags = (_lib.BATCH_AUTOTUNE if autotune else 0) | (_lib.BATCH_SHARED_LDPC if shared_ldpc else 0)
+        flags = _lib.BATCH_AUTOTUNE if autotune else 0
+        if shared_ldpc == "passes":
+            flags |= _lib.BATCH_SHARED_LDPC
+        elif shared_ldpc == "persistent":
+            flags |= _lib.BATCH_SHARED_PERSISTENT
+        elif shared_ldpc not in (None, False):
+            raise ValueError("shared_ldpc must be None, 'passes' or 'persistent'")
         _check(_L.fecl_batch_create(arr, len(jobs), flags, C.byref(h)))
         self._h = h
         self._device = jobs[0][1].device

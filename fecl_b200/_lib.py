@@ -91,6 +91,7 @@ class fecl_batch_job(C.Structure):
 
 BATCH_AUTOTUNE = 1
 BATCH_SHARED_LDPC = 2
+BATCH_SHARED_PERSISTENT = 4
 
 
 class fecl_server_options(C.Structure):

@@ -224,7 +224,9 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
     if (!out) fail(FECL_EINVAL, "null output");
     *out = nullptr;
     if (!jobs || njobs == 0) fail(FECL_EINVAL, "empty batch");
-    if (flags & ~(FECL_BATCH_AUTOTUNE | FECL_BATCH_SHARED_LDPC)) fail(FECL_EINVAL, "Invalid batch flags");
+    if (flags & ~(FECL_BATCH_AUTOTUNE | FECL_BATCH_SHARED_LDPC | FECL_BATCH_SHARED_PERSISTENT))
+      fail(FECL_EINVAL, "Invalid batch flags");
+    const bool persistent = (flags & FECL_BATCH_SHARED_PERSISTENT) != 0;
     std::vector<JobState> js(njobs);
     std::set<fecl_codec_s*> codecs;
     for (uint32_t i = 0; i < njobs; ++i) {
@@ -286,7 +288,7 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
     std::ostringstream plan;
     for (auto& s : js) {
       if (s.lte) continue;
-      if ((flags & FECL_BATCH_SHARED_LDPC) && SharedLdpc::eligible(s.c)) {
+      if ((flags & (FECL_BATCH_SHARED_LDPC | FECL_BATCH_SHARED_PERSISTENT)) && SharedLdpc::eligible(s.c)) {
         s.multi = true;
         continue;
       }
@@ -389,8 +391,8 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
       // the shared LDPC launches on branch 0: stage every job, run every class, finish
       // every job
       if (!shared.empty()) {
-        shared.launch(base, b->cap2[0]);
-        plan << shared.describe();
+        shared.launch(base, b->cap2[0], persistent);
+        plan << shared.describe(persistent);
       }
       const int first = shared.empty() ? 0 : 1;  // branch 0 holds the shared launches
       int k = 0;

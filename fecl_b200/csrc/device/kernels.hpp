@@ -120,6 +120,14 @@ int64_t ldpc_lanes_h2_group_bytes(int64_t N, int64_t E);
 cudaError_t launch_ldpc_h2_stage(const LdpcLanesParams& p, cudaStream_t s);
 cudaError_t launch_ldpc_h2_finish(const LdpcLanesParams& p, cudaStream_t s);
 cudaError_t launch_ldpc_h2_multi(LdpcMultiParams m, int d_max, cudaStream_t s);
+// The same groups with one launch per pass instead of one persistent launch: per
+// wave, the initial bit pass, then per iteration one check launch (all the wave's
+// groups, one check-degree class) and one bit launch.
+struct LdpcManyWave {
+  int32_t q0 = 0, groups = 0;      // the wave's groups [q0, q0 + groups) of the table
+  int32_t max_rows = 0, max_bits = 0, iterations = 0;  // largest M, N and iteration limit among them
+};
+cudaError_t launch_ldpc_h2_many(const LdpcMultiParams& m, const LdpcManyWave& w, int d_max, cudaStream_t s);
 
 // Flooding BP with each frame's messages resident in the shared memory of a
 // thread-block cluster of `cluster` CTAs (ldpc_cluster.cu).  The address tables are

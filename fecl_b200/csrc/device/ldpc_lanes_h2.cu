@@ -510,6 +510,68 @@ dim3 grid_for(int64_t per_group, int groups) {
 // than two).
 constexpr int64_t kWaveCap = 96ll << 20;
 
+// ---- several codes, one launch per pass ---------------------------------------
+
+// The passes of h2_check / h2_bit over the groups [q0, q0 + gridDim.y) of a group
+// table spanning several codes (each group's code parameters copied to shared memory
+// by its blocks), so that one check launch per check-degree class and one bit launch
+// serve every code of a batch in an iteration.  A block's rows (or bits) are those of
+// h2_check / h2_bit for its group, so every frame gets exactly its own code's passes;
+// blocks past their group's rows return at once.
+__device__ __forceinline__ void load_group_params(const LdpcMultiParams& m, int q, LdpcLanesParams& sp, int& g) {
+  const LdpcMultiGroup gr = m.groups[q];
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(m.codes + gr.code);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&sp);
+  for (int i = threadIdx.x; i < int(sizeof(LdpcLanesParams) / 4); i += blockDim.x) dst[i] = src[i];
+  g = gr.group;
+  __syncthreads();
+}
+
+template <int DMAX>
+__global__ void __launch_bounds__(kWarps * 32) h2_check_many(LdpcMultiParams m, int it, int q0) {
+  pdl_enter();
+  __shared__ LdpcLanesParams sp;
+  int g;
+  load_group_params(m, q0 + int(blockIdx.y), sp, g);
+  const LdpcLanesParams& p = sp;
+  constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  if (it >= p.iterations) return;
+  const int lane = threadIdx.x & 31;
+  const int warps = int(gridDim.x) * kWarps;
+  const bool check_syndrome = it > 0 && !p.fixed_iterations;
+  const uint32_t ax = active_of(p, it)[2 * g], ay = active_of(p, it)[2 * g + 1];
+  if ((ax | ay) == 0) return;
+  const bool mx = (ax >> lane) & 1, my = (ay >> lane) & 1;
+  const bool keep_all = p.msg_out || p.syst_out || p.parity_out || p.state_out;
+  uint32_t bx = 0, by = 0;
+  const int w0 = int(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  for (int r = w0 * kRows; r < p.M; r += warps * kRows)
+    check_rows<DMAX>(p, it, g, r, lane, mx, my, keep_all, check_syndrome, bx, by);
+  bx &= ax;
+  by &= ay;
+  if (lane == 0) {
+    if (bx) atomicOr(fail_of(p, it) + 2 * g, bx);
+    if (by) atomicOr(fail_of(p, it) + 2 * g + 1, by);
+  }
+}
+
+__global__ void __launch_bounds__(kWarps * 32) h2_bit_many(LdpcMultiParams m, int it, int q0) {
+  pdl_enter();
+  __shared__ LdpcLanesParams sp;
+  int g;
+  load_group_params(m, q0 + int(blockIdx.y), sp, g);
+  const LdpcLanesParams& p = sp;
+  if (it >= p.iterations) return;
+  const int lane = threadIdx.x & 31;
+  const int warps = int(gridDim.x) * kWarps;
+  const uint32_t ax = it < 0 ? 0xffffffffu : active_of(p, it)[2 * g];
+  const uint32_t ay = it < 0 ? 0xffffffffu : active_of(p, it)[2 * g + 1];
+  if (it >= 0 && blockIdx.x == 0 && threadIdx.x < 2) retire_half(p, it, g, threadIdx.x);
+  const bool mx = (ax >> lane) & 1, my = (ay >> lane) & 1;
+  if (!mx && !my) return;
+  for (int b = int(blockIdx.x) * kWarps + (threadIdx.x >> 5); b < p.N; b += warps) bit_one(p, g, b, lane, mx, my);
+}
+
 // One persistent launch when asked for (persist == 1) for batches of at most
 // kPersistGroups groups, all in one wave, on a stream that is not capturing (the
 // per-pass launches are the built-in choice: see ldpc_lanes.cu).
@@ -653,6 +715,21 @@ cudaError_t launch_ldpc_h2_finish(const LdpcLanesParams& p, cudaStream_t s) {
   if (p.groups <= 0) return cudaSuccess;
   h2_finish<<<dim3((148 * 8 + p.groups - 1) / p.groups, p.groups), 256, 0, s>>>(p);
   return cudaGetLastError();
+}
+
+cudaError_t launch_ldpc_h2_many(const LdpcMultiParams& m, const LdpcManyWave& w, int d_max, cudaStream_t s) {
+  if (w.groups <= 0 || w.groups > 65535) return w.groups == 0 ? cudaSuccess : cudaErrorInvalidValue;
+  const dim3 gbit = grid_for(w.max_bits, w.groups);
+  const int kRows = d_max <= 8 ? 2 : 1;
+  const dim3 gchk = grid_for((w.max_rows + kRows - 1) / kRows, w.groups);
+  cudaError_t e = launch_pdl(h2_bit_many, gbit, dim3(kWarps * 32), s, m, -1, w.q0);
+  for (int it = 0; e == cudaSuccess && it < w.iterations; ++it) {
+    if (d_max <= 8) e = launch_pdl(h2_check_many<8>, gchk, dim3(kWarps * 32), s, m, it, w.q0);
+    else if (d_max <= 16) e = launch_pdl(h2_check_many<16>, gchk, dim3(kWarps * 32), s, m, it, w.q0);
+    else e = launch_pdl(h2_check_many<32>, gchk, dim3(kWarps * 32), s, m, it, w.q0);
+    if (e == cudaSuccess) e = launch_pdl(h2_bit_many, gbit, dim3(kWarps * 32), s, m, it, w.q0);
+  }
+  return e;
 }
 
 cudaError_t launch_ldpc_h2_multi(LdpcMultiParams m, int d_max, cudaStream_t s) {

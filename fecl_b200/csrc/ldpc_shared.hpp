@@ -1,9 +1,9 @@
-// The shared persistent LDPC launch of a mixed batch (batch.cu) or of a server batch
-// (server.cu): the LDPC jobs that take the packed FP16 decoder, grouped by
-// check-degree class, every class's frame groups packed into waves that fit in L2
-// and decoded by one cooperative launch (ldpc_lanes_h2.cu, h2_multi).  Each job keeps
-// its own scratch, stage and finish launches; the results are those of decoding each
-// job alone, bit for bit.
+// Shared LDPC launches of a mixed batch (batch.cu) or of a server batch (server.cu):
+// the LDPC jobs that take the packed FP16 decoder, grouped by check-degree class,
+// every class's frame groups packed into waves that fit in L2 and decoded either with
+// one launch per pass over all of a wave's groups (h2_check_many / h2_bit_many) or by
+// one cooperative launch per class (h2_multi).  Each job keeps its own scratch, stage
+// and finish launches; the results are those of decoding each job alone, bit for bit.
 #pragma once
 
 #include <algorithm>
@@ -121,21 +121,41 @@ class SharedLdpc {
     return e;
   }
 
-  // Stage every job, run every launch, finish every job, all on stream s.
-  void launch(char* dev_base, cudaStream_t s) const {
+  // Stage every job, run every class's passes (persistent: one cooperative launch per
+  // class; else one launch per pass over each wave's groups), finish every job, all on
+  // stream s.
+  void launch(char* dev_base, cudaStream_t s, bool persistent) const {
     for (auto& j : jobs) cuda_check(fecl::launch_ldpc_h2_stage(j.lp, s), "LDPC stage");
-    for (auto& ml : passes_)
-      cuda_check(fecl::launch_ldpc_h2_multi(params(ml, dev_base), ml.d_max, s), "LDPC shared launch");
+    for (auto& ml : passes_) {
+      const fecl::LdpcMultiParams m = params(ml, dev_base);
+      if (persistent) {
+        cuda_check(fecl::launch_ldpc_h2_multi(m, ml.d_max, s), "LDPC shared launch");
+        continue;
+      }
+      for (size_t w = 0; w + 1 < ml.wave_ptr.size(); ++w) {
+        fecl::LdpcManyWave wave;
+        wave.q0 = ml.wave_ptr[w];
+        wave.groups = ml.wave_ptr[w + 1] - ml.wave_ptr[w];
+        for (int q = wave.q0; q < wave.q0 + wave.groups; ++q) {
+          const fecl::LdpcLanesParams& p = jobs[ml.jobs[ml.groups[q].code]].lp;
+          wave.max_rows = std::max(wave.max_rows, p.M);
+          wave.max_bits = std::max(wave.max_bits, p.N);
+          wave.iterations = std::max(wave.iterations, p.iterations);
+        }
+        cuda_check(fecl::launch_ldpc_h2_many(m, wave, ml.d_max, s), "LDPC shared passes");
+      }
+    }
     for (auto& j : jobs) cuda_check(fecl::launch_ldpc_h2_finish(j.lp, s), "LDPC finish");
   }
 
-  // One line per launch.
-  std::string describe() const {
+  // One line per class.
+  std::string describe(bool persistent) const {
     std::string t;
     for (auto& ml : passes_)
-      t += "ldpc shared launch (check degree <= " + std::to_string(ml.d_max) + "): " + std::to_string(ml.jobs.size()) +
-           " codes, " + std::to_string(ml.groups.size()) + " groups of 64 frames in " +
-           std::to_string(ml.wave_ptr.size() - 1) + " waves\n";
+      t += std::string(persistent ? "ldpc shared persistent launch" : "ldpc shared launches per pass") +
+           " (check degree <= " + std::to_string(ml.d_max) + "): " + std::to_string(ml.jobs.size()) + " codes, " +
+           std::to_string(ml.groups.size()) + " groups of 64 frames in " + std::to_string(ml.wave_ptr.size() - 1) +
+           " waves\n";
     return t;
   }
   bool empty() const { return passes_.empty(); }

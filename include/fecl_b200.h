@@ -378,8 +378,8 @@ int fecl_lte_turbo_decode_noalloc(uint32_t K, int32_t algorithm, uint32_t iterat
  * LTE turbo codes of any K, any other turbo code -- with one CUDA graph launch.
  * Every LTE turbo frame goes into one persistent launch over all K (longest
  * frames first); every other job gets the decoder fecl_decode would pick for it
- * (with FECL_BATCH_SHARED_LDPC the packed FP16 LDPC jobs instead share one persistent
- * launch per check-degree class),
+ * (with FECL_BATCH_SHARED_LDPC the packed FP16 LDPC jobs instead share their
+ * launches),
  * or, with FECL_BATCH_AUTOTUNE, the fastest of the LDPC kernel shapes that compute
  * the same bits, timed on the job's own data at creation and remembered for the
  * process.  Results equal those of fecl_decode on each job alone, bit for bit.
@@ -399,10 +399,13 @@ typedef struct {
   int32_t* iterations; /* [nframes] or NULL */
 } fecl_batch_job;
 #define FECL_BATCH_AUTOTUNE 1
-/* The LDPC jobs that take the packed FP16 decoder share one persistent launch per
- * check-degree class, wave by wave, grid barriers between the passes (the same bits
- * as their own launches, which are the default: they measured faster). */
+/* The LDPC jobs that take the packed FP16 decoder share their launches: per wave of
+ * frame groups (from every such code, fitting in L2 together) one launch per check
+ * pass and check-degree class and one per bit pass -- or, with
+ * FECL_BATCH_SHARED_PERSISTENT, one persistent launch per class with grid barriers
+ * between the passes.  The same bits as each job's own launches. */
 #define FECL_BATCH_SHARED_LDPC 2
+#define FECL_BATCH_SHARED_PERSISTENT 4
 int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags, fecl_batch_t* out);
 /* Launches the batch's graph on `stream` (asynchronous). */
 int fecl_batch_run(fecl_batch_t batch, void* stream);

@@ -94,7 +94,7 @@ def test_batch_rerun_with_new_inputs_and_option_change():
         b.run()
 
 
-@pytest.mark.parametrize("shared", [True, False])
+@pytest.mark.parametrize("shared", [None, "passes", "persistent"])
 def test_batch_shared_ldpc_launch_equals_each_codec_alone(shared):
     """FP16-message LDPC jobs of several codes and check-degree classes, several
     frame groups each and more than one wave, beside turbo frames: with the shared
@@ -119,7 +119,7 @@ def test_batch_shared_ldpc_launch_equals_each_codec_alone(shared):
                      torch.zeros(nf, dtype=torch.int32, device="cuda")))
     ref = _alone(jobs)
     b = F.Batch(jobs, shared_ldpc=shared)
-    assert ("shared launch" in b.describe()) == shared
+    assert ("ldpc shared" in b.describe()) == (shared is not None)
     for rep in range(2):
         for _, _, m, it in jobs:
             m.fill_(7)
