@@ -816,12 +816,6 @@ class Turbo(Codec):
         (32 or 64, 0 for the built-in choice)."""
         _check(_L.fecl_turbo_set_window_segments(self._h, int(segments)))
 
-    def setWindowWarm(self, steps):
-        """Extension: training steps of the windowed LTE decoder's segments from the
-        previous pass's metrics (multiple of 8; -2 for flat starts, -1 for the built-in
-        choice)."""
-        _check(_L.fecl_turbo_set_window_warm(self._h, int(steps)))
-
     def windowStats(self):
         """Extension: (passes, fix-up rounds, recomputed segments) since the last call."""
         a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()

@@ -338,7 +338,6 @@ void launch_decode(fecl_codec_s* c, const Launch& d, const ScratchPlan& sp, uint
     r.algorithm = c->tdev.algorithm;
     r.train = c->lte_train;
     r.segs = c->lte_segs;
-    r.train_warm = c->lte_warm;
     r.perm[0] = c->tdev.c[0].perm;
     r.perm[1] = c->tdev.c[1].perm;
     r.sf = c->tdev.sf;
@@ -997,17 +996,6 @@ int fecl_turbo_set_window_segments(fecl_codec_t codec, int32_t segments) {
     if (segments != 0 && segments != 32 && segments != 64) fail(FECL_EINVAL, "window segments must be 0, 32 or 64");
     std::lock_guard<std::mutex> lk(c->mu);
     c->lte_segs = segments;
-  });
-}
-
-int fecl_turbo_set_window_warm(fecl_codec_t codec, int32_t steps) {
-  return guarded([&] {
-    auto c = checked(codec);
-    if (c->kind != 1) fail(FECL_EINVAL, "not a turbo codec");
-    if (steps != -1 && steps != -2 && (steps < 0 || steps % 8 != 0 || steps > 4096))
-      fail(FECL_EINVAL, "warm training steps must be -1, -2 or a multiple of 8");
-    std::lock_guard<std::mutex> lk(c->mu);
-    c->lte_warm = steps;
   });
 }
 

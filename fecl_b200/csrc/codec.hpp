@@ -340,7 +340,6 @@ struct fecl_codec_s {
   std::atomic<uint64_t> generation{0};  // bumped whenever the decoder options (and their device tables) change
   int lte_train = -1;
   int lte_segs = 0;  // windowed LTE decoder: segments per direction (0: built-in choice)
-  int lte_warm = -1;  // windowed LTE decoder: warm training steps (-1: built-in choice, -2: flat starts)
   int kernel_sel = FECL_KERNEL_AUTO;
   bool force_generic_() const { return kernel_sel == FECL_KERNEL_GENERIC; }
 

@@ -234,7 +234,6 @@ struct TurboLteParams {
   int32_t iterations = 6;
   int32_t algorithm = 2;
   int32_t train = -1;  // training steps before each segment (-1: default)
-  int32_t train_warm = -1;  // after a constituent's first pass: training steps from its previous pass's checkpoints (-1: default, -2: flat starts)
   int32_t segs = 0;    // segments per direction, 32 or 64 (0: default)
   const uint32_t* perm[2] = {nullptr, nullptr};  // interleavers of the constituents
   const float* sf = nullptr;                     // [2][iterations]
@@ -289,7 +288,6 @@ struct TurboLteBatchParams {
   int32_t max_K = 0;           // largest K in the batch (sizes shared memory)
   int32_t algorithm = 2;       // one algorithm per launch
   int32_t train = -1;          // training steps (-1: default)
-  int32_t train_warm = -1;     // warm training steps (-1: default, -2: flat starts)
   int32_t ctas = 0;            // persistent CTAs (0: as many as are resident at once)
   unsigned long long* stats = nullptr;
 };

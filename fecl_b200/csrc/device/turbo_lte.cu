@@ -65,9 +65,6 @@ struct Tol {
 constexpr Tol kDecodeTol = {1e-3f, 1e-5f};
 constexpr Tol kSoftTol = {1e-6f, 1e-6f};
 constexpr int kDefaultSegs = 64;
-// Training steps before a segment whose start comes from the previous pass's
-// checkpoints (-2: none, every pass trains from a flat start).
-constexpr int kDefaultWarm = -2;
 
 __constant__ LinearLut c_lut;
 
@@ -125,7 +122,22 @@ struct Gam {
   }
 };
 
-// alpha_{t+1} from alpha_t (MapDecoderImpl.cpp:117-139, :237-274), not normalised.
+// The log-MAP recursions keep the reference's normalisation after every step (max-log
+// normalises once per chunk, see above): their table and exp/log corrections are not
+// translation-invariant in FP32, so this keeps their rounding that of the reference.
+template <int ALG>
+__device__ __forceinline__ void normalize_step(float v[8]) {
+  if constexpr (ALG != kApproximate) {
+    float m = kNegInf;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) m = fmaxf(v[s], m);
+#pragma unroll
+    for (int s = 0; s < 8; ++s) v[s] = v[s] - m;
+  }
+}
+
+// alpha_{t+1} from alpha_t (MapDecoderImpl.cpp:117-139, :237-274); normalised here only
+// by the log-MAP algorithms.
 template <int ALG>
 __device__ __forceinline__ void fwd_step(float a[8], const Gam& g) {
   float c0[8], c1[8];
@@ -151,9 +163,11 @@ __device__ __forceinline__ void fwd_step(float a[8], const Gam& g) {
     else if (ALG == kApproximate) a[s] = fmaxf(c0[s], c1[s]);
     else a[s] = lsum<ALG>(lsum<ALG>(kNegInf, c0[s]), c1[s]);
   }
+  normalize_step<ALG>(a);
 }
 
-// beta_t from beta_{t+1} (MapDecoderImpl.cpp:141-172, :276-329), not normalised.
+// beta_t from beta_{t+1} (MapDecoderImpl.cpp:141-172, :276-329); normalised here only by
+// the log-MAP algorithms.
 template <int ALG>
 __device__ __forceinline__ void bwd_step(float b[8], const Gam& g) {
   float n[8];
@@ -167,6 +181,7 @@ __device__ __forceinline__ void bwd_step(float b[8], const Gam& g) {
   }
 #pragma unroll
   for (int s = 0; s < 8; ++s) b[s] = n[s];
+  normalize_step<ALG>(b);
 }
 
 // Extrinsic value of one step, L(u) - La (msgUpdateImpl, MapDecoderImpl.cpp:331-376).
@@ -299,7 +314,6 @@ template <int SEGS>
 struct Shared {
   float sv[2][SEGS][8];  // metrics at the segment boundary after training (fwd, bwd)
   float ev[2][SEGS][8];  // end metrics of each segment (fwd, bwd)
-  float in[2][SEGS][8];  // warm training starts: the previous pass's checkpoints
   float flat[8];         // training start: all states equal
   float term[8];         // trellis termination: state 0
   uint32_t crc_part[2 * SEGS / 32];  // per-warp CRC syndromes
@@ -561,11 +575,10 @@ __device__ __forceinline__ void ext_block(int j, int b, int K, int T, const Fram
 // One frame's geometry and buffers, as the decode loop below sees them.
 struct LteJob {
   int32_t K = 0, Kp = 0, Tp = 0, seg_len = 0, train = 0, iterations = 0;
-  int32_t train_warm = -1;              // training steps from the previous pass's checkpoints (< 0: flat starts)
   const float* sf = nullptr;            // [2][iterations]
   const uint32_t* perm = nullptr;       // interleaver of constituent 1, padded by 16 entries
   const float* scratch = nullptr;       // staged L-values: Ls [Kp] | Lp0 [Tp] | Lp1 [Tp] | tail [8]
-  float* ck = nullptr;                  // checkpoints [2 constituents][2 directions][nblk + 1][8]
+  float* ck = nullptr;                  // checkpoints [2][nblk + 1][8]
   uint8_t* hard = nullptr;              // [K]
   int32_t* iters = nullptr;             // nullable
   unsigned long long* stats = nullptr;  // nullable
@@ -609,7 +622,6 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
   fr.ts = base + q.Kp + 2 * q.Tp;
   fr.cka = q.ck;
   fr.ckb = fr.cka + (nblk + 1) * 8;
-  const int ck_stride = 2 * (nblk + 1) * 8;  // one constituent's checkpoints
   const int tid = threadIdx.x;
   const int L = q.seg_len;
   const int S = (T + L - 1) / L;
@@ -642,23 +654,6 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
     for (int jj = 0; jj < 2; ++jj) {
       const int j = q.parallel ? 1 - jj : jj;  // parallel: constituent 1 first, on the old X
       const uint32_t* perm = q.perm;
-      fr.cka = q.ck + j * ck_stride;
-      fr.ckb = fr.cka + (nblk + 1) * 8;
-      // Warm training: after its first pass a constituent's checkpoints hold its last
-      // pass's (verified) metrics, which start this pass's training runs better than a
-      // flat vector: they are read into shared memory before any walk rewrites them.
-      const bool warm = q.train_warm >= 0 && it > 0;
-      const int G = warm ? q.train_warm : q.train;
-      if (warm) {
-        const bool fwd = tid < SEGS;
-        const int w = fwd ? tid : tid - SEGS;
-        if (w < S) {
-          const int a0 = w * L, a1 = min(T, a0 + L);
-          if (fwd && w > 0 && a0 - G > 0) load_ck(fr.cka + ((a0 - G) / kBlk) * 8, sh.in[0][w]);
-          if (!fwd && w < S - 1 && a1 + G < T) load_ck(fr.ckb + ((a1 + G) / kBlk) * 8, sh.in[1][w]);
-        }
-        __syncthreads();
-      }
       // ---- A: segments with training starts
       {
         const bool fwd = tid < SEGS;
@@ -668,13 +663,13 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
           int t_train;
           const float* vin;
           if (fwd) {
-            const bool exact = (w == 0 || a0 - G <= 0);
-            t_train = exact ? 0 : a0 - G;
-            vin = exact ? sh.term : (warm ? sh.in[0][w] : sh.flat);
+            const bool exact = (w == 0 || a0 - q.train <= 0);
+            t_train = exact ? 0 : a0 - q.train;
+            vin = exact ? sh.term : sh.flat;
           } else {
-            const bool exact = (w == S - 1 || a1 + G >= T);
-            t_train = exact ? T : a1 + G;
-            vin = exact ? sh.term : (warm ? sh.in[1][w] : sh.flat);
+            const bool exact = (w == S - 1 || a1 + q.train >= T);
+            t_train = exact ? T : a1 + q.train;
+            vin = exact ? sh.term : sh.flat;
           }
           segment_walk<ALG>(fwd, j, t_train, a0, a1, vin, sh.sv[fwd ? 0 : 1][w], sh.ev[fwd ? 0 : 1][w], K, T, fr, X,
                             Y, perm, false, tol);
@@ -818,8 +813,7 @@ __global__ void __launch_bounds__(2 * SEGS, SEGS == 32 ? 4 : 3) turbo_lte_kernel
   q.sf = p.sf;
   q.perm = p.perm[1];
   q.scratch = p.scratch + f * p.frame_stride;
-  q.ck = p.ck + f * int64_t(4 * (nblk + 1) * 8);
-  q.train_warm = p.train_warm;
+  q.ck = p.ck + f * int64_t(2 * (nblk + 1) * 8);
   q.hard = p.hard + f * p.K;
   q.iters = p.iters ? p.iters + f : nullptr;
   q.stats = p.stats;
@@ -889,7 +883,7 @@ struct LteGeometry {
     seg_len = lte_seg_len(T, segs);
   }
   // Staged inputs then checkpoints, rounded to 128 bytes so frames share no cache line.
-  __host__ __device__ int frame_floats() const { return (stride + 4 * (nblk + 1) * 8 + 31) & ~31; }
+  __host__ __device__ int frame_floats() const { return (stride + 2 * (nblk + 1) * 8 + 31) & ~31; }
 };
 
 // Stages element i of a frame's staged inputs from FeCl's turbo layout
@@ -940,7 +934,6 @@ __global__ void __launch_bounds__(2 * SEGS, SEGS == 32 ? 4 : 3) turbo_lte_batch_
     q.perm = d.perm;
     q.scratch = d.scratch;
     q.ck = d.scratch + g.stride;
-    q.train_warm = p.train_warm;
     q.hard = d.hard;
     q.iters = d.iters;
     q.stats = p.stats;
@@ -972,7 +965,7 @@ size_t turbo_lte_scratch_bytes(int K, int64_t nframes, bool extra) {
   const int Tp = nblk * kBlk;
   const int Kp = Tp;
   const int64_t stride = Kp + 2 * Tp + 8;
-  return size_t(nframes) * (size_t(stride) + size_t(4 * (nblk + 1) * 8) + (extra ? size_t(3 * Tp) : 0)) * sizeof(float);
+  return size_t(nframes) * (size_t(stride) + size_t(2 * (nblk + 1) * 8) + (extra ? size_t(3 * Tp) : 0)) * sizeof(float);
 }
 
 cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
@@ -987,11 +980,10 @@ cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
   p.ck = p.scratch + p.nframes * p.frame_stride;
   // parallel scheduling and soDecode: per frame ynew [Tp] | soft_ext [2][Tp] after the
   // checkpoints (turbo_lte_scratch_bytes(K, n, true))
-  p.ynew = (p.parallel || p.soft) ? p.ck + p.nframes * int64_t(4 * (g.nblk + 1) * 8) : nullptr;
+  p.ynew = (p.parallel || p.soft) ? p.ck + p.nframes * int64_t(2 * (g.nblk + 1) * 8) : nullptr;
   if (p.soft) p.crc = nullptr;
   p.seg_len = g.seg_len;
   if (p.train < 0) p.train = 96;
-  if (p.train_warm == -1) p.train_warm = kDefaultWarm;
   const unsigned stage_blocks = unsigned(p.nframes < 148 * 8 ? p.nframes : 148 * 8);
   switch (p.llr_dtype) {
     case kF64: turbo_lte_stage<double><<<stage_blocks, 256, 0, s>>>(p); break;
@@ -1059,7 +1051,6 @@ cudaError_t launch_turbo_lte_batch(const TurboLteBatchParams& p, cudaStream_t s)
   if (p.max_K <= 0 || p.max_K > 12288) return cudaErrorInvalidValue;
   TurboLteBatchParams q = p;
   if (q.train < 0) q.train = 96;
-  if (q.train_warm == -1) q.train_warm = kDefaultWarm;
   e = cudaMemsetAsync(q.counter, 0, sizeof(int32_t), s);
   if (e != cudaSuccess) return e;
   const unsigned stage_blocks = unsigned(q.nframes < 148 * 8 ? q.nframes : 148 * 8);

@@ -338,14 +338,6 @@ int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps);
  * reference. */
 int fecl_turbo_set_window_segments(fecl_codec_t codec, int32_t segments);
 
-/* Windowed turbo decoder: after a constituent's first pass, start each segment's
- * training run this many steps (a multiple of 8) before the segment from the
- * metrics that constituent's previous pass left there, instead of from a flat vector
- * `training` steps before (-2: always flat starts; -1 restores the built-in choice).
- * Results do not depend on it beyond FP32 rounding.  Extension: no counterpart in
- * the reference. */
-int fecl_turbo_set_window_warm(fecl_codec_t codec, int32_t steps);
-
 /* Windowed turbo decoder counters since the previous call (which resets them):
  * constituent passes run, verification rounds that found a boundary to
  * recompute, and segments recomputed. */

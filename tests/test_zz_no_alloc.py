@@ -42,7 +42,7 @@ def _decode_pair(K, n, alg, dtype, seed, ebn0):
 
 def test_noalloc_matches_allocating_decode_on_two_calls():
     import fecl_b200 as F
-    K, n = 6144, 32
+    K, n = 6144, 48
     for call, seed in enumerate((501, 502)):
         expected, got = _decode_pair(K, n, F.Approximate, "f32", seed, 0.7 + 0.2 * call)
         assert np.array_equal(got, expected), "call %d: %d bits differ" % (call, int(np.sum(got != expected)))
