@@ -833,7 +833,9 @@ def run_serving(args, embedded=False):
         row = {"offered_frames_per_s": rate, "requests": n, "sustained_info_mbps": round(bits / rep["wall_s"] / 1e6, 2),
                "completed_frames_per_s": round(n / rep["wall_s"], 1), "p50_ms": round(1e3 * float(np.median(lat)), 3),
                "p99_ms": round(1e3 * float(np.quantile(lat, 0.99)), 3), "batches": rep["batches"],
-               "fer": round(errs / n, 4), "replay_wall_s": round(wall, 3)}
+               "fer": round(errs / n, 4), "replay_wall_s": round(wall, 3),
+               "batch_frames_mean": round(rep["batch_frames"], 1), "batch_gpu_ms_mean": round(1e3 * rep["batch_gpu_s"], 3),
+               "batch_host_ms_mean": round(1e3 * rep["batch_host_s"], 3)}
         rows.append(row)
         if peak is None or row["sustained_info_mbps"] > peak["sustained_info_mbps"]:
             peak = row

@@ -102,6 +102,7 @@ class fecl_server_stats(C.Structure):
     _fields_ = [
         ("requests", C.c_uint64), ("frames", C.c_uint64), ("info_bits", C.c_uint64), ("batches", C.c_uint64),
         ("p50_s", C.c_double), ("p99_s", C.c_double), ("max_s", C.c_double), ("wall_s", C.c_double),
+        ("batch_gpu_s", C.c_double), ("batch_host_s", C.c_double), ("batch_frames", C.c_double),
     ]
 
 

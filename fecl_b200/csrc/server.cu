@@ -95,6 +95,7 @@ struct Slot {
   cudaStream_t side[kSideStreams] = {};
   cudaEvent_t fork = nullptr, joined[kSideStreams] = {};
   cudaEvent_t done = nullptr;
+  cudaEvent_t start = nullptr;  // timing: the batch's first operation
   DeviceBuffer arena;
   PinnedBuffer in, out;
   std::vector<std::shared_ptr<Request>> reqs;
@@ -117,6 +118,7 @@ struct fecl_server_s {
   // statistics since creation or the last reset
   std::vector<double> latencies;
   uint64_t frames_done = 0, bits_done = 0, batches = 0;
+  double gpu_s_sum = 0.0, host_s_sum = 0.0;
   Clock::time_point first_submit{}, last_done{};
   bool any_submit = false;
   std::string error;
@@ -265,6 +267,7 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
   s.in.reserve(std::max<size_t>(host_end, 256));
   s.out.reserve(std::max<size_t>(out_end, 256));
   for (auto& r : batch) std::memcpy(s.in.as() + r->llr_off, r->llr, r->in_bytes);
+  cuda_check(cudaEventRecord(s.start, s.stream), "cudaEventRecord");
   cuda_check(cudaMemcpyAsync(base, s.in.as(), in_end, cudaMemcpyHostToDevice, s.stream), "copy in");
   for (auto& kv : tdesc) {
     auto& v = kv.second;
@@ -327,7 +330,10 @@ void fecl_server_s::harvest(Slot& s) {
     if (r->iters) std::memcpy(r->iters, s.out.as() + r->it_off, r->n * 4);
   }
   const auto now = Clock::now();
+  float gpu_ms = 0.0f;
+  if (cudaEventElapsedTime(&gpu_ms, s.start, s.done) != cudaSuccess) cudaGetLastError();
   std::lock_guard<std::mutex> lk(mu);
+  gpu_s_sum += 1e-3 * double(gpu_ms);
   for (auto& r : s.reqs) {
     r->t_done = now;
     r->done = true;
@@ -420,7 +426,11 @@ void fecl_server_s::run() {
         for (auto& r : batch) cs.insert(r->c);
         std::vector<std::unique_lock<std::mutex>> locks;
         for (auto* c : cs) locks.emplace_back(c->mu);
+        const auto t0 = Clock::now();
         launch(*free_slot, batch);
+        const double host_s = std::chrono::duration<double>(Clock::now() - t0).count();
+        std::lock_guard<std::mutex> lk(mu);
+        host_s_sum += host_s;
       } catch (const Error& e) {
         std::lock_guard<std::mutex> lk(mu);
         for (auto& r : batch) {
@@ -463,7 +473,8 @@ int fecl_server_create(const fecl_server_options* options, fecl_server_t* out) {
     for (uint32_t i = 0; i < o.slots; ++i) {
       std::unique_ptr<Slot> sl(new Slot);
       cuda_check(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-      cuda_check(cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming), "cudaEventCreate");
+      cuda_check(cudaEventCreate(&sl->done), "cudaEventCreate");
+      cuda_check(cudaEventCreate(&sl->start), "cudaEventCreate");
       cuda_check(cudaEventCreateWithFlags(&sl->fork, cudaEventDisableTiming), "cudaEventCreate");
       for (int q = 0; q < kSideStreams; ++q) {
         cuda_check(cudaStreamCreateWithFlags(&sl->side[q], cudaStreamNonBlocking), "cudaStreamCreate");
@@ -544,6 +555,10 @@ int fecl_server_report(fecl_server_t server, fecl_server_stats* st) {
     st->p99_s = pct(0.99);
     st->max_s = l.empty() ? 0.0 : l.back();
     st->wall_s = server->any_submit ? std::chrono::duration<double>(server->last_done - server->first_submit).count() : 0.0;
+    const double nb = server->batches ? double(server->batches) : 1.0;
+    st->batch_gpu_s = server->gpu_s_sum / nb;
+    st->batch_host_s = server->host_s_sum / nb;
+    st->batch_frames = double(server->frames_done) / nb;
   });
 }
 
@@ -553,6 +568,7 @@ int fecl_server_reset_stats(fecl_server_t server) {
     std::lock_guard<std::mutex> lk(server->mu);
     server->latencies.clear();
     server->frames_done = server->bits_done = server->batches = 0;
+    server->gpu_s_sum = server->host_s_sum = 0.0;
     server->any_submit = false;
   });
 }
@@ -603,6 +619,7 @@ void fecl_server_destroy(fecl_server_t server) {
     }
     cudaEventDestroy(s->fork);
     cudaEventDestroy(s->done);
+    cudaEventDestroy(s->start);
     cudaStreamDestroy(s->stream);
   }
   delete server;

@@ -428,6 +428,9 @@ typedef struct {
   uint64_t requests, frames, info_bits, batches; /* finished since creation or the last reset */
   double p50_s, p99_s, max_s; /* request latency, submission to decisions in host memory */
   double wall_s;              /* first submission to last completion */
+  double batch_gpu_s;         /* mean device time of a batch, first copy in to last copy out */
+  double batch_host_s;        /* mean host time to lay out and launch a batch */
+  double batch_frames;        /* mean frames per batch */
 } fecl_server_stats;
 int fecl_server_create(const fecl_server_options* options, fecl_server_t* out);
 /* Queues nframes frames of `codec`: llr [nframes][paritySize] of llr_dtype, msg
