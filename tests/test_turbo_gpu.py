@@ -239,9 +239,10 @@ def test_custom_scheduling_matches_reference(stages, alg):
         assert_soft_parity(getattr(got, k)(), out[k], ok, size, what=k, exact=alg == 0)
 
 
+@pytest.mark.parametrize("kernel", ["auto", "generic"])
 @pytest.mark.parametrize("sched", [0, 1])
 @pytest.mark.parametrize("alg", [2, 1, 0])
-def test_windowed_soDecode_and_parallel_match_reference(alg, sched, has_ref):
+def test_windowed_soDecode_and_parallel_match_reference(alg, sched, kernel, has_ref):
     """LTE soDecode (with a-priori and state inputs, every soft output) and Parallel
     scheduling on the windowed kernel against the compiled FP64 reference on the same
     L-values, under the parity rules: hard decisions equal in every frame the
@@ -253,7 +254,7 @@ def test_windowed_soDecode_and_parallel_match_reference(alg, sched, has_ref):
     from oracle import ref
     K, n = 1024, 24
     code = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(alg).iterations(5).scheduling(sched))
-    code.setKernel("auto")
+    code.setKernel(kernel)
     msg = ch.random_bits(n * K, 70 + alg)
     llr = ch.awgn_llr(code.encode(msg), 1.2, K / code.paritySize(), 70 + alg, np.float32)
     syst = (0.05 * ch.awgn_llr(ch.random_bits(n * code.systSize(), 9), 0.0, 1.0, 9)).astype(np.float32)
