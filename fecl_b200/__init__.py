@@ -816,6 +816,22 @@ class Turbo(Codec):
         (32 or 64, 0 for the built-in choice)."""
         _check(_L.fecl_turbo_set_window_segments(self._h, int(segments)))
 
+    def tuneWindow(self, llr, out=None):
+        """Extension: time the windowed LTE decoder's equivalent window shapes on these
+        device L-values (a torch CUDA tensor) and keep the fastest; returns (segments,
+        training steps).  `out` (uint8 CUDA tensor of the decisions) is optional."""
+        import torch
+        if not _is_device(llr):
+            raise ValueError("tuneWindow needs L-values in device memory")
+        n = self._frames(llr.numel(), self.paritySize(), "parity")
+        if out is None:
+            out = torch.empty(n * self.msgSize(), dtype=torch.uint8, device=llr.device)
+        segs, train = C.c_int32(), C.c_int32()
+        stream = torch.cuda.current_stream(llr.device).cuda_stream
+        _check(_L.fecl_turbo_tune_window(self._h, C.c_void_p(llr.data_ptr()), _dtype_code(llr), n,
+                                         C.c_void_p(out.data_ptr()), C.c_void_p(stream), C.byref(segs), C.byref(train)))
+        return segs.value, train.value
+
     def windowStats(self):
         """Extension: (passes, fix-up rounds, recomputed segments) since the last call."""
         a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()

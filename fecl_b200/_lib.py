@@ -146,6 +146,8 @@ SIGNATURES = [
     ("fecl_ldpc_set_persistent", C.c_int, [C.c_void_p, C.c_int32]),
     ("fecl_turbo_set_window_training", C.c_int, [C.c_void_p, C.c_int32]),
     ("fecl_turbo_set_window_segments", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fecl_turbo_tune_window", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_uint64, C.c_void_p, C.c_void_p,
+                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("fecl_turbo_window_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("fecl_lte_turbo_decode_noalloc", C.c_int, [C.c_uint32, C.c_int32, C.c_uint32, C.c_void_p, C.c_int32, C.c_uint64, C.c_void_p, C.c_void_p]),
     ("fecl_batch_create", C.c_int, [C.POINTER(fecl_batch_job), C.c_uint32, C.c_int32, C.POINTER(C.c_void_p)]),

@@ -13,6 +13,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -820,6 +821,77 @@ int fecl_so_decode(fecl_codec_t codec, const fecl_so_io* io, uint64_t nframes, i
     if (!io->parity) fail(FECL_EINVAL, "Input must contains parity");
     std::lock_guard<std::mutex> lk(c->mu);
     run_decode(c, io, nframes, nullptr, nullptr, true, flags, static_cast<cudaStream_t>(stream));
+  });
+}
+
+// Process-wide results of the windowed turbo decoder's autotuner: (K, frames,
+// algorithm, iterations, scheduling) -> (segments, training steps).
+static std::mutex g_window_mu;
+static std::map<std::tuple<uint64_t, uint64_t, int, int, int>, std::pair<int, int>> g_window_tuned;
+
+int fecl_turbo_tune_window(fecl_codec_t codec, const void* llr, int32_t llr_dtype, uint64_t nframes, uint8_t* msg,
+                           void* stream, int32_t* segments, int32_t* training) {
+  return guarded([&] {
+    auto c = checked(codec);
+    if (c->kind != 1) fail(FECL_EINVAL, "not a turbo codec");
+    if (!llr || !msg || nframes == 0) fail(FECL_EINVAL, "null buffer or no frames");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->lte_fast_ok()) fail(FECL_EUNSUPPORTED, "the codec does not take the windowed decoder");
+    const auto& d = c->turbo->decoder();
+    const auto key = std::make_tuple(c->msg(), nframes, int(d.algorithm), int(d.iterations), int(d.scheduling));
+    std::pair<int, int> best{0, -1};
+    bool cached = false;
+    {
+      std::lock_guard<std::mutex> g(g_window_mu);
+      auto it = g_window_tuned.find(key);
+      if (it != g_window_tuned.end()) {
+        best = it->second;
+        cached = true;
+      }
+    }
+    if (!cached) {
+      // Every candidate computes the full-frame recursion up to FP32 rounding; each is
+      // timed on the caller's own L-values (second of two decodes) and the fastest kept.
+      cudaStream_t s = static_cast<cudaStream_t>(stream);
+      cudaEvent_t e0, e1;
+      cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
+      cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+      float best_ms = -1.0f;
+      fecl_so_io io{};
+      io.parity = llr;
+      io.in_dtype = llr_dtype;
+      io.out_dtype = FECL_F32;
+      try {
+        for (int segs : {64, 32})
+          for (int train : {48, 64, 80, 96, 128}) {
+            c->lte_segs = segs;
+            c->lte_train = train;
+            run_decode(c, &io, nframes, msg, nullptr, false, FECL_DEVICE_MEMORY, s);
+            cuda_check(cudaEventRecord(e0, s), "cudaEventRecord");
+            run_decode(c, &io, nframes, msg, nullptr, false, FECL_DEVICE_MEMORY, s);
+            cuda_check(cudaEventRecord(e1, s), "cudaEventRecord");
+            cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+            float ms = 0.0f;
+            cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+            if (best_ms < 0.0f || ms < best_ms) {
+              best_ms = ms;
+              best = {segs, train};
+            }
+          }
+      } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      std::lock_guard<std::mutex> g(g_window_mu);
+      g_window_tuned[key] = best;
+    }
+    c->lte_segs = best.first;
+    c->lte_train = best.second;
+    if (segments) *segments = best.first;
+    if (training) *training = best.second;
   });
 }
 

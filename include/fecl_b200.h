@@ -338,6 +338,16 @@ int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps);
  * reference. */
 int fecl_turbo_set_window_segments(fecl_codec_t codec, int32_t segments);
 
+/* Windowed turbo decoder autotuner: decodes the caller's `nframes` frames of device
+ * memory L-values (into msg) with every equivalent window shape -- 32 or 64
+ * segments per direction, 48 to 128 training steps -- keeps the fastest in the
+ * codec and returns it.  Results are remembered per (K, nframes, algorithm,
+ * iterations, scheduling) for the process, so later calls only apply them.  Every
+ * shape computes the full-frame recursion up to FP32 rounding.  Extension: no
+ * counterpart in the reference. */
+int fecl_turbo_tune_window(fecl_codec_t codec, const void* llr, int32_t llr_dtype, uint64_t nframes, uint8_t* msg,
+                           void* stream, int32_t* segments, int32_t* training);
+
 /* Windowed turbo decoder counters since the previous call (which resets them):
  * constituent passes run, verification rounds that found a boundary to
  * recompute, and segments recomputed. */

@@ -276,3 +276,24 @@ def test_windowed_soDecode_and_parallel_match_reference(alg, sched, kernel, has_
                              ("parity", so.parity(), r_so["parity"], code.paritySize()),
                              ("state2", so.state(), r_so["state"], code.stateSize())):
         assert_soft_parity(a, b, ok, size, what=name, exact=(alg == 0), linear=(alg == 1))
+
+
+def test_tune_window(has_ref):
+    """The window autotuner picks one of the equivalent shapes on the caller's inputs,
+    remembers it for the same (K, frames, options), and the tuned decoder still meets
+    the parity rules against the FP64 reference."""
+    import torch
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    from oracle import checker
+    K, n = 2048, 48
+    code = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(F.Approximate).iterations(6).scheduling(F.Serial))
+    msg = ch.random_bits(n * K, 91)
+    llr = ch.awgn_llr(code.encode(msg), 0.7, K / code.paritySize(), 91, np.float32)
+    d_llr = torch.from_numpy(llr).cuda()
+    segs, train = code.tuneWindow(d_llr)
+    assert segs in (32, 64) and train in (48, 64, 80, 96, 128)
+    assert code.tuneWindow(d_llr) == (segs, train)
+    bits = code.decode(llr)
+    ref_bits, ref_app = checker.turbo_lte_decode(K, F.Approximate, 6, F.Serial, llr)
+    assert_hard_parity(bits, ref_bits, msg, K, ref_app=ref_app)
