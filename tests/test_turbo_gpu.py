@@ -239,14 +239,16 @@ def test_custom_scheduling_matches_reference(stages, alg):
         assert_soft_parity(getattr(got, k)(), out[k], ok, size, what=k, exact=alg == 0)
 
 
-@pytest.mark.parametrize("kernel", ["auto", "generic"])
 @pytest.mark.parametrize("sched", [0, 1])
 @pytest.mark.parametrize("alg", [2, 1, 0])
-def test_windowed_soDecode_and_parallel_match_reference(alg, sched, kernel, has_ref):
+def test_windowed_soDecode_and_parallel_match_reference(alg, sched, has_ref):
     """LTE soDecode (with a-priori and state inputs, every soft output) and Parallel
     scheduling on the windowed kernel against the compiled FP64 reference on the same
     L-values, under the parity rules: hard decisions equal in every frame the
-    reference decodes, soft outputs within 1e-4 relative there."""
+    reference decodes, soft outputs within 1e-4 relative there.  With the Linear
+    algorithm the windowed kernel's soft outputs are also held to the generic kernel's
+    (the reference's operation order in FP32) under the strict tail bound, so the
+    Linear tail allowance against FP64 covers FP32 itself, not the windowing."""
     if not has_ref:
         pytest.skip("the compiled reference (oracle/_ref) is not built")
     import fecl_b200 as F
@@ -254,28 +256,36 @@ def test_windowed_soDecode_and_parallel_match_reference(alg, sched, kernel, has_
     from oracle import ref
     K, n = 1024, 24
     code = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(alg).iterations(5).scheduling(sched))
-    code.setKernel(kernel)
     msg = ch.random_bits(n * K, 70 + alg)
     llr = ch.awgn_llr(code.encode(msg), 1.2, K / code.paritySize(), 70 + alg, np.float32)
     syst = (0.05 * ch.awgn_llr(ch.random_bits(n * code.systSize(), 9), 0.0, 1.0, 9)).astype(np.float32)
     rc = ref.RefCodec.turbo([([4], [[0o15]], [0o13])], [np.arange(K), F.Turbo.Lte3Gpp.interleaver(K)], 0, alg, sched, 5,
                             workgroup=8)
     r_first = rc.so_decode(llr, outputs=("state",))
-    r_so = rc.so_decode(llr, syst=syst, state=r_first["state"].astype(np.float32),
-                        outputs=("msg", "syst", "parity", "state"))
+    state_in = r_first["state"].astype(np.float32)
+    r_so = rc.so_decode(llr, syst=syst, state=state_in, outputs=("msg", "syst", "parity", "state"))
     r_bits, r_app = rc.decode(llr), rc.so_decode(llr, outputs=("msg",))["msg"]
-    bits = code.decode(llr)
+
+    def run(kernel):
+        code.setKernel(kernel)
+        first = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output(np.float32).state())
+        so = code.soDecode(F.Codec.Input().parity(llr).syst(syst).state(state_in),
+                           F.Codec.Output(np.float32).msg().syst().parity().state())
+        return code.decode(llr), (first.state(), so.msg(), so.syst(), so.parity(), so.state())
+
+    bits, outs = run("auto")
     assert_hard_parity(bits, r_bits, msg, K, ref_app=r_app)
-    first = code.soDecode(F.Codec.Input().parity(llr), F.Codec.Output(np.float32).state())
-    so = code.soDecode(F.Codec.Input().parity(llr).syst(syst).state(r_first["state"].astype(np.float32)),
-                       F.Codec.Output(np.float32).msg().syst().parity().state())
     ok = frame_ok(r_app > 0, msg, K)
     assert ok.sum() >= n // 3
-    for name, a, b, size in (("state", first.state(), r_first["state"], code.stateSize()),
-                             ("msg", so.msg(), r_so["msg"], K), ("syst", so.syst(), r_so["syst"], code.systSize()),
-                             ("parity", so.parity(), r_so["parity"], code.paritySize()),
-                             ("state2", so.state(), r_so["state"], code.stateSize())):
+    names = ("state", "msg", "syst", "parity", "state2")
+    sizes = (code.stateSize(), K, code.systSize(), code.paritySize(), code.stateSize())
+    refs = (r_first["state"], r_so["msg"], r_so["syst"], r_so["parity"], r_so["state"])
+    for name, a, b, size in zip(names, outs, refs, sizes):
         assert_soft_parity(a, b, ok, size, what=name, exact=(alg == 0), linear=(alg == 1))
+    if alg == 1:
+        _, gen = run("generic")
+        for name, a, b, size in zip(names, outs, gen, sizes):
+            assert_soft_parity(a, b, ok, size, what=name + " vs generic")
 
 
 def test_tune_window(has_ref):
