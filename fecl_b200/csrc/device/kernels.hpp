@@ -122,7 +122,8 @@ cudaError_t launch_ldpc_h2_finish(const LdpcLanesParams& p, cudaStream_t s);
 cudaError_t launch_ldpc_h2_multi(LdpcMultiParams m, int d_max, cudaStream_t s);
 // The same groups with one launch per pass instead of one persistent launch: per
 // wave, the initial bit pass, then per iteration one check launch (all the wave's
-// groups, one check-degree class) and one bit launch.
+// groups: of one check-degree class d_max, or of every class with d_max = 0) and one
+// bit launch.
 struct LdpcManyWave {
   int32_t q0 = 0, groups = 0;      // the wave's groups [q0, q0 + groups) of the table
   int32_t max_rows = 0, max_bits = 0, iterations = 0;  // largest M, N and iteration limit among them

@@ -527,6 +527,20 @@ __device__ __forceinline__ void load_group_params(const LdpcMultiParams& m, int 
   __syncthreads();
 }
 
+// The rows of group g spread over the x blocks of its grid row (a warp per row or row
+// pair), the lanes whose syndrome failed accumulated in bx / by.
+template <int DMAX>
+__device__ __forceinline__ void check_group(const LdpcLanesParams& p, int it, int g, int lane, bool mx, bool my,
+                                            bool keep_all, bool check_syndrome, uint32_t& bx, uint32_t& by) {
+  constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  const int warps = int(gridDim.x) * kWarps;
+  const int w0 = int(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  for (int r = w0 * kRows; r < p.M; r += warps * kRows)
+    check_rows<DMAX>(p, it, g, r, lane, mx, my, keep_all, check_syndrome, bx, by);
+}
+
+// DMAX = 0: groups of every check-degree class in one launch, each block taking its
+// group's class (blocks of a grid row share a group, so the choice is uniform).
 template <int DMAX>
 __global__ void __launch_bounds__(kWarps * 32) h2_check_many(LdpcMultiParams m, int it, int q0) {
   pdl_enter();
@@ -534,19 +548,18 @@ __global__ void __launch_bounds__(kWarps * 32) h2_check_many(LdpcMultiParams m, 
   int g;
   load_group_params(m, q0 + int(blockIdx.y), sp, g);
   const LdpcLanesParams& p = sp;
-  constexpr int kRows = DMAX <= 8 ? 2 : 1;
   if (it >= p.iterations) return;
   const int lane = threadIdx.x & 31;
-  const int warps = int(gridDim.x) * kWarps;
   const bool check_syndrome = it > 0 && !p.fixed_iterations;
   const uint32_t ax = active_of(p, it)[2 * g], ay = active_of(p, it)[2 * g + 1];
   if ((ax | ay) == 0) return;
   const bool mx = (ax >> lane) & 1, my = (ay >> lane) & 1;
   const bool keep_all = p.msg_out || p.syst_out || p.parity_out || p.state_out;
   uint32_t bx = 0, by = 0;
-  const int w0 = int(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-  for (int r = w0 * kRows; r < p.M; r += warps * kRows)
-    check_rows<DMAX>(p, it, g, r, lane, mx, my, keep_all, check_syndrome, bx, by);
+  const int cls = DMAX ? DMAX : (p.d_max <= 8 ? 8 : (p.d_max <= 16 ? 16 : 32));
+  if (cls == 8) check_group<8>(p, it, g, lane, mx, my, keep_all, check_syndrome, bx, by);
+  else if (cls == 16) check_group<16>(p, it, g, lane, mx, my, keep_all, check_syndrome, bx, by);
+  else check_group<32>(p, it, g, lane, mx, my, keep_all, check_syndrome, bx, by);
   bx &= ax;
   by &= ay;
   if (lane == 0) {
@@ -720,11 +733,12 @@ cudaError_t launch_ldpc_h2_finish(const LdpcLanesParams& p, cudaStream_t s) {
 cudaError_t launch_ldpc_h2_many(const LdpcMultiParams& m, const LdpcManyWave& w, int d_max, cudaStream_t s) {
   if (w.groups <= 0 || w.groups > 65535) return w.groups == 0 ? cudaSuccess : cudaErrorInvalidValue;
   const dim3 gbit = grid_for(w.max_bits, w.groups);
-  const int kRows = d_max <= 8 ? 2 : 1;
+  const int kRows = d_max > 0 && d_max <= 8 ? 2 : 1;
   const dim3 gchk = grid_for((w.max_rows + kRows - 1) / kRows, w.groups);
   cudaError_t e = launch_pdl(h2_bit_many, gbit, dim3(kWarps * 32), s, m, -1, w.q0);
   for (int it = 0; e == cudaSuccess && it < w.iterations; ++it) {
-    if (d_max <= 8) e = launch_pdl(h2_check_many<8>, gchk, dim3(kWarps * 32), s, m, it, w.q0);
+    if (d_max <= 0) e = launch_pdl(h2_check_many<0>, gchk, dim3(kWarps * 32), s, m, it, w.q0);
+    else if (d_max <= 8) e = launch_pdl(h2_check_many<8>, gchk, dim3(kWarps * 32), s, m, it, w.q0);
     else if (d_max <= 16) e = launch_pdl(h2_check_many<16>, gchk, dim3(kWarps * 32), s, m, it, w.q0);
     else e = launch_pdl(h2_check_many<32>, gchk, dim3(kWarps * 32), s, m, it, w.q0);
     if (e == cudaSuccess) e = launch_pdl(h2_bit_many, gbit, dim3(kWarps * 32), s, m, it, w.q0);

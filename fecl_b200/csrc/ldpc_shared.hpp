@@ -45,13 +45,15 @@ class SharedLdpc {
 
   std::vector<SharedLdpcJob> jobs;
 
-  // Plans the launches over `jobs` and carves their tables out of cv.
-  void plan(Carver& cv) {
+  // Plans the launches over `jobs` and carves their tables out of cv: one pass per
+  // check-degree class (split_classes, needed by the persistent form) or one for every
+  // class, its groups in waves of at most wave_bytes of working set.
+  void plan(Carver& cv, bool split_classes = true, int64_t wave_bytes = kWaveBytes) {
     passes_.clear();
     std::map<int, std::vector<int>> by_class;
     for (size_t i = 0; i < jobs.size(); ++i) {
       const int d = jobs[i].c->ldev.d_max;
-      by_class[d <= 8 ? 8 : (d <= 16 ? 16 : 32)].push_back(int(i));
+      by_class[split_classes ? (d <= 8 ? 8 : (d <= 16 ? 16 : 32)) : 0].push_back(int(i));
     }
     for (auto& kv : by_class) {
       for (size_t j0 = 0; j0 < kv.second.size(); j0 += fecl::kMultiMaxCodes) {
@@ -66,7 +68,7 @@ class SharedLdpc {
           const int64_t gb = fecl::ldpc_lanes_h2_group_bytes(s.c->ldev.N, s.c->ldev.E);
           const int groups = int((s.n + 63) / 64);
           for (int g = 0; g < groups; ++g) {
-            if (in_wave > 0 && (bytes + gb > kWaveBytes || in_wave == fecl::kMultiMaxWaveGroups)) {
+            if (in_wave > 0 && (bytes + gb > wave_bytes || in_wave == fecl::kMultiMaxWaveGroups)) {
               ml.wave_ptr.push_back(int32_t(ml.groups.size()));
               bytes = 0;
               in_wave = 0;
@@ -148,21 +150,23 @@ class SharedLdpc {
     for (auto& j : jobs) cuda_check(fecl::launch_ldpc_h2_finish(j.lp, s), "LDPC finish");
   }
 
-  // One line per class.
+  // One line per pass.
   std::string describe(bool persistent) const {
     std::string t;
     for (auto& ml : passes_)
       t += std::string(persistent ? "ldpc shared persistent launch" : "ldpc shared launches per pass") +
-           " (check degree <= " + std::to_string(ml.d_max) + "): " + std::to_string(ml.jobs.size()) + " codes, " +
+           (ml.d_max ? " (check degree <= " + std::to_string(ml.d_max) + "): " : " (every check degree): ") +
+           std::to_string(ml.jobs.size()) + " codes, " +
            std::to_string(ml.groups.size()) + " groups of 64 frames in " + std::to_string(ml.wave_ptr.size() - 1) +
            " waves\n";
     return t;
   }
   bool empty() const { return passes_.empty(); }
 
- private:
   // Waves hold at most this many bytes of working set (the packed decoder's own cap).
   static constexpr int64_t kWaveBytes = 96ll << 20;
+
+ private:
   struct Pass {
     int d_max = 0;
     std::vector<int> jobs;

@@ -7,10 +7,14 @@
 // waiting requests that fit its arena and its frame limit -- requests that arrived
 // while the other slots' batches were on the GPU join the next batch as soon as a
 // slot and its memory free up -- and launches them: every LTE turbo frame of the
-// batch in one persistent mixed-K launch on the slot's stream, the other frames one
-// launch sequence per codec spread over the slot's side streams, so codecs of one
-// batch and batches of different slots overlap on the device.  The same thread harvests finished slots, copies each request's decisions
-// out and stamps its completion time.  Results do not depend on what a request was
+// batch in one persistent mixed-K launch on the slot's stream; the LDPC frames of the
+// packed FP16 decoder, whatever their codes, with one check launch and one bit launch
+// per iteration on a side stream (a batch holds a few frames of many codes, so the
+// number of launches, not their work, would otherwise set its time); any other
+// frames one launch sequence per codec on the other side streams.  Codecs of one
+// batch and batches of different slots overlap on the device.  The same thread
+// harvests finished slots, copies each request's decisions out and stamps its
+// completion time.  Results do not depend on what a request was
 // batched with: every kernel decodes each frame independently of the others.
 #include <cuda_runtime.h>
 
@@ -29,6 +33,7 @@
 #include <vector>
 
 #include "codec.hpp"
+#include "ldpc_shared.hpp"
 
 namespace {
 
@@ -144,7 +149,14 @@ struct Group {
   std::vector<Request*> reqs;
   size_t llr_off = 0, msg_off = 0, it_off = 0, scratch_off = 0;
   ScratchPlan sp;
+  bool shared = false;  // in the shared persistent LDPC launch
 };
+
+char* base_of(Slot& s) { return s.arena.as<char>(); }
+
+// Arena bytes set aside for the tables of the shared LDPC launches (a few KB for the
+// codes and groups a batch can hold).
+constexpr size_t kSharedTableSlack = size_t(256) << 10;
 
 // Admission accounting of a forming batch: an upper bound of the arena bytes, kept
 // up to date request by request.
@@ -164,7 +176,7 @@ struct Admission {
     const uint64_t lf = lte_frames + (r.lte ? r.n : 0);
     // per group three I/O regions (rounded), descriptors and counters for up to three algorithms
     return io + 3 * 256 * (frames.size() + 1) + al256(r.in_bytes) + al256(r.n * r.c->msg()) + al256(r.n * 4) + sc + lte +
-           al256(lf * sizeof(fecl::TurboLteBatchFrame)) * 2 + 3 * 256;
+           al256(lf * sizeof(fecl::TurboLteBatchFrame)) * 2 + 3 * 256 + kSharedTableSlack;
   }
   void add(const Request& r) {
     const auto key = std::make_pair(r.c, r.dtype);
@@ -226,12 +238,31 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
     }
   }
   const size_t out_end = cv.off;
+  // LDPC groups that take the packed FP16 decoder share their launches (per iteration
+  // one check and one bit launch over all of them); the others get their own decoder
+  SharedLdpc shared;
   for (auto& kv : groups) {
     Group& g = kv.second;
     if (g.lte) continue;
+    if (SharedLdpc::eligible(g.c)) {
+      g.shared = true;
+      SharedLdpcJob j;
+      j.c = g.c;
+      j.n = g.n;
+      j.llr = base_of(s) + g.llr_off;
+      j.dtype = g.dtype;
+      j.msg = reinterpret_cast<uint8_t*>(base_of(s) + g.msg_off);
+      j.iters = reinterpret_cast<int32_t*>(base_of(s) + g.it_off);
+      j.scratch_off = cv.take(SharedLdpc::scratch_bytes(j));
+      shared.jobs.push_back(j);
+      continue;
+    }
     g.sp = plan_scratch(g.c, g.n, false);
     g.scratch_off = cv.take(g.sp.bytes);
   }
+  // one pass over every check-degree class and one wave: a server batch holds a few
+  // frames of many codes, and its launches, not its memory traffic, set its time
+  shared.plan(cv, false, INT64_MAX);
   char* base = s.arena.as<char>();
   std::map<int, std::vector<fecl::TurboLteBatchFrame>> tdesc;
   for (auto& kv : groups) {
@@ -264,6 +295,11 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
   size_t host_desc = al256(in_end);
   size_t host_end = host_desc;
   for (auto& kv : tdesc) host_end += al256(kv.second.size() * sizeof(fecl::TurboLteBatchFrame));
+  // the shared LDPC tables are staged after the descriptors, at their arena offsets
+  // shifted by host_tab - tables_begin()
+  const size_t tab0 = shared.tables_begin(), tab1 = shared.tables_end();
+  const size_t host_tab = al256(host_end);
+  if (!shared.empty()) host_end = host_tab + (tab1 - tab0);
   s.in.reserve(std::max<size_t>(host_end, 256));
   s.out.reserve(std::max<size_t>(out_end, 256));
   for (auto& r : batch) std::memcpy(s.in.as() + r->llr_off, r->llr, r->in_bytes);
@@ -280,6 +316,11 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
                "copy descriptors");
     host_desc += al256(v.size() * sizeof(v[0]));
   }
+  if (!shared.empty()) {
+    shared.fill(base, s.in.as() + host_tab - tab0);
+    cuda_check(cudaMemcpyAsync(base + tab0, s.in.as() + host_tab, tab1 - tab0, cudaMemcpyHostToDevice, s.stream),
+               "copy LDPC tables");
+  }
 
   // ---- launches: every turbo frame in one mixed-K launch per algorithm, then one
   // launch sequence per other group
@@ -295,12 +336,18 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
   // the other groups on the side streams, forked after the copies in and joined before
   // the copy out, so that groups of different codes run at once
   cuda_check(cudaEventRecord(s.fork, s.stream), "cudaEventRecord");
-  int k = 0;
   bool used[kSideStreams] = {};
+  if (!shared.empty()) {
+    cuda_check(cudaStreamWaitEvent(s.side[0], s.fork, 0), "cudaStreamWaitEvent");
+    used[0] = true;
+    shared.launch(base, s.side[0], false);
+  }
+  const int first = shared.empty() ? 0 : 1;  // side stream 0 holds the shared launches
+  int k = 0;
   for (auto& kv : groups) {
     Group& g = kv.second;
-    if (g.lte) continue;
-    const int q = k++ % kSideStreams;
+    if (g.lte || g.shared) continue;
+    const int q = first + k++ % (kSideStreams - first);
     if (!used[q]) cuda_check(cudaStreamWaitEvent(s.side[q], s.fork, 0), "cudaStreamWaitEvent");
     used[q] = true;
     Launch d;
