@@ -7,12 +7,10 @@
 // waiting requests that fit its arena and its frame limit -- requests that arrived
 // while the other slots' batches were on the GPU join the next batch as soon as a
 // slot and its memory free up -- and launches them: every LTE turbo frame of the
-// batch in one persistent mixed-K launch on the slot's stream; the LDPC frames of the
-// packed FP16 decoder, whatever their codes, with one check launch and one bit launch
-// per iteration on a side stream (a batch holds a few frames of many codes, so the
-// number of launches, not their work, would otherwise set its time); any other
-// frames one launch sequence per codec on the other side streams.  Codecs of one
-// batch and batches of different slots overlap on the device.  The same thread
+// batch in one persistent mixed-K launch on the slot's stream, the other frames one
+// launch sequence per codec spread over the slot's side streams (kServerSharedLdpc
+// would give the FP16 LDPC groups shared launches instead), so codecs of one batch
+// and batches of different slots overlap on the device.  The same thread
 // harvests finished slots, copies each request's decisions out and stamps its
 // completion time.  Results do not depend on what a request was
 // batched with: every kernel decodes each frame independently of the others.
@@ -154,6 +152,12 @@ struct Group {
 
 char* base_of(Slot& s) { return s.arena.as<char>(); }
 
+// Whether the FP16 LDPC groups of a batch share their launches (one check and one bit
+// launch per iteration over every code).  Off: measured on Poisson loads of 5k frames/s
+// it tripled the device time of a batch (27 ms against 8.7 ms per ~70 frames), each
+// shared launch being sized for the largest group it serves.
+constexpr bool kServerSharedLdpc = false;
+
 // Arena bytes set aside for the tables of the shared LDPC launches (a few KB for the
 // codes and groups a batch can hold).
 constexpr size_t kSharedTableSlack = size_t(256) << 10;
@@ -244,7 +248,7 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
   for (auto& kv : groups) {
     Group& g = kv.second;
     if (g.lte) continue;
-    if (SharedLdpc::eligible(g.c)) {
+    if (kServerSharedLdpc && SharedLdpc::eligible(g.c)) {
       g.shared = true;
       SharedLdpcJob j;
       j.c = g.c;
