@@ -115,7 +115,7 @@ struct LdpcMultiParams {
   int32_t nwaves = 0;
   unsigned* barrier = nullptr;             // [2] zeroed by the launcher
 };
-void ldpc_lanes_h2_layout(LdpcLanesParams& p, void* scratch);
+void ldpc_lanes_h2_layout(LdpcLanesParams& p, void* scratch, int lanes = 32);
 int64_t ldpc_lanes_h2_group_bytes(int64_t N, int64_t E);
 cudaError_t launch_ldpc_h2_stage(const LdpcLanesParams& p, cudaStream_t s);
 cudaError_t launch_ldpc_h2_finish(const LdpcLanesParams& p, cudaStream_t s);

@@ -17,6 +17,14 @@
 // Ties are exact: two equal minima give m2 == m1.  The syndrome stop, the retirement
 // of frames and the waves are those of ldpc_lanes.cu, with a pair of lane masks per
 // group (.x frames, .y frames).
+//
+// Narrow groups.  The per-pass kernels also take groups of W = 2, 4, 8 or 16 lanes
+// (2 W frames):
+// chan / app [g][n][W] and c2v [g][e][W], a warp serving 32 / W rows (or bits) of its
+// group at once, lane l on row (or bit) l / W and frame pair l % W.  A batch of a few
+// frames then runs as many warps per pass as its frames need (one frame of a 64800-bit
+// code: 64800 / 16 warps per bit pass with W = 2, against 64800 with W = 32), with the
+// same arithmetic per frame, so the results do not depend on W.
 #include <cuda_fp16.h>
 #include <math.h>
 
@@ -56,21 +64,21 @@ struct Row {
   unsigned px, py;  // parity of the hard decisions of the previous APP
 };
 
-template <int DMAX>
-__device__ __forceinline__ void load_row(const LdpcLanesParams& p, int g, int r, int lane, Row<DMAX>& w) {
+template <int DMAX, int W = kLanes>
+__device__ __forceinline__ void load_row(const LdpcLanesParams& p, int g, int r, int sub, Row<DMAX>& w) {
   const __half2* c2v = static_cast<const __half2*>(p.c2v);
   const float2* app = reinterpret_cast<const float2*>(p.app);
   w.e0 = __ldg(p.row_ptr + r);
   w.d = int(__ldg(p.row_ptr + r + 1) - w.e0);
-  const __half2* cg = c2v + (int64_t(g) * p.E + w.e0) * kLanes + lane;
-  const float2* ag = app + int64_t(g) * p.N * kLanes + lane;
+  const __half2* cg = c2v + (int64_t(g) * p.E + w.e0) * W + sub;
+  const float2* ag = app + int64_t(g) * p.N * W + sub;
   w.px = w.py = 0;
 #pragma unroll
   for (int j = 0; j < DMAX; ++j) {
     if (j < w.d) {
       const uint32_t col = __ldg(p.col_idx + w.e0 + j);
-      const float2 a = ag[int64_t(col) * kLanes];
-      const float2 c = __half22float2(cg[j * kLanes]);
+      const float2 a = ag[int64_t(col) * W];
+      const float2 c = __half22float2(cg[j * W]);
       w.px ^= unsigned(a.x >= 0.0f);
       w.py ^= unsigned(a.y >= 0.0f);
       // a - c in FP32, rounded to FP16 and kept finite (saturated at +-65504)
@@ -79,8 +87,8 @@ __device__ __forceinline__ void load_row(const LdpcLanesParams& p, int g, int r,
   }
 }
 
-template <int DMAX>
-__device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, int lane, const Row<DMAX>& w, __half2 sf2,
+template <int DMAX, int W = kLanes>
+__device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, int sub, const Row<DMAX>& w, __half2 sf2,
                                           bool mine_x, bool mine_y, bool keep_all) {
   __half2* c2v = static_cast<__half2*>(p.c2v);
   const __half2 inf2 = __floats2half2_rn(INFINITY, INFINITY);
@@ -101,7 +109,7 @@ __device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, int l
   // which are sums of these messages, are wanted; a hard-decision decode reads only
   // the a-posteriori values, which the bit pass freezes for retired frames.
   const uint32_t keep = keep_all ? (mine_x ? 0u : 0x0000ffffu) | (mine_y ? 0u : 0xffff0000u) : 0u;
-  __half2* cg = c2v + (int64_t(g) * p.E + w.e0) * kLanes + lane;
+  __half2* cg = c2v + (int64_t(g) * p.E + w.e0) * W + sub;
   // The scaling is applied to the two magnitudes once per row: rounding to nearest is
   // symmetric, so (-m) * s is -(m * s) bit for bit and the edge's sign can be xored
   // into the scaled magnitude.
@@ -116,10 +124,10 @@ __device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, int l
         const uint32_t eq = __heq2_mask(__habs2(w.v[j]), m1);
         const __half2 out = from_bits(((b2 & eq) | (b1 & ~eq)) ^ (bits(w.v[j]) & kSigns));
         if (keep == 0u) {
-          cg[j * kLanes] = out;
+          cg[j * W] = out;
         } else if (keep != 0xffffffffu) {
-          const uint32_t old = bits(cg[j * kLanes]);
-          cg[j * kLanes] = from_bits((bits(out) & ~keep) | (old & keep));
+          const uint32_t old = bits(cg[j * W]);
+          cg[j * W] = from_bits((bits(out) & ~keep) | (old & keep));
         }
       }
     }
@@ -134,57 +142,73 @@ __device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, int l
       const uint32_t sign = (sg ^ bits(w.v[j])) & kSigns;
       const __half2 out = from_bits(mag ^ sign);
       if (keep == 0u) {
-        cg[j * kLanes] = out;
+        cg[j * W] = out;
       } else if (keep != 0xffffffffu) {
-        const uint32_t old = bits(cg[j * kLanes]);
-        cg[j * kLanes] = from_bits((bits(out) & ~keep) | (old & keep));
+        const uint32_t old = bits(cg[j * W]);
+        cg[j * W] = from_bits((bits(out) & ~keep) | (old & keep));
       }
     }
   }
 }
 
+// The lanes of a W-lane group whose bit is set in a warp ballot (lane l standing for
+// frame pair l % W).
+template <int W>
+__device__ __forceinline__ uint32_t fold_lanes(uint32_t b) {
+  if constexpr (W == 32) {
+    return b;
+  } else {
+#pragma unroll
+    for (int s = W; s < 32; s *= 2) b |= b >> s;
+    return b & ((1u << W) - 1u);
+  }
+}
+
 // Rows r .. r + kRows - 1 of group g at iteration `it` (kRows = 2 for rows of degree
-// <= 8): the row updates; bx / by collect the lanes whose syndrome bit is set.
-template <int DMAX>
-__device__ __forceinline__ void check_rows(const LdpcLanesParams& p, int it, int g, int r, int lane, bool mx, bool my,
+// <= 8; r is this lane's, rows past the last are skipped): the row updates; bx / by
+// collect the lanes whose syndrome bit is set.  Every lane of the warp calls it.
+template <int DMAX, int W = kLanes>
+__device__ __forceinline__ void check_rows(const LdpcLanesParams& p, int it, int g, int r, int sub, bool mx, bool my,
                                            bool keep_all, bool check_syndrome, uint32_t& bx, uint32_t& by) {
   constexpr int kRows = DMAX <= 8 ? 2 : 1;
   Row<DMAX> w[kRows];
 #pragma unroll
   for (int q = 0; q < kRows; ++q) {
     w[q].d = 0;
-    if (r + q < p.M) load_row<DMAX>(p, g, r + q, lane, w[q]);
+    if (r + q < p.M) load_row<DMAX, W>(p, g, r + q, sub, w[q]);
   }
 #pragma unroll
   for (int q = 0; q < kRows; ++q) {
+    if (check_syndrome) {
+      bx |= fold_lanes<W>(__ballot_sync(0xffffffffu, w[q].d > 0 && w[q].px != 0));
+      by |= fold_lanes<W>(__ballot_sync(0xffffffffu, w[q].d > 0 && w[q].py != 0));
+    }
     if (w[q].d > 0) {
-      if (check_syndrome) {
-        bx |= __ballot_sync(0xffffffffu, w[q].px != 0);
-        by |= __ballot_sync(0xffffffffu, w[q].py != 0);
-      }
       // the scaling of rows of this degree (constant across iterations on this path)
       const float s = p.sf[size_t(it % p.n_sf) * p.sf_stride + (w[q].d >= 2 ? w[q].d - 2 : 0)];
-      store_row<DMAX>(p, g, lane, w[q], __float2half2_rn(s), mx, my, keep_all);
+      store_row<DMAX, W>(p, g, sub, w[q], __float2half2_rn(s), mx, my, keep_all);
     }
   }
 }
 
-template <int DMAX>
+template <int DMAX, int W>
 __global__ void __launch_bounds__(kWarps * 32) h2_check(LdpcLanesParams p, int it, int g0) {
   pdl_enter();
   constexpr int kRows = DMAX <= 8 ? 2 : 1;
+  constexpr int kSlots = 32 / W;  // rows (or row pairs) per warp step
   const int lane = threadIdx.x & 31;
+  const int sub = lane % W, slot = lane / W;
   const int warps = int(gridDim.x) * kWarps;
   const bool check_syndrome = it > 0 && !p.fixed_iterations;
   const int g = g0 + int(blockIdx.y);
   const uint32_t ax = active_of(p, it)[2 * g], ay = active_of(p, it)[2 * g + 1];
   if ((ax | ay) == 0) return;
-  const bool mx = (ax >> lane) & 1, my = (ay >> lane) & 1;
+  const bool mx = (ax >> sub) & 1, my = (ay >> sub) & 1;
   const bool keep_all = p.msg_out || p.syst_out || p.parity_out || p.state_out;
   uint32_t bx = 0, by = 0;
   const int w0 = int(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-  for (int r = w0 * kRows; r < p.M; r += warps * kRows)
-    check_rows<DMAX>(p, it, g, r, lane, mx, my, keep_all, check_syndrome, bx, by);
+  for (int r = w0 * kSlots * kRows; r < p.M; r += warps * kSlots * kRows)
+    check_rows<DMAX, W>(p, it, g, r + slot * kRows, sub, mx, my, keep_all, check_syndrome, bx, by);
   bx &= ax;
   by &= ay;
   if (lane == 0) {
@@ -195,12 +219,13 @@ __global__ void __launch_bounds__(kWarps * 32) h2_check(LdpcLanesParams p, int i
 
 // Retirement of the .x (h = 0) or .y (h = 1) frames of group g after the check pass of
 // iteration `it`, and their masks for iteration it + 1.
+template <int W = kLanes>
 __device__ __forceinline__ void retire_half(const LdpcLanesParams& p, int it, int g, int h) {
   const uint32_t a = active_of(p, it)[2 * g + h];
   uint32_t done = 0;
   if (it == p.iterations - 1) done = a;
   else if (it > 0 && !p.fixed_iterations) done = a & ~fail_of(p, it)[2 * g + h];
-  for (uint32_t m = done; m; m &= m - 1) p.iters_ws[int64_t(g) * 64 + h * 32 + (__ffs(m) - 1)] = it + 1;
+  for (uint32_t m = done; m; m &= m - 1) p.iters_ws[int64_t(g) * 2 * W + h * W + (__ffs(m) - 1)] = it + 1;
   active_of(p, it + 1)[2 * g + h] = a & ~done;
   fail_of(p, it + 1)[2 * g + h] = 0;
 }
@@ -209,12 +234,13 @@ __device__ __forceinline__ void retire_half(const LdpcLanesParams& p, int it, in
 // frames; a retired frame's value stays.  The edges go in runs of 8 (one run for most
 // bits): every edge id of a run is loaded, then every message, then they are added in
 // order, so a bit costs three dependent loads rather than two per edge.
-__device__ __forceinline__ void bit_one(const LdpcLanesParams& p, int g, int b, int lane, bool mx, bool my) {
+template <int W = kLanes>
+__device__ __forceinline__ void bit_one(const LdpcLanesParams& p, int g, int b, int sub, bool mx, bool my) {
   constexpr uint32_t kRun = 8;
-  const __half2* cg = static_cast<const __half2*>(p.c2v) + int64_t(g) * p.E * kLanes + lane;
+  const __half2* cg = static_cast<const __half2*>(p.c2v) + int64_t(g) * p.E * W + sub;
   const float2* chan = reinterpret_cast<const float2*>(p.chan);
   float2* app = reinterpret_cast<float2*>(p.app);
-  const int64_t base = (int64_t(g) * p.N + b) * kLanes + lane;
+  const int64_t base = (int64_t(g) * p.N + b) * W + sub;
   const uint32_t k0 = __ldg(p.col_ptr + b), k1 = __ldg(p.col_ptr + b + 1);
   float2 acc = chan[base];
   for (uint32_t k = k0; k < k1; k += kRun) {
@@ -223,7 +249,7 @@ __device__ __forceinline__ void bit_one(const LdpcLanesParams& p, int g, int b, 
 #pragma unroll
     for (uint32_t j = 0; j < kRun; ++j) e[j] = k + j < k1 ? __ldg(p.col_edges + k + j) : 0u;
 #pragma unroll
-    for (uint32_t j = 0; j < kRun; ++j) x[j] = k + j < k1 ? cg[int64_t(e[j]) * kLanes] : __half2{};
+    for (uint32_t j = 0; j < kRun; ++j) x[j] = k + j < k1 ? cg[int64_t(e[j]) * W] : __half2{};
 #pragma unroll
     for (uint32_t j = 0; j < kRun; ++j)
       if (k + j < k1) acc = __fadd2_rn(acc, __half22float2(x[j]));
@@ -240,17 +266,21 @@ __device__ __forceinline__ void bit_one(const LdpcLanesParams& p, int g, int b, 
 
 // Bit pass; with it < 0 the initial APP for every lane.  Block (0, y) retires frames
 // and writes the group's masks for iteration it + 1.
+template <int W>
 __global__ void __launch_bounds__(kWarps * 32) h2_bit(LdpcLanesParams p, int it, int g0) {
   pdl_enter();
+  constexpr int kSlots = 32 / W;
   const int lane = threadIdx.x & 31;
+  const int sub = lane % W, slot = lane / W;
   const int warps = int(gridDim.x) * kWarps;
   const int g = g0 + int(blockIdx.y);
   const uint32_t ax = it < 0 ? 0xffffffffu : active_of(p, it)[2 * g];
   const uint32_t ay = it < 0 ? 0xffffffffu : active_of(p, it)[2 * g + 1];
-  if (it >= 0 && blockIdx.x == 0 && threadIdx.x < 2) retire_half(p, it, g, threadIdx.x);
-  const bool mx = (ax >> lane) & 1, my = (ay >> lane) & 1;
+  if (it >= 0 && blockIdx.x == 0 && threadIdx.x < 2) retire_half<W>(p, it, g, threadIdx.x);
+  const bool mx = (ax >> sub) & 1, my = (ay >> sub) & 1;
   if (!mx && !my) return;
-  for (int b = int(blockIdx.x) * kWarps + (threadIdx.x >> 5); b < p.N; b += warps) bit_one(p, g, b, lane, mx, my);
+  for (int b = (int(blockIdx.x) * kWarps + (threadIdx.x >> 5)) * kSlots + slot; b < p.N; b += warps * kSlots)
+    bit_one<W>(p, g, b, sub, mx, my);
 }
 
 // Persistent decoder for a small batch (at most kPersistGroups groups of 64 frames,
@@ -411,35 +441,38 @@ __global__ void __launch_bounds__(kWarps * 32, DMAX <= 16 ? 3 : 2) h2_multi(Ldpc
       for (int i = threadIdx.x; i < s_codes[c].groups * 64; i += blockDim.x) s_codes[c].iters_ws[i] = -1;
 }
 
-// Frame f of group g sits in lane f % 32, half (f / 32) % 2.
-__device__ __forceinline__ int64_t frame_of(int g, int lane, int h) { return int64_t(g) * 64 + h * 32 + lane; }
+// Frame f of a W-lane group g sits in lane f % W, half (f / W) % 2.
+template <int W>
+__device__ __forceinline__ int64_t frame_of(int g, int sub, int h) { return int64_t(g) * 2 * W + h * W + sub; }
 
+template <int W>
 __global__ void h2_stage(LdpcLanesParams p) {
   float2* chan = reinterpret_cast<float2*>(p.chan);
   __half2* c2v = static_cast<__half2*>(p.c2v);
   const int g = int(blockIdx.y);
   const int stride = int(gridDim.x) * blockDim.x;
   const int t0 = int(blockIdx.x) * blockDim.x + threadIdx.x;
-  for (int i = t0; i < p.N * kLanes; i += stride) {
-    const int lane = i % kLanes, b = i / kLanes;
+  for (int i = t0; i < p.N * W; i += stride) {
+    const int sub = i % W, b = i / W;
     float v[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int64_t f = frame_of(g, lane, h);
+      const int64_t f = frame_of<W>(g, sub, h);
       v[h] = 0.0f;
       if (f < p.nframes) {
         v[h] = load_llr(p.llr, p.llr_dtype, f * p.N + b);
         if (p.syst_in && b < p.msg) v[h] += load_llr(p.syst_in, p.llr_dtype, f * p.msg + b);
       }
     }
-    chan[int64_t(g) * p.N * kLanes + i] = make_float2(v[0], v[1]);
+    chan[int64_t(g) * p.N * W + i] = make_float2(v[0], v[1]);
   }
-  for (int64_t i = t0; i < p.E * kLanes; i += stride) c2v[int64_t(g) * p.E * kLanes + i] = __floats2half2_rn(0.0f, 0.0f);
+  for (int64_t i = t0; i < p.E * W; i += stride) c2v[int64_t(g) * p.E * W + i] = __floats2half2_rn(0.0f, 0.0f);
   if (t0 == 0) {
+    constexpr uint32_t kAll = W == 32 ? 0xffffffffu : (1u << W) - 1u;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int64_t left = p.nframes - int64_t(g) * 64 - h * 32;
-      p.active[2 * g + h] = left >= 32 ? 0xffffffffu : (left > 0 ? ((1u << left) - 1u) : 0u);
+      const int64_t left = p.nframes - int64_t(g) * 2 * W - h * W;
+      p.active[2 * g + h] = left >= W ? kAll : (left > 0 ? ((1u << left) - 1u) : 0u);
       p.active[2 * p.groups + 2 * g + h] = 0;
       p.fail[2 * g + h] = 0;
       p.fail[2 * p.groups + 2 * g + h] = 0;
@@ -447,6 +480,7 @@ __global__ void h2_stage(LdpcLanesParams p) {
   }
 }
 
+template <int W>
 __global__ void h2_finish(LdpcLanesParams p) {
   const float2* chan = reinterpret_cast<const float2*>(p.chan);
   const float2* app = reinterpret_cast<const float2*>(p.app);
@@ -455,19 +489,19 @@ __global__ void h2_finish(LdpcLanesParams p) {
   const int stride = int(gridDim.x) * blockDim.x;
   const int t0 = int(blockIdx.x) * blockDim.x + threadIdx.x;
   const bool soft = p.msg_out || p.syst_out || p.parity_out;
-  const __half2* cg = c2v + int64_t(g) * p.E * kLanes;
-  for (int i = t0; i < p.N * kLanes; i += stride) {
-    const int lane = i % kLanes, b = i / kLanes;
-    const int64_t at = int64_t(g) * p.N * kLanes + i;
+  const __half2* cg = c2v + int64_t(g) * p.E * W;
+  for (int i = t0; i < p.N * W; i += stride) {
+    const int sub = i % W, b = i / W;
+    const int64_t at = int64_t(g) * p.N * W + i;
     const float2 a = app[at];
     float2 ext = make_float2(0.0f, 0.0f);
     if (soft)
       for (uint32_t k = __ldg(p.col_ptr + b); k < __ldg(p.col_ptr + b + 1); ++k)
-        ext = __fadd2_rn(ext, __half22float2(cg[int64_t(__ldg(p.col_edges + k)) * kLanes + lane]));
+        ext = __fadd2_rn(ext, __half22float2(cg[int64_t(__ldg(p.col_edges + k)) * W + sub]));
     const float2 ch = chan[at];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int64_t f = frame_of(g, lane, h);
+      const int64_t f = frame_of<W>(g, sub, h);
       if (f >= p.nframes) continue;
       const float av = h ? a.y : a.x, ev = h ? ext.y : ext.x, cv = h ? ch.y : ch.x;
       if (p.hard && b < p.msg) p.hard[f * p.msg + b] = uint8_t(av >= 0.0f);
@@ -481,19 +515,19 @@ __global__ void h2_finish(LdpcLanesParams p) {
     }
   }
   if (p.state_out) {
-    for (int64_t i = t0; i < p.E * kLanes; i += stride) {
-      const int lane = int(i % kLanes);
-      const int64_t e = i / kLanes;
+    for (int64_t i = t0; i < p.E * W; i += stride) {
+      const int sub = int(i % W);
+      const int64_t e = i / W;
       const float2 c = __half22float2(cg[i]);
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int64_t f = frame_of(g, lane, h);
+        const int64_t f = frame_of<W>(g, sub, h);
         if (f < p.nframes) store_llr(p.state_out, p.out_dtype, f * p.E + e, h ? c.y : c.x);
       }
     }
   }
-  if (p.iters && t0 < 64) {
-    const int64_t f = int64_t(g) * 64 + t0;
+  if (p.iters && t0 < 2 * W) {
+    const int64_t f = int64_t(g) * 2 * W + t0;
     if (f < p.nframes) p.iters[f] = p.iters_ws[f];
   }
 }
@@ -618,17 +652,27 @@ cudaError_t launch_persistent(LdpcLanesParams p, cudaStream_t s) {
   return ldpc_persist_launch(s, reinterpret_cast<const void*>(kern), unsigned(blocks), kWarps * 32, args);
 }
 
-template <int DMAX>
+// The grid of the staging and finishing kernels: 256 threads per block over the
+// larger of a group's bit and edge slots, at most about eight blocks per SM in all.
+dim3 stage_grid(const LdpcLanesParams& p, int W) {
+  const int64_t need = ((p.N > p.E ? int64_t(p.N) : p.E) * W + 255) / 256;
+  const int64_t share = (148 * 8 + p.groups - 1) / p.groups;
+  const int64_t x = need < share ? need : share;
+  return dim3(unsigned(x > 0 ? x : 1), unsigned(p.groups));
+}
+
+template <int DMAX, int W>
 cudaError_t run(const LdpcLanesParams& p, cudaStream_t s) {
   if (p.groups > 65535) return cudaErrorInvalidValue;
-  const int64_t gb = int64_t(kLanes) * (2 * 8 * int64_t(p.N) + 4 * p.E);
+  constexpr int kSlots = 32 / W;
+  const int64_t gb = int64_t(W) * (2 * 8 * int64_t(p.N) + 4 * p.E);
   int64_t wave = p.wave_groups > 0 ? p.wave_groups : kWaveCap / gb;
   if (wave < 1) wave = 1;
   if (wave > p.groups) wave = p.groups;
-  const dim3 gs((148 * 8 + p.groups - 1) / p.groups, p.groups);
-  h2_stage<<<gs, 256, 0, s>>>(p);
+  const dim3 gs = stage_grid(p, W);
+  h2_stage<W><<<gs, 256, 0, s>>>(p);
   bool done = false;
-  if (use_persistent(p, wave, s)) {
+  if (W == kLanes && use_persistent(p, wave, s)) {
     const cudaError_t e = launch_persistent<DMAX>(p, s);
     if (e == cudaSuccess) done = true;
     else if (e != cudaErrorCooperativeLaunchTooLarge && e != cudaErrorNotSupported && e != cudaErrorInvalidConfiguration)
@@ -637,17 +681,29 @@ cudaError_t run(const LdpcLanesParams& p, cudaStream_t s) {
   }
   for (int w0 = 0; !done && w0 < p.groups; w0 += int(wave)) {
     const int nw = p.groups - w0 < wave ? p.groups - w0 : int(wave);
-    const dim3 gbit = grid_for(p.N, nw);
-    const dim3 gchk = grid_for((p.M + (DMAX <= 8 ? 1 : 0)) / (DMAX <= 8 ? 2 : 1), nw);
-    cudaError_t e = launch_pdl(h2_bit, gbit, dim3(kWarps * 32), s, p, -1, w0);
+    constexpr int kRows = DMAX <= 8 ? 2 : 1;
+    const dim3 gbit = grid_for((p.N + kSlots - 1) / kSlots, nw);
+    const dim3 gchk = grid_for((p.M + kRows * kSlots - 1) / (kRows * kSlots), nw);
+    cudaError_t e = launch_pdl(h2_bit<W>, gbit, dim3(kWarps * 32), s, p, -1, w0);
     for (int it = 0; e == cudaSuccess && it < p.iterations; ++it) {
-      e = launch_pdl(h2_check<DMAX>, gchk, dim3(kWarps * 32), s, p, it, w0);
-      if (e == cudaSuccess) e = launch_pdl(h2_bit, gbit, dim3(kWarps * 32), s, p, it, w0);
+      e = launch_pdl(h2_check<DMAX, W>, gchk, dim3(kWarps * 32), s, p, it, w0);
+      if (e == cudaSuccess) e = launch_pdl(h2_bit<W>, gbit, dim3(kWarps * 32), s, p, it, w0);
     }
     if (e != cudaSuccess) return e;
   }
-  h2_finish<<<gs, 256, 0, s>>>(p);
+  h2_finish<W><<<gs, 256, 0, s>>>(p);
   return cudaGetLastError();
+}
+
+template <int DMAX>
+cudaError_t run_width(const LdpcLanesParams& p, int W, cudaStream_t s) {
+  switch (W) {
+    case 2: return run<DMAX, 2>(p, s);
+    case 4: return run<DMAX, 4>(p, s);
+    case 8: return run<DMAX, 8>(p, s);
+    case 16: return run<DMAX, 16>(p, s);
+    default: return run<DMAX, kLanes>(p, s);
+  }
 }
 
 template <int DMAX>
@@ -698,35 +754,44 @@ size_t ldpc_lanes_h2_scratch_bytes(int64_t N, int64_t E, int64_t nframes) {
          al(size_t(groups) * 64 * 4) + al(2 * sizeof(unsigned));
 }
 
-void ldpc_lanes_h2_layout(LdpcLanesParams& p, void* scratch) {
-  p.groups = int32_t((p.nframes + 63) / 64);
+void ldpc_lanes_h2_layout(LdpcLanesParams& p, void* scratch, int W) {
+  p.groups = int32_t((p.nframes + 2 * W - 1) / (2 * W));
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   char* q = static_cast<char*>(scratch);
   p.chan = reinterpret_cast<float*>(q);
-  q += al(size_t(p.groups) * p.N * kLanes * 8);
+  q += al(size_t(p.groups) * p.N * W * 8);
   p.app = reinterpret_cast<float*>(q);
-  q += al(size_t(p.groups) * p.N * kLanes * 8);
+  q += al(size_t(p.groups) * p.N * W * 8);
   p.c2v = q;
-  q += al(size_t(p.groups) * p.E * kLanes * 4);
+  q += al(size_t(p.groups) * p.E * W * 4);
   p.active = reinterpret_cast<uint32_t*>(q);  // [2][groups][2]
   p.fail = p.active + 4 * p.groups;          // [2][groups][2]
   q += al(size_t(p.groups) * 32);
   p.iters_ws = reinterpret_cast<int32_t*>(q);
-  q += al(size_t(p.groups) * 64 * 4);
+  q += al(size_t(p.groups) * 2 * W * 4);
   p.barrier = reinterpret_cast<unsigned*>(q);
+}
+
+// Lanes per group for a batch of n frames: the narrowest power of two from 2 to 32
+// whose group (2 W frames) holds the batch, so that a batch of a few frames runs few
+// idle lanes; batches of more than 64 frames take full groups of 32.
+int ldpc_lanes_h2_width(int64_t nframes) {
+  int W = 2;
+  while (W < kLanes && 2 * W < nframes) W *= 2;
+  return W;
 }
 
 int64_t ldpc_lanes_h2_group_bytes(int64_t N, int64_t E) { return int64_t(kLanes) * (2 * 8 * N + 4 * E); }
 
 cudaError_t launch_ldpc_h2_stage(const LdpcLanesParams& p, cudaStream_t s) {
   if (p.groups <= 0) return cudaSuccess;
-  h2_stage<<<dim3((148 * 8 + p.groups - 1) / p.groups, p.groups), 256, 0, s>>>(p);
+  h2_stage<kLanes><<<dim3((148 * 8 + p.groups - 1) / p.groups, p.groups), 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ldpc_h2_finish(const LdpcLanesParams& p, cudaStream_t s) {
   if (p.groups <= 0) return cudaSuccess;
-  h2_finish<<<dim3((148 * 8 + p.groups - 1) / p.groups, p.groups), 256, 0, s>>>(p);
+  h2_finish<kLanes><<<dim3((148 * 8 + p.groups - 1) / p.groups, p.groups), 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 
@@ -758,10 +823,11 @@ cudaError_t launch_ldpc_h2_multi(LdpcMultiParams m, int d_max, cudaStream_t s) {
 cudaError_t launch_ldpc_lanes_h2(LdpcLanesParams p, void* scratch, cudaStream_t s) {
   if (p.nframes <= 0) return cudaSuccess;
   if (p.state_in || p.algorithm != 2) return cudaErrorInvalidValue;
-  ldpc_lanes_h2_layout(p, scratch);
-  if (p.d_max <= 8) return run<8>(p, s);
-  if (p.d_max <= 16) return run<16>(p, s);
-  if (p.d_max <= 32) return run<32>(p, s);
+  const int W = ldpc_lanes_h2_width(p.nframes);
+  ldpc_lanes_h2_layout(p, scratch, W);
+  if (p.d_max <= 8) return run_width<8>(p, W, s);
+  if (p.d_max <= 16) return run_width<16>(p, W, s);
+  if (p.d_max <= 32) return run_width<32>(p, W, s);
   return cudaErrorInvalidValue;
 }
 

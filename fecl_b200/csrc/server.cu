@@ -57,6 +57,9 @@ int guarded(F&& f) {
 
 using Clock = std::chrono::steady_clock;
 
+// Pinned staging memory of a slot.  It grows at least twofold when a batch needs more:
+// cudaFreeHost waits for the whole device, so every regrowth stalls the batches of the
+// other slots, and a load that ramps up must not pay that once per batch.
 struct PinnedBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;
@@ -65,6 +68,7 @@ struct PinnedBuffer {
   }
   void reserve(size_t n) {
     if (n <= bytes) return;
+    n = std::max(n, 2 * bytes);
     if (ptr) cudaFreeHost(ptr);
     ptr = nullptr;
     bytes = 0;
@@ -91,7 +95,11 @@ struct Request {
   size_t llr_off = 0, msg_off = 0, it_off = 0;
 };
 
-constexpr int kSideStreams = 4;  // per slot: codec groups of a batch run on these at once
+constexpr int kSideStreams = 8;  // per slot: codec groups of a batch run on these at once
+// Pinned staging reserved per slot at creation: the L-values (and turbo descriptors)
+// of a few hundred frames, and their decisions.
+constexpr size_t kInitialStagingIn = size_t(32) << 20;
+constexpr size_t kInitialStagingOut = size_t(4) << 20;
 
 struct Slot {
   cudaStream_t stream = nullptr;
@@ -101,6 +109,7 @@ struct Slot {
   cudaEvent_t start = nullptr;  // timing: the batch's first operation
   DeviceBuffer arena;
   PinnedBuffer in, out;
+  size_t out_begin = 0;  // arena offset of out's first byte
   std::vector<std::shared_ptr<Request>> reqs;
   bool busy = false;
 };
@@ -305,7 +314,8 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
   const size_t host_tab = al256(host_end);
   if (!shared.empty()) host_end = host_tab + (tab1 - tab0);
   s.in.reserve(std::max<size_t>(host_end, 256));
-  s.out.reserve(std::max<size_t>(out_end, 256));
+  s.out.reserve(std::max<size_t>(out_end - out_begin, 256));  // holds [out_begin, out_end)
+  s.out_begin = out_begin;
   for (auto& r : batch) std::memcpy(s.in.as() + r->llr_off, r->llr, r->in_bytes);
   cuda_check(cudaEventRecord(s.start, s.stream), "cudaEventRecord");
   cuda_check(cudaMemcpyAsync(base, s.in.as(), in_end, cudaMemcpyHostToDevice, s.stream), "copy in");
@@ -326,8 +336,12 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
                "copy LDPC tables");
   }
 
-  // ---- launches: every turbo frame in one mixed-K launch per algorithm, then one
-  // launch sequence per other group
+  // ---- launches: every turbo frame in one mixed-K launch per algorithm on the slot's
+  // stream, one launch sequence per other group on the side streams, forked after the
+  // copies in (before the turbo launch, which the LDPC decoders need not wait for) and
+  // joined before the copy out, so that the turbo frames and groups of different codes
+  // run at once
+  cuda_check(cudaEventRecord(s.fork, s.stream), "cudaEventRecord");
   for (auto& kv : tdesc) {
     fecl::TurboLteBatchParams p;
     p.frames = reinterpret_cast<const fecl::TurboLteBatchFrame*>(base + tdev_off[kv.first].first);
@@ -337,9 +351,6 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
     p.algorithm = kv.first;
     cuda_check(fecl::launch_turbo_lte_batch(p, s.stream), "turbo batch launch");
   }
-  // the other groups on the side streams, forked after the copies in and joined before
-  // the copy out, so that groups of different codes run at once
-  cuda_check(cudaEventRecord(s.fork, s.stream), "cudaEventRecord");
   bool used[kSideStreams] = {};
   if (!shared.empty()) {
     cuda_check(cudaStreamWaitEvent(s.side[0], s.fork, 0), "cudaStreamWaitEvent");
@@ -347,11 +358,23 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
     shared.launch(base, s.side[0], false);
   }
   const int first = shared.empty() ? 0 : 1;  // side stream 0 holds the shared launches
-  int k = 0;
-  for (auto& kv : groups) {
-    Group& g = kv.second;
-    if (g.lte || g.shared) continue;
-    const int q = first + k++ % (kSideStreams - first);
+  // longest first, each to the side stream with the least work so far; a group's work
+  // is estimated by its parity bits times its iteration limit times its frame groups
+  std::vector<Group*> order;
+  for (auto& kv : groups)
+    if (!kv.second.lte && !kv.second.shared) order.push_back(&kv.second);
+  auto cost = [](const Group* g) {
+    const double it = g->c->kind == 0 ? double(std::max(1, g->c->ldev.iterations)) : 1.0;
+    return double(g->c->parity()) * it * double((g->n + 63) / 64);
+  };
+  std::stable_sort(order.begin(), order.end(), [&](const Group* a, const Group* b) { return cost(a) > cost(b); });
+  double load[kSideStreams] = {};
+  for (Group* gp : order) {
+    Group& g = *gp;
+    int q = first;
+    for (int i = first + 1; i < kSideStreams; ++i)
+      if (load[i] < load[q]) q = i;
+    load[q] += cost(gp);
     if (!used[q]) cuda_check(cudaStreamWaitEvent(s.side[q], s.fork, 0), "cudaStreamWaitEvent");
     used[q] = true;
     Launch d;
@@ -366,7 +389,7 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
     cuda_check(cudaEventRecord(s.joined[q], s.side[q]), "cudaEventRecord");
     cuda_check(cudaStreamWaitEvent(s.stream, s.joined[q], 0), "cudaStreamWaitEvent");
   }
-  cuda_check(cudaMemcpyAsync(s.out.as() + out_begin, base + out_begin, out_end - out_begin, cudaMemcpyDeviceToHost,
+  cuda_check(cudaMemcpyAsync(s.out.as(), base + out_begin, out_end - out_begin, cudaMemcpyDeviceToHost,
                              s.stream),
              "copy out");
   cuda_check(cudaEventRecord(s.done, s.stream), "cudaEventRecord");
@@ -377,8 +400,8 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
 
 void fecl_server_s::harvest(Slot& s) {
   for (auto& r : s.reqs) {
-    std::memcpy(r->msg, s.out.as() + r->msg_off, r->n * r->c->msg());
-    if (r->iters) std::memcpy(r->iters, s.out.as() + r->it_off, r->n * 4);
+    std::memcpy(r->msg, s.out.as() + (r->msg_off - s.out_begin), r->n * r->c->msg());
+    if (r->iters) std::memcpy(r->iters, s.out.as() + (r->it_off - s.out_begin), r->n * 4);
   }
   const auto now = Clock::now();
   float gpu_ms = 0.0f;
@@ -532,6 +555,8 @@ int fecl_server_create(const fecl_server_options* options, fecl_server_t* out) {
         cuda_check(cudaEventCreateWithFlags(&sl->joined[q], cudaEventDisableTiming), "cudaEventCreate");
       }
       sl->arena.reserve(s->arena_bytes());
+      sl->in.reserve(kInitialStagingIn);
+      sl->out.reserve(kInitialStagingOut);
       s->slots.push_back(std::move(sl));
     }
     s->worker = std::thread([p = s.get()] { p->run(); });
