@@ -772,13 +772,22 @@ void ldpc_lanes_h2_layout(LdpcLanesParams& p, void* scratch, int W) {
   p.barrier = reinterpret_cast<unsigned*>(q);
 }
 
-// Lanes per group for a batch of n frames: the narrowest power of two from 2 to 32
-// whose group (2 W frames) holds the batch, so that a batch of a few frames runs few
-// idle lanes; batches of more than 64 frames take full groups of 32.
+// Lanes per group for a batch of n frames.  Up to 16 frames: the narrowest power of
+// two from 2 to 8 whose group (2 W frames) holds the batch.  Beyond: 32, 16 or 8
+// lanes, whichever leaves the fewest idle frame slots in the last group, the wider
+// unless a narrower one saves more than n / 16 of them -- groups of 8 lanes and up
+// still use every 32-byte sector they touch, narrower ones would not.
 int ldpc_lanes_h2_width(int64_t nframes) {
-  int W = 2;
-  while (W < kLanes && 2 * W < nframes) W *= 2;
-  return W;
+  if (nframes <= 16) {
+    int W = 2;
+    while (2 * W < nframes) W *= 2;
+    return W;
+  }
+  auto idle = [&](int64_t w) { return (nframes + 2 * w - 1) / (2 * w) * (2 * w) - nframes; };
+  int best = kLanes;
+  for (int W : {16, 8})
+    if (idle(best) - idle(W) > nframes / 16) best = W;
+  return best;
 }
 
 int64_t ldpc_lanes_h2_group_bytes(int64_t N, int64_t E) { return int64_t(kLanes) * (2 * 8 * N + 4 * E); }

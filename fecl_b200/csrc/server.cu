@@ -57,22 +57,26 @@ int guarded(F&& f) {
 
 using Clock = std::chrono::steady_clock;
 
-// Pinned staging memory of a slot.  It grows at least twofold when a batch needs more:
-// cudaFreeHost waits for the whole device, so every regrowth stalls the batches of the
-// other slots, and a load that ramps up must not pay that once per batch.
+// Pinned staging memory of a slot.  It grows at least twofold when a batch needs more,
+// and the buffers it outgrows are released only with the server: cudaFreeHost waits
+// for the whole device, so freeing one while other slots' batches run would stall
+// them (on a ramping load, batch after batch).  The retired buffers add up to less
+// than the current one.
 struct PinnedBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;
+  std::vector<void*> retired;
   ~PinnedBuffer() {
     if (ptr) cudaFreeHost(ptr);
+    for (void* q : retired) cudaFreeHost(q);
   }
   void reserve(size_t n) {
     if (n <= bytes) return;
     n = std::max(n, 2 * bytes);
-    if (ptr) cudaFreeHost(ptr);
-    ptr = nullptr;
-    bytes = 0;
-    cuda_check(cudaHostAlloc(&ptr, n, cudaHostAllocDefault), "cudaHostAlloc");
+    void* q = nullptr;
+    cuda_check(cudaHostAlloc(&q, n, cudaHostAllocDefault), "cudaHostAlloc");
+    if (ptr) retired.push_back(ptr);
+    ptr = q;
     bytes = n;
   }
   char* as() const { return static_cast<char*>(ptr); }
@@ -98,8 +102,8 @@ struct Request {
 constexpr int kSideStreams = 8;  // per slot: codec groups of a batch run on these at once
 // Pinned staging reserved per slot at creation: the L-values (and turbo descriptors)
 // of a few hundred frames, and their decisions.
-constexpr size_t kInitialStagingIn = size_t(32) << 20;
-constexpr size_t kInitialStagingOut = size_t(4) << 20;
+constexpr size_t kInitialStagingIn = size_t(64) << 20;
+constexpr size_t kInitialStagingOut = size_t(16) << 20;
 
 struct Slot {
   cudaStream_t stream = nullptr;

@@ -338,17 +338,18 @@ def test_packed_fp16_frames_are_independent():
 
 @pytest.mark.parametrize("n,rate", [(16200, (3, 5)), (64800, (1, 2))])
 def test_packed_fp16_group_width_does_not_change_results(n, rate):
-    """A batch of n <= 64 frames runs one group of W lanes (2 W frames), W the
-    smallest power of two from 2 to 32 with 2 W >= n; larger batches groups of 32
-    lanes: every frame's bits, iteration count and soft outputs (a-posteriori,
-    extrinsic, edge state) are the same bit for bit in batches of every width as in
-    one of 40 frames (W = 32)."""
+    """Batches of up to 16 frames run one group of 2, 4 or 8 lanes (2 W frames);
+    larger ones groups of 8, 16 or 32 lanes, whichever idles the fewest frame slots:
+    every frame's bits, iteration count and soft outputs (a-posteriori, extrinsic,
+    edge state) are the same bit for bit in batches of every width (1, 3 and 4
+    frames: W = 2; 5: 4; 16 and 37: 8; 17 and 32: 16) as in one of 64 frames
+    (W = 32)."""
     import fecl_b200 as F
     from fecl_b200 import channel as ch
     H = F.Ldpc.DvbS2.matrix(n, Fraction(*rate))
     code = _nms(H, 1, 30)
     K, N = code.msgSize(), code.paritySize()
-    total = 40
+    total = 64
     msg = ch.random_bits(total * K, 47)
     lo, hi = (1.6, 3.2) if n == 16200 else (0.9, 1.8)
     llr = ch.awgn_llr_per_frame(code.encode(msg), N, np.linspace(lo, hi, total), K / N, 47, np.float32)
@@ -363,7 +364,7 @@ def test_packed_fp16_group_width_does_not_change_results(n, rate):
     full = run(0, total)
     assert len(set(full[1].tolist())) > 2
     sizes = {"bits": K, "iterations": 1, "msg": K, "syst": K, "parity": N, "state": code.stateSize()}
-    for a, b in ((0, 1), (5, 8), (9, 13), (13, 18), (20, 36), (3, 20), (2, 34)):
+    for a, b in ((0, 1), (5, 8), (9, 13), (13, 18), (20, 36), (3, 20), (2, 34), (27, 64)):
         got = run(a, b)
         for (what, size), x, y in zip(sizes.items(), full, got):
             assert np.array_equal(np.asarray(x)[a * size:b * size], np.asarray(y)), (a, b, what)
