@@ -261,6 +261,7 @@ struct TurboLteParams {
   int32_t out_dtype = 1;
   // filled by the launcher
   int32_t Kp = 0, Tp = 0, seg_len = 0;
+  int64_t frame0 = 0;  // frame of the launch's first CTA
   int64_t frame_stride = 0;
   float* ck = nullptr;
   float* ynew = nullptr;  // parallel: [nframes][Kp] the constituent-1 extrinsic values of this iteration

@@ -43,6 +43,10 @@
 // block load is 16-byte aligned.
 #include <math.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "common.cuh"
 #include "kernels.hpp"
 
@@ -82,10 +86,18 @@ __device__ __forceinline__ float lsum(float a, float b) {
   return fmaxf(a, b) + lut_log1pexpm(c_lut, fabsf(a - b));
 }
 
+// max(a, b, c) in one instruction (the three-input form of max.f32, sm_100): the same
+// value as fmaxf(fmaxf(a, b), c), a maximum being exact.
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
 // v[s] -= max(v), with the subtraction as four packed f32x2 adds of -m (x - m is
 // x + (-m) exactly).
 __device__ __forceinline__ void normalize8(float v[8]) {
-  const float m = fmaxf(fmaxf(fmaxf(v[0], v[1]), fmaxf(v[2], v[3])), fmaxf(fmaxf(v[4], v[5]), fmaxf(v[6], v[7])));
+  const float m = fmax3(fmax3(v[0], v[1], v[2]), fmax3(v[3], v[4], v[5]), fmaxf(v[6], v[7]));
   const float2 nm = make_float2(-m, -m);
 #pragma unroll
   for (int s = 0; s < 8; s += 2) {
@@ -200,10 +212,10 @@ __device__ __forceinline__ float ext_step(const float a[8], const float b[8], co
     }
     const float lp = g.g[1];
     // u = 0: parity 0 at s in {0,1,6,7}, parity 1 at {2,3,4,5}; u = 1 the reverse.
-    const float m0p0 = fmaxf(fmaxf(w0[0], w0[1]), fmaxf(w0[6], w0[7]));
-    const float m0p1 = fmaxf(fmaxf(w0[2], w0[3]), fmaxf(w0[4], w0[5]));
-    const float m1p0 = fmaxf(fmaxf(w1[2], w1[3]), fmaxf(w1[4], w1[5]));
-    const float m1p1 = fmaxf(fmaxf(w1[0], w1[1]), fmaxf(w1[6], w1[7]));
+    const float m0p0 = fmax3(fmaxf(w0[0], w0[1]), w0[6], w0[7]);
+    const float m0p1 = fmax3(fmaxf(w0[2], w0[3]), w0[4], w0[5]);
+    const float m1p0 = fmax3(fmaxf(w1[2], w1[3]), w1[4], w1[5]);
+    const float m1p1 = fmax3(fmaxf(w1[0], w1[1]), w1[6], w1[7]);
     const float m0 = fmaxf(m0p0, m0p1 + lp);
     const float m1 = fmaxf(m1p0, m1p1 + lp);
     return m1 - m0;
@@ -255,10 +267,10 @@ __device__ __forceinline__ float par_step(const float a[8], const float b[8], co
       w1[s] = a[s] + b[lte_next(s, 1)];
     }
     const float la = g.g[2];
-    const float m0p0 = fmaxf(fmaxf(w0[0], w0[1]), fmaxf(w0[6], w0[7]));
-    const float m0p1 = fmaxf(fmaxf(w0[2], w0[3]), fmaxf(w0[4], w0[5]));
-    const float m1p0 = fmaxf(fmaxf(w1[2], w1[3]), fmaxf(w1[4], w1[5]));
-    const float m1p1 = fmaxf(fmaxf(w1[0], w1[1]), fmaxf(w1[6], w1[7]));
+    const float m0p0 = fmax3(fmaxf(w0[0], w0[1]), w0[6], w0[7]);
+    const float m0p1 = fmax3(fmaxf(w0[2], w0[3]), w0[4], w0[5]);
+    const float m1p0 = fmax3(fmaxf(w1[2], w1[3]), w1[4], w1[5]);
+    const float m1p1 = fmax3(fmaxf(w1[0], w1[1]), w1[6], w1[7]);
     return fmaxf(m0p1, m1p1 + la) - fmaxf(m0p0, m1p0 + la);
   } else {
     float d[16];
@@ -801,7 +813,7 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
 template <int ALG, int SEGS, bool SOFT = false>
 __global__ void __launch_bounds__(2 * SEGS, SEGS == 32 ? 4 : 3) turbo_lte_kernel(TurboLteParams p) {
   extern __shared__ float smem[];
-  const int64_t f = blockIdx.x;
+  const int64_t f = p.frame0 + blockIdx.x;
   const int nblk = (p.K + 3 + kBlk - 1) / kBlk;
   LteJob q;
   q.K = p.K;
@@ -949,6 +961,62 @@ size_t lte_smem_bytes(int max_K) {
 
 int resolve_segs(int segs) { return segs == 32 ? 32 : (segs == 64 ? 64 : kDefaultSegs); }
 
+// Resident CTAs of kern on the whole GPU (0 if the query fails).
+template <class Kern>
+int64_t resident_ctas(Kern kern, int threads, size_t smem) {
+  int per_sm = 0, dev = 0, sms = 0;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess ||
+      cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return int64_t(per_sm) * sms;
+}
+
+// Frames (from the first) that the 32-segment shape decodes when the segment count
+// is left to the launcher; the rest take the 64-segment shape.  A CTA decodes one
+// frame start to end, so n frames take ceil(n / resident) rounds of about equal time
+// and a last round holding a few frames leaves most of the GPU idle for a whole
+// frame's decode.  When the 64-segment shape (fewer resident CTAs: 3 per SM against
+// 4, register-bound) would end on a round less than half full, whole rounds of the
+// 32-segment shape go first so that the 64-segment rounds are full or nearly so:
+// K=6144 x 1024 frames on 148 SMs is 592 + 432 frames in two rounds (1.12 ms measured)
+// instead of 444 + 444 + 136 in three (1.23 ms).  Which frames take which shape does not
+// change their results beyond FP32 rounding of the window boundaries.
+template <int ALG>
+int64_t split_frames(int K, int64_t nframes) {
+  // resident CTAs of both shapes, remembered per (device, K)
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, std::pair<int64_t, int64_t>> known;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int64_t r64, r32;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = known.find({dev, K});
+    if (it == known.end()) {
+      const std::pair<int64_t, int64_t> r{resident_ctas(turbo_lte_kernel<ALG, 64>, 128, lte_smem_bytes<64>(K)),
+                                          resident_ctas(turbo_lte_kernel<ALG, 32>, 64, lte_smem_bytes<32>(K))};
+      it = known.emplace(std::make_pair(dev, K), r).first;
+    }
+    r64 = it->second.first;
+    r32 = it->second.second;
+  }
+  if (r64 <= 0 || r32 <= 0 || nframes <= r64) return 0;
+  auto rounds = [](int64_t n, int64_t r) { return (n + r - 1) / r; };
+  auto tail_ok = [&](int64_t n) { return n % r64 == 0 || 2 * (n % r64) >= r64; };
+  if (tail_ok(nframes)) return 0;
+  for (int64_t n32 = r32; n32 < nframes; n32 += r32) {
+    const int64_t rest = nframes - n32;
+    if (tail_ok(rest) && rounds(n32, r32) + rounds(rest, r64) <= rounds(nframes, r64)) return n32;
+  }
+  return 0;
+}
+
 }  // namespace
 
 cudaError_t turbo_lte_init() {
@@ -1013,6 +1081,36 @@ cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
     }
   }
   const size_t smem = lte_smem_bytes<64>(p.K);
+  if (p.segs == 0) {
+    // the launcher's choice: whole rounds of the 32-segment shape first where that
+    // fills the rounds better (split_frames)
+    const int64_t n32 = p.algorithm == kExact    ? split_frames<kExact>(p.K, p.nframes)
+                        : p.algorithm == kLinear ? split_frames<kLinear>(p.K, p.nframes)
+                                                 : split_frames<kApproximate>(p.K, p.nframes);
+    if (n32 > 0) {
+      TurboLteParams a = p;
+      a.nframes = n32;
+      a.seg_len = LteGeometry(p.K, 32).seg_len;
+      const size_t smem32 = lte_smem_bytes<32>(p.K);
+      auto run = [&](auto k32, auto k64) -> cudaError_t {
+        cudaError_t err = cudaFuncSetAttribute(k32, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem32));
+        if (err != cudaSuccess) return err;
+        k32<<<unsigned(n32), 64, smem32, s>>>(a);
+        if ((err = cudaGetLastError()) != cudaSuccess) return err;
+        TurboLteParams b = p;
+        b.frame0 = n32;
+        if ((err = cudaFuncSetAttribute(k64, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))) != cudaSuccess)
+          return err;
+        k64<<<unsigned(p.nframes - n32), 128, smem, s>>>(b);
+        return cudaGetLastError();
+      };
+      switch (p.algorithm) {
+        case kExact: return run(turbo_lte_kernel<kExact, 32>, turbo_lte_kernel<kExact, 64>);
+        case kLinear: return run(turbo_lte_kernel<kLinear, 32>, turbo_lte_kernel<kLinear, 64>);
+        default: return run(turbo_lte_kernel<kApproximate, 32>, turbo_lte_kernel<kApproximate, 64>);
+      }
+    }
+  }
   switch (p.algorithm) {
     case kExact: return launch(turbo_lte_kernel<kExact, 64>, 128, smem);
     case kLinear: return launch(turbo_lte_kernel<kLinear, 64>, 128, smem);
