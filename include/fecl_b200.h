@@ -326,7 +326,8 @@ int fecl_ldpc_set_wave(fecl_codec_t codec, int32_t groups);
 int fecl_ldpc_set_persistent(fecl_codec_t codec, int32_t mode);
 
 /* Windowed turbo decoder: training steps run before each segment's forward and
- * backward walk (a multiple of 8; -1 restores the default of 96).  Training only
+ * backward walk (a multiple of 8; -1 restores the default: 80 for max-log, 96 for
+ * the log-MAP algorithms).  Training only
  * sets how often a segment boundary fails verification and is recomputed; results
  * do not depend on it beyond FP32 rounding. */
 int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps);
