@@ -322,12 +322,15 @@ struct Frame {
   float* ckb;        // [nblk + 1][8]
 };
 
+// A segment's boundary vectors: a forward segment's start (after training) is its
+// first checkpoint and a backward segment's end its last, so those two stay in the
+// checkpoint arrays (global memory); the other two are kept here.
 template <int SEGS>
 struct Shared {
-  float sv[2][SEGS][8];  // metrics at the segment boundary after training (fwd, bwd)
-  float ev[2][SEGS][8];  // end metrics of each segment (fwd, bwd)
-  float flat[8];         // training start: all states equal
-  float term[8];         // trellis termination: state 0
+  float bwd_start[SEGS][8];  // backward segment w's metrics at its end a1 after training
+  float fwd_end[SEGS][8];    // forward segment w's metrics at a1
+  float flat[8];             // training start: all states equal
+  float term[8];             // trellis termination: state 0
   uint32_t crc_part[2 * SEGS / 32];  // per-warp CRC syndromes
 };
 
@@ -434,7 +437,7 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
       const RawChunk cur = nxt;
       if (c + 1 < c_end) load_raw(j, c + 1, fr, perm, nxt);
       const int t0 = c * kBlk;
-      if (t0 == a0) {
+      if (t0 == a0 && vstart) {
 #pragma unroll
         for (int s = 0; s < 8; ++s) vstart[s] = v[s];
       }
@@ -471,8 +474,10 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
   } else {
     const int nblk = (T + kBlk - 1) / kBlk;
     if (t_train == a1) {
+      if (vstart) {
 #pragma unroll
-      for (int s = 0; s < 8; ++s) vstart[s] = v[s];
+        for (int s = 0; s < 8; ++s) vstart[s] = v[s];
+      }
       if (a1 == T) store_ck(fr.ckb + nblk * 8, v);
     }
     const int c_lo = a0 / kBlk;
@@ -504,7 +509,7 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
       }
       normalize8(v);
       const int tm = c * kBlk;  // v now holds the metrics at time tm
-      if (tm == a1) {
+      if (tm == a1 && vstart) {
 #pragma unroll
         for (int s = 0; s < 8; ++s) vstart[s] = v[s];
       }
@@ -518,8 +523,10 @@ __device__ __noinline__ void segment_walk(int fwd, int j, int t_train, int a0, i
       }
     }
   }
+  if (vend) {
 #pragma unroll
-  for (int s = 0; s < 8; ++s) vend[s] = v[s];
+    for (int s = 0; s < 8; ++s) vend[s] = v[s];
+  }
 }
 
 // Where soDecode's last iteration leaves its values: the constituent's extrinsic values
@@ -683,7 +690,9 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
             t_train = exact ? T : a1 + q.train;
             vin = exact ? sh.term : sh.flat;
           }
-          segment_walk<ALG>(fwd, j, t_train, a0, a1, vin, sh.sv[fwd ? 0 : 1][w], sh.ev[fwd ? 0 : 1][w], K, T, fr, X,
+          // a forward start is the checkpoint at a0, a backward end the one at a0
+          segment_walk<ALG>(fwd, j, t_train, a0, a1, vin, fwd ? nullptr : sh.bwd_start[w], fwd ? sh.fwd_end[w] : nullptr,
+                            K, T, fr, X,
                             Y, perm, false, tol);
         }
       }
@@ -697,8 +706,11 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
         const int w = fwd ? tid : tid - SEGS;
         bool bad = false;
         if (w < S) {
-          if (fwd && w > 0) bad = !close8(sh.sv[0][w], sh.ev[0][w - 1], tol);
-          if (!fwd && w < S - 1) bad = !close8(sh.sv[1][w], sh.ev[1][w + 1], tol);
+          // forward: this segment's start (its checkpoint at a0) against the previous
+          // segment's end; backward: this segment's start at a1 against the next
+          // segment's end (its checkpoint at a1)
+          if (fwd && w > 0) bad = !close8(fr.cka + (w * L / kBlk) * 8, sh.fwd_end[w - 1], tol);
+          if (!fwd && w < S - 1) bad = !close8(sh.bwd_start[w], fr.ckb + ((w + 1) * L / kBlk) * 8, tol);
         }
         if (!__syncthreads_or(bad)) break;
         ++rounds;
@@ -709,16 +721,20 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
         float start[8];
         if (bad) {
 #pragma unroll
-          for (int s = 0; s < 8; ++s) start[s] = fwd ? sh.ev[0][w - 1][s] : sh.ev[1][w + 1][s];
+          for (int s = 0; s < 8; ++s) start[s] = fwd ? sh.fwd_end[w - 1][s] : fr.ckb[((w + 1) * L / kBlk) * 8 + s];
         }
         __syncthreads();
         if (bad) {
           if (q.stats) atomicAdd(q.stats + 2, 1ull);
-          float* sv = sh.sv[fwd ? 0 : 1][w];
+          // the walk reads its start from sv: a forward segment's checkpoint at a0
+          // (which the walk writes again with the same values), a backward segment's
+          // start vector
+          float* sv = fwd ? fr.cka + (w * L / kBlk) * 8 : sh.bwd_start[w];
 #pragma unroll
           for (int s = 0; s < 8; ++s) sv[s] = start[s];
           const int a0 = w * L, a1 = min(T, a0 + L);
-          segment_walk<ALG>(fwd, j, fwd ? a0 : a1, a0, a1, sv, sv, sh.ev[fwd ? 0 : 1][w], K, T, fr, X, Y, perm, true,
+          segment_walk<ALG>(fwd, j, fwd ? a0 : a1, a0, a1, sv, fwd ? nullptr : sv, fwd ? sh.fwd_end[w] : nullptr, K, T, fr,
+                            X, Y, perm, true,
                             tol);
         }
         __syncthreads();

@@ -333,10 +333,11 @@ int fecl_ldpc_set_persistent(fecl_codec_t codec, int32_t mode);
 int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps);
 
 /* Windowed turbo decoder: forward (and backward) segments per frame, 32 or 64, one
- * thread each (0 restores the built-in choice).  Fewer, longer segments spend a
- * smaller share of each walk on training and fit more frames on an SM; results do
- * not depend on it beyond FP32 rounding.  Extension: no counterpart in the
- * reference. */
+ * thread each (0 restores the built-in choice: 64, with whole GPU rounds of 32-segment
+ * frames first where a batch would otherwise end on a round less than half full).
+ * Fewer, longer segments spend a smaller share of each walk on training and fit more
+ * frames on an SM; results do not depend on it beyond FP32 rounding.  Extension: no
+ * counterpart in the reference. */
 int fecl_turbo_set_window_segments(fecl_codec_t codec, int32_t segments);
 
 /* Windowed turbo decoder autotuner: decodes the caller's `nframes` frames of device
