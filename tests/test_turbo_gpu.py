@@ -86,6 +86,40 @@ def test_windowed_equals_generic_kernel():
             assert_hard_parity(code.decode(llr), ref, msg, K) > n // 4, (train, segs)
 
 
+@pytest.mark.parametrize("alg", [2, 1, 0])
+def test_balanced_rounds_match_generic_kernel(alg):
+    """1024 frames with the segment count left to the launcher run as two launches
+    (whole GPU rounds of 32-segment frames, then 64-segment ones, the second launch's
+    frame offset applied to every buffer).  With a CRC-24A stop, under the parity
+    rules: the decisions equal the generic kernel's in every frame it decodes and the
+    same frames fail; every frame of either launch that stopped early passes its
+    CRC, each reporting its own iteration count; a single 64-segment launch gives
+    the same decisions in the decoded frames."""
+    import torch
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    K, n = 1024, 1024
+    code = F.Turbo.lte(K, F.Turbo.DecoderOptions().algorithm(alg).iterations(6).crc(F.CRC24A))
+    info = torch.from_numpy(ch.random_bits(n * (K - 24), 35 + alg)).cuda()
+    msg = F.crc24_attach(info, F.CRC24A, n).cpu().numpy()
+    ebn0 = np.repeat(np.linspace(0.3, 1.5, 8), n // 8)
+    llr = ch.awgn_llr_per_frame(code.encode(msg), code.paritySize(), ebn0, K / code.paritySize(), 35 + alg,
+                                np.float32)
+    code.setKernel("generic")
+    ref, ref_it = code.decode(llr, iterations=True)
+    code.setKernel("auto")
+    split, split_it = code.decode(llr, iterations=True)
+    assert assert_hard_parity(split, ref, msg, K) > n // 4
+    ok = frame_ok(ref, msg, K)
+    early = split_it < 6
+    assert early[: n // 2].sum() > n // 16 and early[n // 2:].sum() > n // 16 and len(set(split_it.tolist())) > 2
+    crc_ok = F.crc24_check(torch.from_numpy(split).cuda(), F.CRC24A, n).cpu().numpy()
+    assert crc_ok[early].all()
+    code.setWindowSegments(64)
+    single = code.decode(llr)
+    assert np.array_equal(split.reshape(n, K)[ok], single.reshape(n, K)[ok])
+
+
 @pytest.mark.parametrize("K", [40, 1008, 4096, 6144])
 def test_lte_sizes(K):
     """Every LTE block size the windowed kernel sees decodes like the generic kernel."""
