@@ -11,8 +11,9 @@
 //      wave sizes, cluster-resident LDPC with several cluster shapes), timed on
 //      the job's own inputs and remembered per (code, batch size) for the process;
 //   3. carves every job's scratch out of one workspace and captures the launches
-//      into a graph: the turbo launch on one branch, the other jobs spread over four
-//      more branches forked from it, so they all run at once on different SMs.
+//      into a graph: the turbo launch on one branch, the other jobs spread over eight
+//      more branches forked from it (longest first, each to the branch with the least
+//      work so far), so they all run at once on different SMs.
 // fecl_batch_run replays the graph.  The codecs' options and tables are read when
 // the graph is built: changing a codec's options or destroying it invalidates the
 // batch.
@@ -136,7 +137,7 @@ struct ChoiceScope {
 
 }  // namespace
 
-constexpr int kBranches = 4;  // graph branches the non-turbo-batch jobs are spread over
+constexpr int kBranches = 8;  // graph branches the non-turbo-batch jobs are spread over
 
 struct fecl_batch_s {
   int device = 0;
@@ -395,10 +396,24 @@ int fecl_batch_create(const fecl_batch_job* jobs, uint32_t njobs, int32_t flags,
         plan << shared.describe(persistent);
       }
       const int first = shared.empty() ? 0 : 1;  // branch 0 holds the shared launches
-      int k = 0;
-      for (auto& s : js) {
-        if (s.lte || s.multi) continue;
-        cudaStream_t st = b->cap2[first + k++ % (kBranches - first)];
+      // longest first, each to the least loaded branch; a job's work is estimated by
+      // its parity bits times its iteration limit times its frames
+      std::vector<JobState*> order;
+      for (auto& s : js)
+        if (!s.lte && !s.multi) order.push_back(&s);
+      auto cost = [](const JobState* s) {
+        const double it = s->c->kind == 0 ? double(std::max(1, s->c->ldev.iterations)) : 1.0;
+        return double(s->c->parity()) * it * double(s->job->nframes);
+      };
+      std::stable_sort(order.begin(), order.end(), [&](const JobState* a, const JobState* c) { return cost(a) > cost(c); });
+      double load[kBranches] = {};
+      for (JobState* sp : order) {
+        auto& s = *sp;
+        int q = first;
+        for (int i = first + 1; i < kBranches; ++i)
+          if (load[i] < load[q]) q = i;
+        load[q] += cost(sp);
+        cudaStream_t st = b->cap2[q];
         ChoiceScope scope(s.c, s.choice);
         Launch d;
         d.llr = s.job->llr;
