@@ -813,7 +813,7 @@ class Turbo(Codec):
 
     def setWindowSegments(self, segments):
         """Extension: forward/backward segments per frame of the windowed LTE decoder
-        (32 or 64, 0 for the built-in choice)."""
+        (32, 64 or 128, 0 for the built-in choice)."""
         _check(_L.fecl_turbo_set_window_segments(self._h, int(segments)))
 
     def tuneWindow(self, llr, out=None):

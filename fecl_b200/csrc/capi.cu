@@ -1065,7 +1065,8 @@ int fecl_turbo_set_window_segments(fecl_codec_t codec, int32_t segments) {
   return guarded([&] {
     auto c = checked(codec);
     if (c->kind != 1) fail(FECL_EINVAL, "not a turbo codec");
-    if (segments != 0 && segments != 32 && segments != 64) fail(FECL_EINVAL, "window segments must be 0, 32 or 64");
+    if (segments != 0 && segments != 32 && segments != 64 && segments != 128)
+      fail(FECL_EINVAL, "window segments must be 0, 32, 64 or 128");
     std::lock_guard<std::mutex> lk(c->mu);
     c->lte_segs = segments;
   });

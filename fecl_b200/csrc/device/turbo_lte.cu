@@ -827,7 +827,7 @@ __device__ __forceinline__ void decode_lte_frame(const LteJob& q, float* smem) {
 }
 
 template <int ALG, int SEGS, bool SOFT = false>
-__global__ void __launch_bounds__(2 * SEGS, SEGS == 32 ? 4 : 3) turbo_lte_kernel(TurboLteParams p) {
+__global__ void __launch_bounds__(2 * SEGS, SEGS == 32 ? 4 : (SEGS == 128 ? 1 : 3)) turbo_lte_kernel(TurboLteParams p) {
   extern __shared__ float smem[];
   const int64_t f = p.frame0 + blockIdx.x;
   const int nblk = (p.K + 3 + kBlk - 1) / kBlk;
@@ -975,7 +975,17 @@ size_t lte_smem_bytes(int max_K) {
   return size_t(2 * LteGeometry(max_K, SEGS).Kp) * sizeof(float) + sizeof(Shared<SEGS>);
 }
 
-int resolve_segs(int segs) { return segs == 32 ? 32 : (segs == 64 ? 64 : kDefaultSegs); }
+int resolve_segs(int segs) { return segs == 32 || segs == 64 || segs == 128 ? segs : kDefaultSegs; }
+
+// Streaming multiprocessors of the current device (0 if the query fails).
+int device_sms() {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return sms;
+}
 
 // Training steps before each segment when the caller leaves them to the launcher.
 // Max-log: 80 (K=6144 x 1024 at 0.7 dB: 1.10 ms against 1.13 ms with 96, the same
@@ -1101,6 +1111,19 @@ cudaError_t launch_turbo_lte(TurboLteParams p, cudaStream_t s) {
       case kExact: return launch(turbo_lte_kernel<kExact, 32>, 64, smem);
       case kLinear: return launch(turbo_lte_kernel<kLinear, 32>, 64, smem);
       default: return launch(turbo_lte_kernel<kApproximate, 32>, 64, smem);
+    }
+  }
+  // A batch of at most one frame per SM decodes in one round whose time is one
+  // frame's latency: with the segment count left to the launcher it takes the
+  // 128-segment shape (one CTA of 256 threads per frame: half as many phase B blocks
+  // per thread and shorter segment walks than with 64), as does an explicit 128.
+  if (segs == 128 || (p.segs == 0 && p.nframes <= device_sms())) {
+    p.seg_len = LteGeometry(p.K, 128).seg_len;
+    const size_t smem = lte_smem_bytes<128>(p.K);
+    switch (p.algorithm) {
+      case kExact: return launch(turbo_lte_kernel<kExact, 128>, 256, smem);
+      case kLinear: return launch(turbo_lte_kernel<kLinear, 128>, 256, smem);
+      default: return launch(turbo_lte_kernel<kApproximate, 128>, 256, smem);
     }
   }
   const size_t smem = lte_smem_bytes<64>(p.K);

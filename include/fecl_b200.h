@@ -332,9 +332,11 @@ int fecl_ldpc_set_persistent(fecl_codec_t codec, int32_t mode);
  * do not depend on it beyond FP32 rounding. */
 int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps);
 
-/* Windowed turbo decoder: forward (and backward) segments per frame, 32 or 64, one
- * thread each (0 restores the built-in choice: 64, with whole GPU rounds of 32-segment
- * frames first where a batch would otherwise end on a round less than half full).
+/* Windowed turbo decoder: forward (and backward) segments per frame, 32, 64 or 128,
+ * one thread each (0 restores the built-in choice: 128 for a batch of at most one
+ * frame per SM, whose time is one frame's latency; otherwise 64, with whole GPU rounds
+ * of 32-segment frames first where a batch would otherwise end on a round less than
+ * half full).  soDecode always uses 64.
  * Fewer, longer segments spend a smaller share of each walk on training and fit more
  * frames on an SM; results do not depend on it beyond FP32 rounding.  Extension: no
  * counterpart in the reference. */
