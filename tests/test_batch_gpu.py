@@ -47,9 +47,17 @@ def _jobs(seed=0, dtype=np.float32):
 
 
 def _alone(jobs):
+    """Each job decoded by its codec alone; LTE turbo codecs with the window shape of
+    the batch's mixed-K kernel (64 segments), which a decode of a few frames would
+    otherwise replace by 128 (a difference of FP32 rounding in frames that fail)."""
+    import fecl_b200 as F
     out = []
     for code, llr, _, _ in jobs:
+        if isinstance(code, F.Turbo):
+            code.setWindowSegments(64)
         bits, its = code.decode(llr, iterations=True)
+        if isinstance(code, F.Turbo):
+            code.setWindowSegments(0)
         out.append((bits.cpu().numpy(), its.cpu().numpy()))
     return out
 
