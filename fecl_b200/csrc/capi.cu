@@ -862,7 +862,9 @@ int fecl_turbo_tune_window(fecl_codec_t codec, const void* llr, int32_t llr_dtyp
       io.in_dtype = llr_dtype;
       io.out_dtype = FECL_F32;
       try {
-        for (int segs : {64, 32})
+        // 0: the launcher's own choice (balanced rounds of the 32- and 64-segment
+        // shapes, or 128 segments for at most one frame per SM)
+        for (int segs : {0, 128, 64, 32})
           for (int train : {48, 64, 80, 96, 128}) {
             c->lte_segs = segs;
             c->lte_train = train;

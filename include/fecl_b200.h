@@ -343,8 +343,9 @@ int fecl_turbo_set_window_training(fecl_codec_t codec, int32_t steps);
 int fecl_turbo_set_window_segments(fecl_codec_t codec, int32_t segments);
 
 /* Windowed turbo decoder autotuner: decodes the caller's `nframes` frames of device
- * memory L-values (into msg) with every equivalent window shape -- 32 or 64
- * segments per direction, 48 to 128 training steps -- keeps the fastest in the
+ * memory L-values (into msg) with every equivalent window shape -- 32, 64 or 128
+ * segments per direction or the launcher's choice (0), 48 to 128 training steps --
+ * keeps the fastest in the
  * codec and returns it.  Results are remembered per (K, nframes, algorithm,
  * iterations, scheduling) for the process, so later calls only apply them.  Every
  * shape computes the full-frame recursion up to FP32 rounding.  Extension: no

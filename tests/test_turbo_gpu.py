@@ -81,7 +81,7 @@ def test_windowed_equals_generic_kernel():
     code.setKernel("auto")
     for train in (0, 32, 96, 256):
         code.setWindowTraining(train)
-        for segs in (32, 64):
+        for segs in (32, 64, 128):
             code.setWindowSegments(segs)
             assert_hard_parity(code.decode(llr), ref, msg, K) > n // 4, (train, segs)
 
@@ -336,7 +336,7 @@ def test_tune_window(has_ref):
     llr = ch.awgn_llr(code.encode(msg), 0.7, K / code.paritySize(), 91, np.float32)
     d_llr = torch.from_numpy(llr).cuda()
     segs, train = code.tuneWindow(d_llr)
-    assert segs in (32, 64) and train in (48, 64, 80, 96, 128)
+    assert segs in (0, 32, 64, 128) and train in (48, 64, 80, 96, 128)
     assert code.tuneWindow(d_llr) == (segs, train)
     bits = code.decode(llr)
     ref_bits, ref_app = checker.turbo_lte_decode(K, F.Approximate, 6, F.Serial, llr)
