@@ -48,6 +48,10 @@ using ldpc::Msg;
 namespace cg = cooperative_groups;
 
 __constant__ LinearLut c_lut;
+// The Linear table copied to shared memory by every CTA that uses it: lanes look up
+// different entries, which constant memory serves one address at a time and shared
+// memory (eight words in eight banks) at once.
+__shared__ LinearLut s_lut;
 
 constexpr uint32_t kOffMask = 0x0fffffffu;
 
@@ -131,6 +135,7 @@ __global__ void __launch_bounds__(THREADS, 1) ldpc_cluster_kernel(LdpcClusterPar
     ctl_base[tid] = CL ? map_rank(ctl_sa, tid) : ctl_sa;
   }
   if (tid == 0) ctl.fail[0] = ctl.fail[1] = 0;
+  if (ALG == ldpc::kLinear && tid < 8) s_lut.y[tid] = c_lut.y[tid];
   __syncthreads();
 
   const int I = p.iterations;
@@ -231,7 +236,7 @@ __global__ void __launch_bounds__(THREADS, 1) ldpc_cluster_kernel(LdpcClusterPar
         }
         bad |= par;
         float out[DMAX];
-        ldpc::row_update<ALG, DMAX>(c_lut, v, out, d, sf_row[d >= 2 ? d - 2 : 0]);
+        ldpc::row_update<ALG, DMAX>(s_lut, v, out, d, sf_row[d >= 2 ? d - 2 : 0]);
 #pragma unroll
         for (int j = 0; j < DMAX; ++j)
           if (j < d) M::store(cr + j, out[j]);

@@ -47,6 +47,15 @@ constexpr int kLanes = 32;
 constexpr int kWarpsPerBlock = 8;
 
 __constant__ LinearLut c_lut;
+// The Linear table copied to shared memory by the check kernels: the lanes of a warp
+// (different frames) look up different entries, which constant memory serves one
+// address at a time and shared memory (eight words in eight banks) at once.
+__shared__ LinearLut s_lut;
+
+__device__ __forceinline__ void share_lut() {
+  if (threadIdx.x < 8) s_lut.y[threadIdx.x] = c_lut.y[threadIdx.x];
+  __syncthreads();
+}
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
@@ -111,7 +120,7 @@ __device__ __forceinline__ void store_row(const LdpcLanesParams& p, int g, uint3
     return;
   }
   float out[DMAX];
-  ldpc::row_update<ALG, DMAX>(c_lut, v, out, d, sf_row[d >= 2 ? d - 2 : 0]);
+  ldpc::row_update<ALG, DMAX>(s_lut, v, out, d, sf_row[d >= 2 ? d - 2 : 0]);
   if (mine) {
     typename M::T* cg = c2v + (int64_t(g) * p.E + e0) * kLanes + lane;
 #pragma unroll
@@ -160,7 +169,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_check(LdpcLanesPara
   const float* sf_row = p.sf + size_t(it % p.n_sf) * p.sf_stride;
   const int g = g0 + int(blockIdx.y);
   const uint32_t active = active_of(p, it)[g];
-  if (active == 0) return;
+  if (active == 0) return;  // the same for the whole block (one group per grid row)
+  if constexpr (ALG == kLinear) share_lut();
   const bool mine = (active >> lane) & 1;
   uint32_t bad = 0;
   const int w0 = int(blockIdx.x) * kWarpsPerBlock + (threadIdx.x >> 5);
@@ -240,6 +250,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) lanes_persist(LdpcLanesPa
   const int warps = int(gridDim.x) * kWarpsPerBlock;
   const int ng = p.groups;
   unsigned epoch = 0;
+  if constexpr (ALG == kLinear) share_lut();
   for (int64_t u = warp; u < int64_t(ng) * p.N; u += warps) bit_one<MSG>(p, int(u / p.N), int(u % p.N), lane);
   bool ok = grid_barrier(p.barrier, p.barrier + 1, epoch);
   const int rows = (p.M + kRows - 1) / kRows;
