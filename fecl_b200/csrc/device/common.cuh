@@ -86,6 +86,22 @@ inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cud
   return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
+// phi(x) = log1p(2 / expm1(x)) = -log(tanh(x / 2)) for x >= 0 (+inf at 0, 0 at +inf),
+// the Exact check node's transform (every LDPC kernel calls this one, so they agree
+// bit for bit).  Built from the hardware exponential and logarithm (__expf, __logf:
+// relative error about 2^-22) where their arguments are well conditioned, and from
+// truncated Taylor series where they are not:
+//   expm1(x) = x (1 + x/2 + x^2/6)  for x < 2^-7  (truncation below x^3/24 < 2^-22),
+//   log1p(z) = z (1 - z/2 + z^2/3)  for z < 2^-7  (truncation below z^3/4 < 2^-22).
+// Outside those ranges e^x - 1 keeps 2^-22 relative to e^x and 1 + z is exact to
+// 2^-24, so the result stays within about 3e-5 relative where phi < 1 and 6e-6 above.
+__device__ __forceinline__ float ldpc_phi(float x) {
+  constexpr float kSmall = 0.0078125f;  // 2^-7
+  const float em1 = x < kSmall ? x * fmaf(x, fmaf(x, 1.0f / 6.0f, 0.5f), 1.0f) : __expf(x) - 1.0f;
+  const float z = __fdividef(2.0f, em1);
+  return z < kSmall ? z * fmaf(z, fmaf(z, 1.0f / 3.0f, -0.5f), 1.0f) : __logf(1.0f + z);
+}
+
 __device__ __forceinline__ float lut_log1pexpm(const LinearLut& t, float x) {
   x *= 2.0f;
   if (x >= 7.0f) return 0.0f;

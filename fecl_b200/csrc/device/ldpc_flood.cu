@@ -46,7 +46,7 @@ __device__ __forceinline__ float box_linear(float a, float b) {
 // multiplies tanh(-x/2) over a row and maps back with -2 atanh; in the phi domain the
 // same boxplus is a sum of phi(|x|) and a sign parity, which keeps FP32 accurate where
 // tanh rounds to +-1 (|x| > 17 in FP32).  Inputs are clamped to 80 so phi stays normal.
-__device__ __forceinline__ float phi(float x) { return log1pf(2.0f / expm1f(x)); }
+__device__ __forceinline__ float phi(float x) { return ldpc_phi(x); }
 
 template <int ALG, int DMAX>
 __device__ __forceinline__ void check_row(const LdpcDeviceCode& c, float* __restrict__ c2v,

@@ -33,7 +33,7 @@ __device__ __forceinline__ float box_linear(const LinearLut& lut, float a, float
 // multiplies tanh(-x/2) over a row and maps back with -2 atanh; in the phi domain the
 // same boxplus is a sum of phi(|x|) and a sign parity, which keeps FP32 accurate where
 // tanh rounds to +-1.  Inputs are clamped to 80 so phi stays normal.
-__device__ __forceinline__ float phi(float x) { return log1pf(2.0f / expm1f(x)); }
+__device__ __forceinline__ float phi(float x) { return ldpc_phi(x); }
 
 // Storage of check-to-bit messages: FP32 (reference parity), saturated FP16 (+-65504),
 // or saturated int8 in Q5.2 (step 1/4, range +-31.75).  Arithmetic is FP32 in every case.
