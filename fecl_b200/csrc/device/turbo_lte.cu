@@ -178,7 +178,10 @@ __device__ __forceinline__ void fwd_step(float a[8], const Gam& g) {
   for (int s = 0; s < 8; ++s) {
     if (ALG == kExact) a[s] = esum2(c0[s], c1[s]);
     else if (ALG == kApproximate) a[s] = fmaxf(c0[s], c1[s]);
-    else a[s] = lsum<ALG>(lsum<ALG>(kNegInf, c0[s]), c1[s]);
+    // Linear: the reference's accumulation starts from -inf, and lsum(-inf, c) is c
+    // (the table gives 0 beyond 3.5), so it is left out; only a -0 metric would come
+    // out as +0, which every later maximum and difference treats alike
+    else a[s] = lsum<ALG>(c0[s], c1[s]);
   }
   normalize_step<ALG>(a);
 }
@@ -194,7 +197,7 @@ __device__ __forceinline__ void bwd_step(float b[8], const Gam& g) {
     const float x1 = g.plus<ALG>(b[lte_next(s, 1)], s, 1);
     if (ALG == kExact) n[s] = esum2(x0, x1);
     else if (ALG == kApproximate) n[s] = fmaxf(x0, x1);
-    else n[s] = lsum<ALG>(lsum<ALG>(kNegInf, x0), x1);
+    else n[s] = lsum<ALG>(x0, x1);  // as in fwd_step
   }
 #pragma unroll
   for (int s = 0; s < 8; ++s) b[s] = n[s];
