@@ -92,6 +92,11 @@ def test_invalid_options_raise():
     t = F.Turbo.lte(40)
     with pytest.raises(ValueError):
         t.setWindowTraining(12)
+    for segs in (0, 32, 64, 128):  # the window shapes the decoder has
+        t.setWindowSegments(segs)
+    for segs in (16, 48, 96, 256):
+        with pytest.raises(ValueError):
+            t.setWindowSegments(segs)
 
 
 def test_decode_without_gpu_reports_no_device():
