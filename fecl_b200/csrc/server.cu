@@ -8,8 +8,7 @@
 // while the other slots' batches were on the GPU join the next batch as soon as a
 // slot and its memory free up -- and launches them: every LTE turbo frame of the
 // batch in one persistent mixed-K launch on the slot's stream, the other frames one
-// launch sequence per codec spread over the slot's side streams (kServerSharedLdpc
-// would give the FP16 LDPC groups shared launches instead), so codecs of one batch
+// launch sequence per codec spread over the slot's side streams, so codecs of one batch
 // and batches of different slots overlap on the device.  The same thread
 // harvests finished slots, copies each request's decisions out and stamps its
 // completion time.  Results do not depend on what a request was
@@ -31,7 +30,6 @@
 #include <vector>
 
 #include "codec.hpp"
-#include "ldpc_shared.hpp"
 
 namespace {
 
@@ -160,20 +158,13 @@ struct Group {
   std::vector<Request*> reqs;
   size_t llr_off = 0, msg_off = 0, it_off = 0, scratch_off = 0;
   ScratchPlan sp;
-  bool shared = false;  // in the shared persistent LDPC launch
 };
 
-char* base_of(Slot& s) { return s.arena.as<char>(); }
-
-// Whether the FP16 LDPC groups of a batch share their launches (one check and one bit
-// launch per iteration over every code).  Off: measured on Poisson loads of 5k frames/s
-// it tripled the device time of a batch (27 ms against 8.7 ms per ~70 frames), each
-// shared launch being sized for the largest group it serves.
-constexpr bool kServerSharedLdpc = false;
-
-// Arena bytes set aside for the tables of the shared LDPC launches (a few KB for the
-// codes and groups a batch can hold).
-constexpr size_t kSharedTableSlack = size_t(256) << 10;
+// The FP16 LDPC groups of a batch keep a launch sequence per codec: shared check and
+// bit launches over every code (ldpc_shared.hpp, an option of mixed batches) measured
+// on Poisson loads of 5k frames/s tripled the device time of a batch (27 ms against
+// 8.7 ms per ~70 frames), each shared launch being sized for the largest group it
+// serves.
 
 // Admission accounting of a forming batch: an upper bound of the arena bytes, kept
 // up to date request by request.
@@ -193,7 +184,7 @@ struct Admission {
     const uint64_t lf = lte_frames + (r.lte ? r.n : 0);
     // per group three I/O regions (rounded), descriptors and counters for up to three algorithms
     return io + 3 * 256 * (frames.size() + 1) + al256(r.in_bytes) + al256(r.n * r.c->msg()) + al256(r.n * 4) + sc + lte +
-           al256(lf * sizeof(fecl::TurboLteBatchFrame)) * 2 + 3 * 256 + kSharedTableSlack;
+           al256(lf * sizeof(fecl::TurboLteBatchFrame)) * 2 + 3 * 256;
   }
   void add(const Request& r) {
     const auto key = std::make_pair(r.c, r.dtype);
@@ -255,31 +246,13 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
     }
   }
   const size_t out_end = cv.off;
-  // LDPC groups that take the packed FP16 decoder share their launches (per iteration
-  // one check and one bit launch over all of them); the others get their own decoder
-  SharedLdpc shared;
+  // every non-LTE group gets its codec's decoder and scratch
   for (auto& kv : groups) {
     Group& g = kv.second;
     if (g.lte) continue;
-    if (kServerSharedLdpc && SharedLdpc::eligible(g.c)) {
-      g.shared = true;
-      SharedLdpcJob j;
-      j.c = g.c;
-      j.n = g.n;
-      j.llr = base_of(s) + g.llr_off;
-      j.dtype = g.dtype;
-      j.msg = reinterpret_cast<uint8_t*>(base_of(s) + g.msg_off);
-      j.iters = reinterpret_cast<int32_t*>(base_of(s) + g.it_off);
-      j.scratch_off = cv.take(SharedLdpc::scratch_bytes(j));
-      shared.jobs.push_back(j);
-      continue;
-    }
     g.sp = plan_scratch(g.c, g.n, false);
     g.scratch_off = cv.take(g.sp.bytes);
   }
-  // one pass over every check-degree class and one wave: a server batch holds a few
-  // frames of many codes, and its launches, not its memory traffic, set its time
-  shared.plan(cv, false, INT64_MAX);
   char* base = s.arena.as<char>();
   std::map<int, std::vector<fecl::TurboLteBatchFrame>> tdesc;
   for (auto& kv : groups) {
@@ -312,11 +285,6 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
   size_t host_desc = al256(in_end);
   size_t host_end = host_desc;
   for (auto& kv : tdesc) host_end += al256(kv.second.size() * sizeof(fecl::TurboLteBatchFrame));
-  // the shared LDPC tables are staged after the descriptors, at their arena offsets
-  // shifted by host_tab - tables_begin()
-  const size_t tab0 = shared.tables_begin(), tab1 = shared.tables_end();
-  const size_t host_tab = al256(host_end);
-  if (!shared.empty()) host_end = host_tab + (tab1 - tab0);
   s.in.reserve(std::max<size_t>(host_end, 256));
   s.out.reserve(std::max<size_t>(out_end - out_begin, 256));  // holds [out_begin, out_end)
   s.out_begin = out_begin;
@@ -333,11 +301,6 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
                                cudaMemcpyHostToDevice, s.stream),
                "copy descriptors");
     host_desc += al256(v.size() * sizeof(v[0]));
-  }
-  if (!shared.empty()) {
-    shared.fill(base, s.in.as() + host_tab - tab0);
-    cuda_check(cudaMemcpyAsync(base + tab0, s.in.as() + host_tab, tab1 - tab0, cudaMemcpyHostToDevice, s.stream),
-               "copy LDPC tables");
   }
 
   // ---- launches: every turbo frame in one mixed-K launch per algorithm on the slot's
@@ -356,27 +319,21 @@ bool fecl_server_s::launch(Slot& s, std::vector<std::shared_ptr<Request>>& batch
     cuda_check(fecl::launch_turbo_lte_batch(p, s.stream), "turbo batch launch");
   }
   bool used[kSideStreams] = {};
-  if (!shared.empty()) {
-    cuda_check(cudaStreamWaitEvent(s.side[0], s.fork, 0), "cudaStreamWaitEvent");
-    used[0] = true;
-    shared.launch(base, s.side[0], false);
-  }
-  const int first = shared.empty() ? 0 : 1;  // side stream 0 holds the shared launches
   // longest first, each to the side stream with the least work so far; a group's work
-  // is estimated by its parity bits times its iteration limit times its frame groups
+  // is estimated by its parity bits times its iteration limit times its frames
   std::vector<Group*> order;
   for (auto& kv : groups)
-    if (!kv.second.lte && !kv.second.shared) order.push_back(&kv.second);
+    if (!kv.second.lte) order.push_back(&kv.second);
   auto cost = [](const Group* g) {
     const double it = g->c->kind == 0 ? double(std::max(1, g->c->ldev.iterations)) : 1.0;
-    return double(g->c->parity()) * it * double((g->n + 63) / 64);
+    return double(g->c->parity()) * it * double(g->n);
   };
   std::stable_sort(order.begin(), order.end(), [&](const Group* a, const Group* b) { return cost(a) > cost(b); });
   double load[kSideStreams] = {};
   for (Group* gp : order) {
     Group& g = *gp;
-    int q = first;
-    for (int i = first + 1; i < kSideStreams; ++i)
+    int q = 0;
+    for (int i = 1; i < kSideStreams; ++i)
       if (load[i] < load[q]) q = i;
     load[q] += cost(gp);
     if (!used[q]) cuda_check(cudaStreamWaitEvent(s.side[q], s.fork, 0), "cudaStreamWaitEvent");
