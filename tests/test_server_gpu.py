@@ -116,3 +116,29 @@ def test_poisson_replay():
         assert np.array_equal(a, m)
     assert np.all(lat > 0)
     srv.close()
+
+
+def test_batches_larger_than_the_initial_staging():
+    """Batches whose L-values (FP32 DVB-S2 normal frames, 259 KB each) and decisions
+    outgrow a slot's initial pinned staging (64 MiB in, 16 MiB out): the buffers grow
+    while other slots' batches are in flight, and every request still gets the
+    decisions of its codec decoding alone."""
+    import fecl_b200 as F
+    from fecl_b200 import channel as ch
+    ms = F.Ldpc.DecoderOptions().algorithm(F.Approximate).iterations(20).scalingFactor(0.75).precision(1)
+    code = F.Ldpc(F.Ldpc.EncoderOptions(F.Ldpc.DvbS2.matrix(64800, Fraction(3, 4))), ms)
+    K, N = code.msgSize(), code.paritySize()
+    reqs = []
+    for i in range(6):
+        n = 100 + 20 * i
+        msg = ch.random_bits(n * K, 600 + i)
+        reqs.append((code, ch.awgn_llr(code.encode(msg), 2.8, K / N, 600 + i, np.float32)))
+    alone = _alone(reqs)
+    srv = F.Server(device_budget=12 << 30, max_batch_frames=400, slots=2)
+    tickets = [srv.submit(c, llr) for c, llr in reqs]
+    for a, t in zip(alone, tickets):
+        msg, _ = srv.wait(t)
+        assert np.array_equal(a, msg)
+    rep = srv.report()
+    assert rep["requests"] == len(reqs) and rep["frames"] == sum(100 + 20 * i for i in range(6))
+    srv.close()
