@@ -890,12 +890,35 @@ __global__ void turbo_lte_stage(TurboLteParams p) {
     // soDecode's a-priori input is added to the channel's systematic values and tails
     // (TurboDecoderImpl.cpp:77-82)
     const T* sys = p.syst_in ? static_cast<const T*>(p.syst_in) + f * int64_t(K + 6) : nullptr;
-    for (int i = threadIdx.x; i < Kp; i += blockDim.x)
-      out[i] = i < K ? (sys ? to_f32(in[i]) + to_f32(sys[i]) : to_f32(in[i])) : 0.0f;
+    // four elements per thread and step, all loaded before any is stored, so that each
+    // thread keeps four loads in flight (load latency, not bandwidth, bounds the copy)
+    constexpr int kU = 4;
+    const int step = int(blockDim.x);
+    for (int i0 = threadIdx.x; i0 < Kp; i0 += kU * step) {
+      float v[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int i = i0 + u * step;
+        v[u] = i < K ? (sys ? to_f32(in[i]) + to_f32(sys[i]) : to_f32(in[i])) : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+        if (i0 + u * step < Kp) out[i0 + u * step] = v[u];
+    }
     for (int c = 0; c < 2; ++c) {
       const T* src = in + K + 6 + c * (K + 3);  // parity (with its tail) of constituent c
       float* dst = out + Kp + c * Tp;
-      for (int t = threadIdx.x; t < Tp; t += blockDim.x) dst[t] = t < K + 3 ? to_f32(src[t]) : 0.0f;
+      for (int t0 = threadIdx.x; t0 < Tp; t0 += kU * step) {
+        float v[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const int t = t0 + u * step;
+          v[u] = t < K + 3 ? to_f32(src[t]) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+          if (t0 + u * step < Tp) dst[t0 + u * step] = v[u];
+      }
     }
     if (threadIdx.x < 8) {
       float v = 0.0f;
